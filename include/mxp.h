@@ -1,0 +1,222 @@
+/*
+ * mxp.h -- C ABI of the B200-native HPL-MxP single-GPU solve path.
+ *
+ * One GPU, 1x1 process grid: LCG matrix generation, blocked no-pivot LU with
+ * a low-precision Schur update on tcgen05 tensor cores, FP64 iterative
+ * refinement whose residual regenerates A on the fly.  Every entry point is
+ * extern "C" with plain pointers and sizes, takes the CUDA stream it runs on
+ * (as void*, 0 = legacy default stream), is asynchronous unless it says
+ * otherwise, and returns an mxp_status.  Matrices are column-major with an
+ * explicit leading dimension, as in the reference (panel.hpp:189-302).
+ * Pointers named d_* are device pointers; h_* are host pointers.
+ *
+ * The comment above each function names the reference interface it replaces
+ * (file:line in the OpenMxP source tree).
+ */
+#ifndef MXP_H
+#define MXP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MXP_OK = 0,
+    MXP_INVALID_ARG = 1,   /* bad size, alignment or pointer */
+    MXP_ZERO_PIVOT = 2,    /* zero / non-finite pivot in the no-pivot LU */
+    MXP_NONFINITE = 3,     /* NaN/Inf met in a vector or panel */
+    MXP_NOT_CONVERGED = 4, /* refinement hit maxit (iterative_refinement.hpp:173) */
+    MXP_TIMEOUT = 5,       /* a bounded device-side wait gave up */
+    MXP_CUDA_ERROR = 6,    /* a CUDA runtime / driver call failed */
+    MXP_UNSUPPORTED = 7,   /* form / size combination not built */
+    MXP_NO_MEMORY = 8
+} mxp_status;
+
+/* Precision form of the Schur update (FLOW in main.cpp:46-48). */
+typedef enum {
+    MXP_FORM_FP16 = 0,   /* plain: FP16 x FP16 -> FP32, as the reference */
+    MXP_FORM_BF16X2 = 1, /* split hi+lo BF16, three products, FP32 accumulate */
+    MXP_FORM_FP8 = 2     /* FP8 E4M3, power-of-two scale per 128x128 tile */
+} mxp_form;
+
+/* Diagonal of the generated matrix. */
+typedef enum {
+    MXP_DIAG_ROWSUM = 0,     /* reference: d_i = sum_{j!=i} |a_ij| (matgen.hpp:26-62) */
+    MXP_DIAG_055_PLUS1 = 1   /* stress form: d_i = 0.55 * rowsum_i + 1 */
+} mxp_diag_rule;
+
+typedef enum {
+    MXP_IR_CLASSIC = 0,      /* iterative_refinement2 (iterative_refinement.hpp:97-174) */
+    MXP_IR_GMRES = 1         /* GMRES-IR preconditioned by the low-precision LU */
+} mxp_ir_method;
+
+/* Per-phase device times of one LU, milliseconds (timer.hpp:58-85 items). */
+typedef struct {
+    double ms_total;
+    double ms_diag_lu;   /* DIAG_LU */
+    double ms_trsm;      /* TRSM_L + TRSM_R */
+    double ms_cast;      /* CONV_L + CONV_R */
+    double ms_schur;     /* GEMM_UPDATE */
+    int info;            /* 0, or 1 + global index of the first bad pivot */
+    int schur_launches;  /* tcgen05 Schur kernel launches */
+} mxp_lu_stats;
+
+typedef struct {
+    int iterations;      /* corrections applied before the residual test passed */
+    int converged;       /* 1 when scaled residual < threshold */
+    double residual;     /* ||b - A x||_inf (IRErrors.residual) */
+    double hpl_harness;  /* scaled residual (IRErrors.hpl_harness) */
+    double norma, normb, normx;
+    double ms_total, ms_gemv, ms_trsv;
+    int gemv_calls, trsv_calls;
+    double history[64];  /* scaled residual of every evaluation */
+} mxp_ir_stats;
+
+typedef struct mxp_workspace mxp_workspace;
+
+/* Library version string and the last error message of the calling thread. */
+const char *mxp_version(void);
+const char *mxp_last_error_string(void);
+
+/* Workspace for the LU and refinement: panel buffers (two L and two R, as
+ * LRPanels lr[4] of build_panels_wGPU, panel.hpp:361-454), FP8 scale
+ * tables, the diagonal-LU and TRSV scratch, IR vectors and a device status
+ * word.  All device memory the hot calls use is allocated here, once.
+ * device: CUDA ordinal the workspace lives on. */
+mxp_status mxp_workspace_create(int n, int b, int form, int device, mxp_workspace **out);
+mxp_status mxp_workspace_destroy(mxp_workspace *ws);
+size_t mxp_workspace_bytes(int n, int b, int form);
+
+/* ---- generation ------------------------------------------------------- */
+
+/* panel_matgen_dev + panel_colvgen (matgen.hpp:84-117, 419-436):
+ * A(i,j) = float(LCG(i + n*j)), d_i = row sum of |a_ij| over j != i in the
+ * reference's GPU reduction order (or the stress rule), A(i,i) = float(d_i),
+ * rhs_i = LCG(i + n*n).  Bit-exact with the reference generator.  Any of
+ * d_A, d_d, d_rowsum, d_rhs may be NULL to skip that output. */
+mxp_status mxp_matgen(int n, uint64_t seed, int diag_rule, float *d_A, int64_t lda, double *d_d,
+                      double *d_rowsum, double *d_rhs, void *stream);
+
+/* ---- granular LU pieces ----------------------------------------------- */
+
+/* GPUSOLVER_SGETRF(h, b, b, A, lda, work, NULL, info) (panel_trf.hpp:
+ * 547-551, 678-681): in-place FP32 no-pivot LU of an n x n block.  A zero
+ * or non-finite pivot is reported through the workspace status. */
+mxp_status mxp_getrf_nopiv(int n, float *d_A, int64_t lda, mxp_workspace *ws, void *stream);
+
+/* update_left_panels_wGPU (panel_trf.hpp:188-207):
+ * STRSM(Right, Upper, NoTrans, NonUnit): B(m x n) <- B * U^{-1}. */
+mxp_status mxp_trsm_right_upper(int m, int n, const float *d_U, int64_t ldu, float *d_B,
+                                int64_t ldb, void *stream);
+
+/* update_right_panels_wGPU (panel_trf.hpp:225-246):
+ * STRSM(Left, Lower, NoTrans, Unit): B(m x n) <- L^{-1} * B. */
+mxp_status mxp_trsm_left_lower_unit(int m, int n, const float *d_L, int64_t ldl, float *d_B,
+                                    int64_t ldb, void *stream);
+
+/* half_conversion_left (fp16_gpu_kernels.h:26-27, .cpp:180-192): FP32 m x b
+ * block (column-major, plda) -> FP16 column-major (lplda), round to nearest.
+ * Reference layout; bit-exact with copyCoalesced. */
+mxp_status mxp_half_conversion_left(const float *d_C, int m, int b, int64_t plda, uint16_t *d_lp,
+                                    int64_t lplda, void *stream);
+
+/* half_conversion_right_trans (fp16_gpu_kernels.h:28-29, .cpp:196-211):
+ * FP32 b x m block (plda) -> FP16 transposed, rp[k*rplda + j] = C(k, j).
+ * Reference layout; bit-exact with transposeCoalesced. */
+mxp_status mxp_half_conversion_right_trans(const float *d_C, int b, int m, int64_t plda,
+                                           uint16_t *d_rp, int64_t rplda, void *stream);
+
+/* Panel casts in the layout the tcgen05 Schur kernel reads: K-major rows
+ * (row i holds its K values contiguously, ld = ldk elements).
+ *  left : L column panel, FP32 m x b column-major (lda)   -> m rows
+ *  right: U row panel,    FP32 b x m column-major (lda)   -> m rows (= U^T)
+ * form FP16: K = b, 2-byte elements.  BF16X2: K = 3b (hi|hi|lo for left,
+ * hi|lo|hi for right).  FP8: K = b, 1-byte elements, plus one UE8M0 scale
+ * byte per 128 x 128 tile in d_scales (row-tile major, ceil(m/128) x
+ * ceil(b/128)).  Replaces convert_left/right_panels_wGPU (panel_trf.hpp:
+ * 258-277, 305-325). */
+mxp_status mxp_panel_cast_left(int form, int m, int b, const float *d_A, int64_t lda, void *d_out,
+                               int64_t ldk, uint8_t *d_scales, void *stream);
+mxp_status mxp_panel_cast_right(int form, int m, int b, const float *d_A, int64_t lda, void *d_out,
+                                int64_t ldk, uint8_t *d_scales, void *stream);
+
+/* GPUBLAS_SGEMM_EX(OP_N, OP_T, m, n, k, -1, L, lda, R, ldb, 1, C, ldc)
+ * (panel_trf.hpp:828-834, rocm_device_macros.h:267-268): C(m x n, FP32,
+ * column-major) -= L * R^T on tcgen05 tensor cores, FP32 accumulation.
+ * L and R are K-major panels from mxp_panel_cast_*; k is the panel width b
+ * (the kernel multiplies it by 3 for BF16X2).  Scales only for FP8. */
+mxp_status mxp_schur_update(int form, int m, int n, int k, const void *d_L, int64_t ldl,
+                            const uint8_t *d_lscales, const void *d_R, int64_t ldr,
+                            const uint8_t *d_rscales, float *d_C, int64_t ldc,
+                            mxp_workspace *ws, void *stream);
+
+/* ---- whole LU ------------------------------------------------------------ */
+
+/* panel_lu_async_wGPU (panel_trf.hpp:470-867) at a 1x1 grid: in-place
+ * blocked no-pivot LU of the n x n FP32 matrix with block size b (n % b ==
+ * 0), Schur update in the workspace's form.  Synchronises the stream at the
+ * end to read the pivot status; fills stats when non-NULL. */
+mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_workspace *ws, void *stream,
+                        mxp_lu_stats *stats);
+
+/* ---- refinement ------------------------------------------------------------ */
+
+/* otf_gemv_h / panel_gemv_h (panel_gemv.hpp:83-179): y = beta*y +
+ * alpha*A*x with a_ij regenerated from the LCG in FP64 (never read from
+ * memory) and the diagonal taken from d.  Deterministic. */
+mxp_status mxp_otf_gemv(int n, uint64_t seed, const double *d_d, double alpha, const double *d_x,
+                        double beta, double *d_y, mxp_workspace *ws, void *stream);
+
+/* trsvL_h + trsvU_h (panel_trsv.hpp:308-597): x <- U^{-1} L^{-1} x with
+ * the FP32 factors of mxp_panel_lu, vectors in FP64, exact block
+ * substitution. */
+mxp_status mxp_lu_solve(int n, const float *d_LU, int64_t lda, double *d_x, mxp_workspace *ws,
+                        void *stream);
+
+/* iterative_refinement2, GPU branch (iterative_refinement.hpp:141-171):
+ * x0 = rhs ./ d, then refine until the scaled residual
+ * ||r||inf / (norma ||x||inf + normb) / (n eps/2) < 16 or maxit.
+ * norma <= 0 selects 2*max(d) (hpl_infnorm, panel_norm.hpp:129-135) or,
+ * with d_rowsum != NULL, max(rowsum + d).  Blocking: returns when done. */
+mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float *d_LU, int64_t lda,
+                                    const double *d_d, const double *d_rowsum,
+                                    const double *d_rhs, double *d_x, double norma, int maxit,
+                                    int method, mxp_workspace *ws, void *stream,
+                                    mxp_ir_stats *stats);
+
+/* The timed region of main.cpp:617-657 in one call: LU then refinement on
+ * a matrix produced by mxp_matgen.  d_A is overwritten by the factors. */
+mxp_status mxp_solve(int n, int b, uint64_t seed, float *d_A, int64_t lda, const double *d_d,
+                     const double *d_rowsum, const double *d_rhs, double *d_x, int maxit,
+                     int method, mxp_workspace *ws, void *stream, mxp_lu_stats *lu_stats,
+                     mxp_ir_stats *ir_stats);
+
+/* Host-buffer variant (the end-to-end call): rhs is read from host memory
+ * and x written to host memory, both copies on the stream inside the call
+ * and staged in the workspace (no allocation).  A, d (and rowsum for the
+ * stress rule) are device-resident, produced by mxp_matgen as in the
+ * reference's default -init 1 path (main.cpp:536-538).  Blocking. */
+mxp_status mxp_solve_host(int n, int b, uint64_t seed, float *d_A, int64_t lda, const double *d_d,
+                          const double *d_rowsum, const double *h_rhs, double *h_x, int maxit,
+                          int method, mxp_workspace *ws, void *stream, mxp_lu_stats *lu_stats,
+                          mxp_ir_stats *ir_stats);
+
+/* ---- small utilities ------------------------------------------------------ */
+
+/* ||x||_inf of a device FP64 vector (colv_infnorm_h, panel_norm.hpp:35-58).
+ * Blocking. */
+mxp_status mxp_infnorm(int n, const double *d_x, double *h_out, mxp_workspace *ws, void *stream);
+
+/* Number of tcgen05 / other kernels this library launched on the calling
+ * thread since the last reset (for launch accounting in benchmarks). */
+int64_t mxp_kernel_launches(void);
+void mxp_reset_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MXP_H */

@@ -1,0 +1,305 @@
+"""openmxp_b200: B200-native single-GPU HPL-MxP solve path.
+
+Python mirror of the reference's host interface for the path (panel_matgen_dev,
+panel_lu_async_wGPU, iterative_refinement2, otf_gemv, the panel casts and the
+Schur gemm_ex), calling the CUDA library libmxp.so through its C ABI
+(include/mxp.h).  torch provides device memory and streams only.  There is no
+CPU fallback: every call fails loudly when the extension is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libmxp.so")
+
+# enums of include/mxp.h
+OK, INVALID_ARG, ZERO_PIVOT, NONFINITE, NOT_CONVERGED, TIMEOUT, CUDA_ERROR, UNSUPPORTED, NO_MEMORY = range(9)
+FORM_FP16, FORM_BF16X2, FORM_FP8 = 0, 1, 2
+FORMS = {"fp16": FORM_FP16, "bf16x2": FORM_BF16X2, "fp8": FORM_FP8}
+DIAG_ROWSUM, DIAG_055_PLUS1 = 0, 1
+IR_CLASSIC, IR_GMRES = 0, 1
+STATUS_NAMES = ["OK", "INVALID_ARG", "ZERO_PIVOT", "NONFINITE", "NOT_CONVERGED", "TIMEOUT",
+                "CUDA_ERROR", "UNSUPPORTED", "NO_MEMORY"]
+
+
+class MxpError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        self.status = status
+        name = STATUS_NAMES[status] if 0 <= status < len(STATUS_NAMES) else str(status)
+        super().__init__(f"{name}: {msg}")
+
+
+class LuStats(C.Structure):
+    _fields_ = [("ms_total", C.c_double), ("ms_diag_lu", C.c_double), ("ms_trsm", C.c_double),
+                ("ms_cast", C.c_double), ("ms_schur", C.c_double), ("info", C.c_int),
+                ("schur_launches", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class IrStats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("residual", C.c_double),
+                ("hpl_harness", C.c_double), ("norma", C.c_double), ("normb", C.c_double),
+                ("normx", C.c_double), ("ms_total", C.c_double), ("ms_gemv", C.c_double),
+                ("ms_trsv", C.c_double), ("gemv_calls", C.c_int), ("trsv_calls", C.c_int),
+                ("history", C.c_double * 64)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "history"}
+        d["history"] = [self.history[i] for i in range(min(64, self.iterations + 1))]
+        return d
+
+
+_lib = None
+_vp, _i32, _i64, _u64, _dbl = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double
+
+# name -> (restype, argtypes); mirrors include/mxp.h
+_SIGS = {
+    "mxp_version": (C.c_char_p, []),
+    "mxp_last_error_string": (C.c_char_p, []),
+    "mxp_workspace_create": (_i32, [_i32, _i32, _i32, _i32, C.POINTER(_vp)]),
+    "mxp_workspace_destroy": (_i32, [_vp]),
+    "mxp_workspace_bytes": (C.c_size_t, [_i32, _i32, _i32]),
+    "mxp_matgen": (_i32, [_i32, _u64, _i32, _vp, _i64, _vp, _vp, _vp, _vp]),
+    "mxp_getrf_nopiv": (_i32, [_i32, _vp, _i64, _vp, _vp]),
+    "mxp_trsm_right_upper": (_i32, [_i32, _i32, _vp, _i64, _vp, _i64, _vp]),
+    "mxp_trsm_left_lower_unit": (_i32, [_i32, _i32, _vp, _i64, _vp, _i64, _vp]),
+    "mxp_half_conversion_left": (_i32, [_vp, _i32, _i32, _i64, _vp, _i64, _vp]),
+    "mxp_half_conversion_right_trans": (_i32, [_vp, _i32, _i32, _i64, _vp, _i64, _vp]),
+    "mxp_panel_cast_left": (_i32, [_i32, _i32, _i32, _vp, _i64, _vp, _i64, _vp, _vp]),
+    "mxp_panel_cast_right": (_i32, [_i32, _i32, _i32, _vp, _i64, _vp, _i64, _vp, _vp]),
+    "mxp_schur_update": (_i32, [_i32, _i32, _i32, _i32, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _i64,
+                                _vp, _vp]),
+    "mxp_panel_lu": (_i32, [_i32, _i32, _vp, _i64, _vp, _vp, C.POINTER(LuStats)]),
+    "mxp_otf_gemv": (_i32, [_i32, _u64, _vp, _dbl, _vp, _dbl, _vp, _vp, _vp]),
+    "mxp_lu_solve": (_i32, [_i32, _vp, _i64, _vp, _vp, _vp]),
+    "mxp_iterative_refinement": (_i32, [_i32, _u64, _vp, _i64, _vp, _vp, _vp, _vp, _dbl, _i32,
+                                        _i32, _vp, _vp, C.POINTER(IrStats)]),
+    "mxp_solve": (_i32, [_i32, _i32, _u64, _vp, _i64, _vp, _vp, _vp, _vp, _i32, _i32, _vp, _vp,
+                         C.POINTER(LuStats), C.POINTER(IrStats)]),
+    "mxp_solve_host": (_i32, [_i32, _i32, _u64, _vp, _i64, _vp, _vp, _vp, _vp, _i32, _i32, _vp,
+                              _vp, C.POINTER(LuStats), C.POINTER(IrStats)]),
+    "mxp_infnorm": (_i32, [_i32, _vp, C.POINTER(_dbl), _vp, _vp]),
+    "mxp_kernel_launches": (_i64, []),
+    "mxp_reset_kernel_launches": (None, []),
+}
+
+
+def lib() -> C.CDLL:
+    """Load libmxp.so (raises if it was not built: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m openmxp_b200.build` "
+                              "(or __graft_entry__.build()) first")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != OK:
+        raise MxpError(status, lib().mxp_last_error_string().decode())
+
+
+def _ptr(t) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _stream(stream=None) -> int:
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+# ---------------------------------------------------------------------------
+# workspace (LRPanels / Workspace of the reference, panel.hpp:169-187, 321-454)
+# ---------------------------------------------------------------------------
+class Workspace:
+    def __init__(self, n: int, b: int, form: int | str = FORM_FP16, device: int = 0):
+        if isinstance(form, str):
+            form = FORMS[form]
+        self.n, self.b, self.form, self.device = n, b, form, device
+        h = _vp()
+        check(lib().mxp_workspace_create(n, b, form, device, C.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            lib().mxp_workspace_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def bytes(n: int, b: int, form: int = FORM_FP16) -> int:
+        return int(lib().mxp_workspace_bytes(n, b, form))
+
+
+# ---------------------------------------------------------------------------
+# matrices (Panels at a 1x1 grid: one column-major n x n FP32 matrix)
+# ---------------------------------------------------------------------------
+@dataclass
+class Problem:
+    n: int
+    seed: int
+    diag_rule: int
+    A: "object"        # torch float32, n*lda elements, column-major
+    lda: int
+    d: "object"        # torch float64 [n]
+    rowsum: "object"   # torch float64 [n]
+    rhs: "object"      # torch float64 [n]
+
+    def matrix(self):
+        """A as an (n x n) torch view with A[i, j] = a_ij (column-major storage)."""
+        return self.A.view(self.n, self.lda)[:, : self.n].t()
+
+
+def panel_matgen(n: int, seed: int = 42, diag_rule: int = DIAG_ROWSUM, device=None,
+                 A=None, lda: int | None = None, stream=None) -> Problem:
+    """panel_matgen_dev + panel_colvgen (matgen.hpp:84-117, 419-436)."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    lda = n if lda is None else lda
+    if A is None:
+        A = torch.empty(n * lda, dtype=torch.float32, device=dev)
+    d = torch.empty(n, dtype=torch.float64, device=dev)
+    rs = torch.empty(n, dtype=torch.float64, device=dev)
+    rhs = torch.empty(n, dtype=torch.float64, device=dev)
+    check(lib().mxp_matgen(n, seed, diag_rule, _ptr(A), lda, _ptr(d), _ptr(rs), _ptr(rhs),
+                           _stream(stream)))
+    return Problem(n, seed, diag_rule, A, lda, d, rs, rhs)
+
+
+def regenerate(p: Problem, stream=None) -> None:
+    """Refill p.A (and d / rowsum / rhs) in place."""
+    check(lib().mxp_matgen(p.n, p.seed, p.diag_rule, _ptr(p.A), p.lda, _ptr(p.d), _ptr(p.rowsum),
+                           _ptr(p.rhs), _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# LU (panel_lu_async_wGPU, panel_trf.hpp:470-867)
+# ---------------------------------------------------------------------------
+def panel_lu(p: Problem, b: int, ws: Workspace, stream=None) -> dict:
+    st = LuStats()
+    check(lib().mxp_panel_lu(p.n, b, _ptr(p.A), p.lda, ws.handle, _stream(stream), C.byref(st)))
+    return st.as_dict()
+
+
+def getrf_nopiv(A, n: int, lda: int, ws: Workspace, stream=None) -> None:
+    check(lib().mxp_getrf_nopiv(n, _ptr(A), lda, ws.handle, _stream(stream)))
+
+
+def trsm_right_upper(m, n, U, ldu, B, ldb, stream=None):
+    check(lib().mxp_trsm_right_upper(m, n, _ptr(U), ldu, _ptr(B), ldb, _stream(stream)))
+
+
+def trsm_left_lower_unit(m, n, L, ldl, B, ldb, stream=None):
+    check(lib().mxp_trsm_left_lower_unit(m, n, _ptr(L), ldl, _ptr(B), ldb, _stream(stream)))
+
+
+def half_conversion_left(Cm, m, b, plda, lp, lplda, stream=None):
+    check(lib().mxp_half_conversion_left(_ptr(Cm), m, b, plda, _ptr(lp), lplda, _stream(stream)))
+
+
+def half_conversion_right_trans(Cm, b, m, plda, rp, rplda, stream=None):
+    check(lib().mxp_half_conversion_right_trans(_ptr(Cm), b, m, plda, _ptr(rp), rplda, _stream(stream)))
+
+
+def panel_cast_left(form, m, b, A, lda, out, ldk, scales=None, stream=None):
+    check(lib().mxp_panel_cast_left(form, m, b, _ptr(A), lda, _ptr(out), ldk, _ptr(scales),
+                                    _stream(stream)))
+
+
+def panel_cast_right(form, m, b, A, lda, out, ldk, scales=None, stream=None):
+    check(lib().mxp_panel_cast_right(form, m, b, _ptr(A), lda, _ptr(out), ldk, _ptr(scales),
+                                     _stream(stream)))
+
+
+def schur_update(form, m, n, k, Lp, ldl, Rp, ldr, Cm, ldc, ws: Workspace, lscales=None,
+                 rscales=None, stream=None):
+    check(lib().mxp_schur_update(form, m, n, k, _ptr(Lp), ldl, _ptr(lscales), _ptr(Rp), ldr,
+                                 _ptr(rscales), _ptr(Cm), ldc, ws.handle, _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# refinement (iterative_refinement2, iterative_refinement.hpp:97-174)
+# ---------------------------------------------------------------------------
+def otf_gemv(n, seed, d, alpha, x, beta, y, ws: Workspace, stream=None):
+    check(lib().mxp_otf_gemv(n, seed, _ptr(d), alpha, _ptr(x), beta, _ptr(y), ws.handle,
+                             _stream(stream)))
+
+
+def lu_solve(LU, n, lda, x, ws: Workspace, stream=None):
+    check(lib().mxp_lu_solve(n, _ptr(LU), lda, _ptr(x), ws.handle, _stream(stream)))
+
+
+def iterative_refinement(p: Problem, ws: Workspace, x=None, maxit: int = 50,
+                         method: int = IR_CLASSIC, stream=None, raise_on_fail: bool = True):
+    import torch
+    if x is None:
+        x = torch.empty(p.n, dtype=torch.float64, device=p.A.device)
+    st = IrStats()
+    rs = p.rowsum if p.diag_rule != DIAG_ROWSUM else None
+    s = lib().mxp_iterative_refinement(p.n, p.seed, _ptr(p.A), p.lda, _ptr(p.d), _ptr(rs),
+                                       _ptr(p.rhs), _ptr(x), 0.0, maxit, method, ws.handle,
+                                       _stream(stream), C.byref(st))
+    if raise_on_fail:
+        check(s)
+    return x, st.as_dict(), s
+
+
+def solve(p: Problem, b: int, ws: Workspace, x=None, maxit: int = 50, method: int = IR_CLASSIC,
+          stream=None):
+    """LU then refinement: the timed region of main.cpp:617-657."""
+    import torch
+    if x is None:
+        x = torch.empty(p.n, dtype=torch.float64, device=p.A.device)
+    lst, ist = LuStats(), IrStats()
+    rs = p.rowsum if p.diag_rule != DIAG_ROWSUM else None
+    check(lib().mxp_solve(p.n, b, p.seed, _ptr(p.A), p.lda, _ptr(p.d), _ptr(rs), _ptr(p.rhs),
+                          _ptr(x), maxit, method, ws.handle, _stream(stream), C.byref(lst),
+                          C.byref(ist)))
+    return x, lst.as_dict(), ist.as_dict()
+
+
+def solve_host(p: Problem, b: int, ws: Workspace, h_rhs, h_x, maxit: int = 50,
+               method: int = IR_CLASSIC, stream=None):
+    """End-to-end call with host buffers (pinned torch CPU tensors)."""
+    lst, ist = LuStats(), IrStats()
+    rs = p.rowsum if p.diag_rule != DIAG_ROWSUM else None
+    check(lib().mxp_solve_host(p.n, b, p.seed, _ptr(p.A), p.lda, _ptr(p.d), _ptr(rs), _ptr(h_rhs),
+                               _ptr(h_x), maxit, method, ws.handle, _stream(stream), C.byref(lst),
+                               C.byref(ist)))
+    return lst.as_dict(), ist.as_dict()
+
+
+def infnorm(x, ws: Workspace, stream=None) -> float:
+    out = C.c_double(0.0)
+    check(lib().mxp_infnorm(x.numel(), _ptr(x), C.byref(out), ws.handle, _stream(stream)))
+    return out.value
+
+
+def kernel_launches() -> int:
+    return int(lib().mxp_kernel_launches())
+
+
+def reset_kernel_launches() -> None:
+    lib().mxp_reset_kernel_launches()
+
+
+def hpl_flops(n: int) -> float:
+    """Credited FLOPs of main.cpp:663: 2/3 n^3 + 3/2 n^2."""
+    return 2.0 / 3.0 * n ** 3 + 1.5 * n ** 2

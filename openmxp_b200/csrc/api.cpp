@@ -1,0 +1,510 @@
+// Host driver and C ABI of libmxp.
+//
+// mxp_panel_lu is the single-GPU (1x1 grid) form of panel_lu_async_wGPU
+// (panel_trf.hpp:470-867): the reference's broadcasts of the diagonal
+// factor and of the FP16 panels (broadcast_pivlu_wGPU, broadcast_left/
+// right_panels, :63-170) and its per-step host copies of the panels become
+// on-device hand-offs: the cast kernels write the panels straight into the
+// buffers the Schur kernel reads.  All calls are stream-ordered; the only
+// synchronisation of the LU is the final read of the device status word.
+//
+// mxp_iterative_refinement follows the GPU branch of iterative_refinement2
+// (iterative_refinement.hpp:141-171); its one host synchronisation per step
+// is the 16-byte read of ||x|| and ||r|| needed for the stopping test.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "mxp_internal.cuh"
+
+// ---------------------------------------------------------------------------
+// status plumbing
+// ---------------------------------------------------------------------------
+namespace mxp {
+
+static thread_local std::string g_last_error;
+static std::atomic<int64_t> g_launches{0};
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+mxp_status fail(mxp_status st, const std::string &msg) {
+    g_last_error = msg;
+    return st;
+}
+
+mxp_status cuda_fail(cudaError_t e, const char *where) {
+    g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+    return MXP_CUDA_ERROR;
+}
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int num_sms() {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 148;
+}
+
+}  // namespace mxp
+
+using namespace mxp;
+
+// ---------------------------------------------------------------------------
+// workspace
+// ---------------------------------------------------------------------------
+struct mxp_workspace {
+    int n = 0, b = 0, form = 0, device = 0;
+    int64_t ldk = 0;         // K-major panel leading dimension (elements)
+    size_t esize = 2;        // panel element size
+    void *lpanel[2] = {nullptr, nullptr};
+    void *rpanel[2] = {nullptr, nullptr};
+    uint8_t *lscale[2] = {nullptr, nullptr};
+    uint8_t *rscale[2] = {nullptr, nullptr};
+    DevStatus *status = nullptr;
+    double *vec = nullptr;   // IR vectors: r, w, x, rhs | gemv partials | scalars
+    double *r = nullptr, *w = nullptr, *xv = nullptr, *rhsv = nullptr;
+    double *partials = nullptr, *scal = nullptr;
+    int max_splits = 16;
+    int *flags = nullptr;
+    double *h_scal = nullptr;  // pinned host scalars
+    std::vector<void *> allocs;
+};
+
+static int64_t panel_ldk(int b, int form) {
+    const int64_t K = form == MXP_FORM_BF16X2 ? 3 * (int64_t)b : b;
+    const int64_t esize = form == MXP_FORM_FP8 ? 1 : 2;
+    const int64_t align = 16 / esize;
+    return (K + align - 1) / align * align;
+}
+
+static size_t ws_layout(int n, int b, int form, size_t *panel_bytes, size_t *scale_bytes,
+                        size_t *vec_doubles, size_t *flag_ints) {
+    const int64_t ldk = panel_ldk(b, form);
+    const int64_t esize = form == MXP_FORM_FP8 ? 1 : 2;
+    const int64_t rows = n > b ? n - b : 1;
+    *panel_bytes = (size_t)(rows * ldk * esize + 1024) / 256 * 256 + 256;
+    *scale_bytes = (size_t)(cdiv(rows, 128) * cdiv(b, 128) + 256) / 256 * 256 + 256;
+    *vec_doubles = (size_t)n * (4 + 16) + 64;
+    *flag_ints = lu_solve_flag_ints(n) + 64;
+    return 4 * *panel_bytes + 4 * *scale_bytes + *vec_doubles * 8 + *flag_ints * 4 + 256;
+}
+
+extern "C" size_t mxp_workspace_bytes(int n, int b, int form) {
+    size_t pb, sb, vd, fi;
+    if (n <= 0 || b <= 0) return 0;
+    return ws_layout(n, b, form, &pb, &sb, &vd, &fi);
+}
+
+extern "C" mxp_status mxp_workspace_destroy(mxp_workspace *ws) {
+    if (!ws) return MXP_OK;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(ws->device);
+    for (void *p : ws->allocs) cudaFree(p);
+    if (ws->h_scal) cudaFreeHost(ws->h_scal);
+    cudaSetDevice(cur);
+    delete ws;
+    return MXP_OK;
+}
+
+extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, mxp_workspace **out) {
+    if (!out) return fail(MXP_INVALID_ARG, "workspace_create: out is NULL");
+    *out = nullptr;
+    if (n <= 0 || b <= 0 || b > n) return fail(MXP_INVALID_ARG, "workspace_create: bad n/b");
+    if (form != MXP_FORM_FP16 && form != MXP_FORM_BF16X2 && form != MXP_FORM_FP8)
+        return fail(MXP_INVALID_ARG, "workspace_create: unknown form");
+    int cur = 0;
+    MXP_CUDA(cudaGetDevice(&cur));
+    MXP_CUDA(cudaSetDevice(device));
+    mxp_workspace *ws = new mxp_workspace();
+    ws->n = n;
+    ws->b = b;
+    ws->form = form;
+    ws->device = device;
+    ws->ldk = panel_ldk(b, form);
+    ws->esize = form == MXP_FORM_FP8 ? 1 : 2;
+    size_t pb, sb, vd, fi;
+    ws_layout(n, b, form, &pb, &sb, &vd, &fi);
+    auto alloc = [&](size_t bytes) -> void * {
+        void *p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+        ws->allocs.push_back(p);
+        return p;
+    };
+    bool ok = true;
+    for (int i = 0; i < 2 && ok; ++i) {
+        ok = (ws->lpanel[i] = alloc(pb)) && (ws->rpanel[i] = alloc(pb)) &&
+             (ws->lscale[i] = (uint8_t *)alloc(sb)) && (ws->rscale[i] = (uint8_t *)alloc(sb));
+    }
+    ok = ok && (ws->status = (DevStatus *)alloc(sizeof(DevStatus) * 4));
+    ok = ok && (ws->vec = (double *)alloc(vd * sizeof(double)));
+    ok = ok && (ws->flags = (int *)alloc(fi * sizeof(int)));
+    if (ok) ok = cudaMallocHost(&ws->h_scal, 64 * sizeof(double)) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        mxp_workspace_destroy(ws);
+        cudaSetDevice(cur);
+        return fail(MXP_NO_MEMORY, "workspace_create: device allocation failed");
+    }
+    ws->r = ws->vec;
+    ws->w = ws->vec + n;
+    ws->xv = ws->vec + 2 * (size_t)n;
+    ws->rhsv = ws->vec + 3 * (size_t)n;
+    ws->partials = ws->vec + 4 * (size_t)n;
+    ws->scal = ws->vec + 20 * (size_t)n;
+    cudaMemset(ws->status, 0, sizeof(DevStatus) * 4);
+    cudaMemset(ws->flags, 0, fi * sizeof(int));
+    cudaDeviceSynchronize();
+    cudaSetDevice(cur);
+    *out = ws;
+    return MXP_OK;
+}
+
+// Read and clear the device status word; synchronises the stream.
+static mxp_status read_status(mxp_workspace *ws, cudaStream_t st, DevStatus *out = nullptr) {
+    DevStatus h;
+    MXP_CUDA(cudaMemcpyAsync(&h, ws->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+    MXP_CUDA(cudaStreamSynchronize(st));
+    if (out) *out = h;
+    if (h.code != 0) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "device status %d (detail %d, %d)", h.code, h.info0, h.info1);
+        MXP_CUDA(cudaMemsetAsync(ws->status, 0, sizeof(DevStatus), st));
+        return fail((mxp_status)h.code, buf);
+    }
+    return MXP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// simple entry points
+// ---------------------------------------------------------------------------
+extern "C" const char *mxp_version(void) { return "openmxp_b200 0.1 (sm_100a)"; }
+extern "C" const char *mxp_last_error_string(void) { return g_last_error.c_str(); }
+extern "C" int64_t mxp_kernel_launches(void) { return g_launches.load(); }
+extern "C" void mxp_reset_kernel_launches(void) { g_launches.store(0); }
+
+extern "C" mxp_status mxp_matgen(int n, uint64_t seed, int diag_rule, float *d_A, int64_t lda,
+                                 double *d_d, double *d_rowsum, double *d_rhs, void *stream) {
+    return launch_matgen(n, seed, diag_rule, d_A, lda, d_d, d_rowsum, d_rhs, as_stream(stream));
+}
+
+extern "C" mxp_status mxp_getrf_nopiv(int n, float *d_A, int64_t lda, mxp_workspace *ws,
+                                      void *stream) {
+    if (!ws) return fail(MXP_INVALID_ARG, "getrf: workspace is NULL");
+    cudaStream_t st = as_stream(stream);
+    mxp_status s = launch_getrf_blocked(n, d_A, lda, ws->status, 0, st);
+    if (s != MXP_OK) return s;
+    return read_status(ws, st);
+}
+
+extern "C" mxp_status mxp_trsm_right_upper(int m, int n, const float *d_U, int64_t ldu, float *d_B,
+                                           int64_t ldb, void *stream) {
+    return launch_trsm_runn(m, n, d_U, ldu, d_B, ldb, as_stream(stream));
+}
+
+extern "C" mxp_status mxp_trsm_left_lower_unit(int m, int n, const float *d_L, int64_t ldl,
+                                               float *d_B, int64_t ldb, void *stream) {
+    return launch_trsm_llnu(m, n, d_L, ldl, d_B, ldb, as_stream(stream));
+}
+
+extern "C" mxp_status mxp_half_conversion_left(const float *d_C, int m, int b, int64_t plda,
+                                               uint16_t *d_lp, int64_t lplda, void *stream) {
+    return launch_half_left_ref(d_C, m, b, plda, d_lp, lplda, as_stream(stream));
+}
+
+extern "C" mxp_status mxp_half_conversion_right_trans(const float *d_C, int b, int m, int64_t plda,
+                                                      uint16_t *d_rp, int64_t rplda, void *stream) {
+    return launch_half_right_trans_ref(d_C, b, m, plda, d_rp, rplda, as_stream(stream));
+}
+
+extern "C" mxp_status mxp_panel_cast_left(int form, int m, int b, const float *d_A, int64_t lda,
+                                          void *d_out, int64_t ldk, uint8_t *d_scales, void *stream) {
+    return launch_cast_left(form, m, b, d_A, lda, d_out, ldk, d_scales, as_stream(stream));
+}
+
+extern "C" mxp_status mxp_panel_cast_right(int form, int m, int b, const float *d_A, int64_t lda,
+                                           void *d_out, int64_t ldk, uint8_t *d_scales, void *stream) {
+    return launch_cast_right(form, m, b, d_A, lda, d_out, ldk, d_scales, as_stream(stream));
+}
+
+extern "C" mxp_status mxp_schur_update(int form, int m, int n, int k, const void *d_L, int64_t ldl,
+                                       const uint8_t *d_lscales, const void *d_R, int64_t ldr,
+                                       const uint8_t *d_rscales, float *d_C, int64_t ldc,
+                                       mxp_workspace *ws, void *stream) {
+    if (!ws) return fail(MXP_INVALID_ARG, "schur: workspace is NULL");
+    return launch_schur(form, m, n, k, d_L, ldl, d_lscales, d_R, ldr, d_rscales, d_C, ldc,
+                        ws->status, as_stream(stream));
+}
+
+// ---------------------------------------------------------------------------
+// LU
+// ---------------------------------------------------------------------------
+namespace {
+struct PhaseTimer {
+    bool on = false;
+    cudaStream_t st = 0;
+    std::vector<std::pair<cudaEvent_t, int>> marks;  // event, phase id after it
+    void mark(int phase) {
+        if (!on) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, st);
+        marks.push_back({e, phase});
+    }
+    // returns ms per phase id
+    void collect(double *ms, int nphase) {
+        for (int i = 0; i < nphase; ++i) ms[i] = 0.0;
+        for (size_t i = 0; i + 1 < marks.size(); ++i) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, marks[i].first, marks[i + 1].first);
+            const int ph = marks[i].second;
+            if (ph >= 0 && ph < nphase) ms[ph] += t;
+        }
+        for (auto &m : marks) cudaEventDestroy(m.first);
+        marks.clear();
+    }
+};
+enum { PH_DIAG = 0, PH_TRSM = 1, PH_CAST = 2, PH_SCHUR = 3, PH_END = 4 };
+}  // namespace
+
+extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_workspace *ws,
+                                   void *stream, mxp_lu_stats *stats) {
+    if (!ws || !d_A) return fail(MXP_INVALID_ARG, "panel_lu: NULL argument");
+    if (n <= 0 || b <= 0 || n % b != 0) return fail(MXP_INVALID_ARG, "panel_lu: n must be a positive multiple of b");
+    if (lda < n) return fail(MXP_INVALID_ARG, "panel_lu: lda < n");
+    if (n > ws->n || b != ws->b) return fail(MXP_INVALID_ARG, "panel_lu: workspace built for another n/b");
+    cudaStream_t st = as_stream(stream);
+    const int form = ws->form;
+    const int nb = n / b;
+    MXP_CUDA(cudaMemsetAsync(ws->status, 0, sizeof(DevStatus), st));
+    PhaseTimer pt;
+    pt.on = stats != nullptr;
+    pt.st = st;
+    int schur_launches = 0;
+    mxp_status s = MXP_OK;
+    for (int k = 0; k < nb && s == MXP_OK; ++k) {
+        const int64_t kk = (int64_t)k * b;
+        float *Akk = d_A + kk + kk * lda;
+        pt.mark(PH_DIAG);
+        s = launch_getrf_blocked(b, Akk, lda, ws->status, (int)kk, st);
+        if (s != MXP_OK) break;
+        const int m = n - (int)kk - b;
+        if (m <= 0) break;
+        float *Lcol = Akk + b;
+        float *Urow = Akk + (int64_t)b * lda;
+        pt.mark(PH_TRSM);
+        s = launch_trsm_runn(m, b, Akk, lda, Lcol, lda, st);
+        if (s == MXP_OK) s = launch_trsm_llnu(b, m, Akk, lda, Urow, lda, st);
+        if (s != MXP_OK) break;
+        const int buf = k & 1;
+        pt.mark(PH_CAST);
+        s = launch_cast_left(form, m, b, Lcol, lda, ws->lpanel[buf], ws->ldk, ws->lscale[buf], st);
+        if (s == MXP_OK)
+            s = launch_cast_right(form, m, b, Urow, lda, ws->rpanel[buf], ws->ldk, ws->rscale[buf], st);
+        if (s != MXP_OK) break;
+        pt.mark(PH_SCHUR);
+        s = launch_schur(form, m, m, b, ws->lpanel[buf], ws->ldk, ws->lscale[buf], ws->rpanel[buf],
+                         ws->ldk, ws->rscale[buf], Akk + b + (int64_t)b * lda, lda, ws->status, st);
+        ++schur_launches;
+    }
+    pt.mark(PH_END);
+    if (s != MXP_OK) {
+        pt.collect(nullptr, 0);
+        return s;
+    }
+    DevStatus h;
+    mxp_status rs = read_status(ws, st, &h);
+    if (stats) {
+        double ms[4];
+        pt.collect(ms, 4);
+        stats->ms_diag_lu = ms[PH_DIAG];
+        stats->ms_trsm = ms[PH_TRSM];
+        stats->ms_cast = ms[PH_CAST];
+        stats->ms_schur = ms[PH_SCHUR];
+        stats->ms_total = ms[0] + ms[1] + ms[2] + ms[3];
+        stats->info = h.code == MXP_ZERO_PIVOT ? h.info0 : 0;
+        stats->schur_launches = schur_launches;
+    }
+    return rs;
+}
+
+// ---------------------------------------------------------------------------
+// refinement
+// ---------------------------------------------------------------------------
+extern "C" mxp_status mxp_otf_gemv(int n, uint64_t seed, const double *d_d, double alpha,
+                                   const double *d_x, double beta, double *d_y, mxp_workspace *ws,
+                                   void *stream) {
+    if (!ws) return fail(MXP_INVALID_ARG, "otf_gemv: workspace is NULL");
+    if (n > ws->n) return fail(MXP_INVALID_ARG, "otf_gemv: n larger than the workspace");
+    return launch_otf_gemv(n, seed, d_d, alpha, d_x, beta, d_y, ws->partials, ws->max_splits,
+                           as_stream(stream));
+}
+
+extern "C" mxp_status mxp_lu_solve(int n, const float *d_LU, int64_t lda, double *d_x,
+                                   mxp_workspace *ws, void *stream) {
+    if (!ws) return fail(MXP_INVALID_ARG, "lu_solve: workspace is NULL");
+    if (n > ws->n) return fail(MXP_INVALID_ARG, "lu_solve: n larger than the workspace");
+    cudaStream_t st = as_stream(stream);
+    mxp_status s = launch_lu_solve(n, d_LU, lda, d_x, ws->flags, ws->status, st);
+    if (s != MXP_OK) return s;
+    return MXP_OK;
+}
+
+extern "C" mxp_status mxp_infnorm(int n, const double *d_x, double *h_out, mxp_workspace *ws,
+                                  void *stream) {
+    if (!ws || !h_out) return fail(MXP_INVALID_ARG, "infnorm: NULL argument");
+    cudaStream_t st = as_stream(stream);
+    mxp_status s = launch_infnorm(n, d_x, ws->scal, st);
+    if (s != MXP_OK) return s;
+    MXP_CUDA(cudaMemcpyAsync(h_out, ws->scal, sizeof(double), cudaMemcpyDeviceToHost, st));
+    MXP_CUDA(cudaStreamSynchronize(st));
+    return MXP_OK;
+}
+
+static double elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    return t;
+}
+
+extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float *d_LU, int64_t lda,
+                                               const double *d_d, const double *d_rowsum,
+                                               const double *d_rhs, double *d_x, double norma,
+                                               int maxit, int method, mxp_workspace *ws,
+                                               void *stream, mxp_ir_stats *stats) {
+    if (!ws || !d_LU || !d_d || !d_rhs || !d_x) return fail(MXP_INVALID_ARG, "IR: NULL argument");
+    if (n > ws->n || lda < n) return fail(MXP_INVALID_ARG, "IR: bad n / lda");
+    if (maxit < 1) return fail(MXP_INVALID_ARG, "IR: maxit < 1");
+    if (method != MXP_IR_CLASSIC) return fail(MXP_UNSUPPORTED, "IR: GMRES refinement not built yet");
+    cudaStream_t st = as_stream(stream);
+    double *r = ws->r;
+    double *sc = ws->scal;  // [0] normx [1] normr [2] norma [3] normb
+    double *h = ws->h_scal;
+    cudaEvent_t e0, e1, g0, g1, t0, t1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&g0);
+    cudaEventCreate(&g1);
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    double ms_gemv = 0.0, ms_trsv = 0.0;
+    mxp_status s = MXP_OK;
+    auto done = [&](mxp_status res) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaEventDestroy(g0);
+        cudaEventDestroy(g1);
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        return res;
+    };
+    cudaEventRecord(e0, st);
+    MXP_CUDA(cudaMemsetAsync(ws->status, 0, sizeof(DevStatus), st));
+    if (norma <= 0.0) {
+        s = launch_norma(n, d_d, d_rowsum, sc + 2, st);
+        if (s != MXP_OK) return done(s);
+    }
+    s = launch_infnorm(n, d_rhs, sc + 3, st);
+    if (s != MXP_OK) return done(s);
+    MXP_CUDA(cudaMemcpyAsync(h + 2, sc + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    MXP_CUDA(cudaStreamSynchronize(st));
+    if (norma <= 0.0) norma = h[2];
+    const double normb = h[3];
+    s = launch_ir_init(n, d_rhs, d_d, d_x, st);
+    if (s != MXP_OK) return done(s);
+    const double eps = 0x1p-53;  // DBL_EPSILON / 2
+    int it = 0;
+    bool converged = false;
+    double normr = -1.0, hpl = -1.0, normx = 0.0;
+    int gemv_calls = 0, trsv_calls = 0;
+    for (it = 0; it < maxit; ++it) {
+        s = launch_copy(n, d_rhs, r, st);
+        if (s == MXP_OK) s = launch_infnorm(n, d_x, sc + 0, st);
+        cudaEventRecord(g0, st);
+        if (s == MXP_OK) s = launch_otf_gemv(n, seed, d_d, -1.0, d_x, 1.0, r, ws->partials, ws->max_splits, st);
+        cudaEventRecord(g1, st);
+        if (s == MXP_OK) s = launch_infnorm(n, r, sc + 1, st);
+        if (s != MXP_OK) return done(s);
+        ++gemv_calls;
+        MXP_CUDA(cudaMemcpyAsync(h, sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        MXP_CUDA(cudaStreamSynchronize(st));
+        ms_gemv += elapsed(g0, g1);
+        normx = h[0];
+        normr = h[1];
+        hpl = normr / (norma * normx + normb) * 1.0 / ((double)n * eps);
+        if (stats && it < 64) stats->history[it] = hpl;
+        if (!std::isfinite(hpl)) {
+            s = fail(MXP_NONFINITE, "IR: non-finite residual");
+            break;
+        }
+        if (hpl < 16.0) {
+            converged = true;
+            break;
+        }
+        cudaEventRecord(t0, st);
+        s = launch_lu_solve(n, d_LU, lda, r, ws->flags, ws->status, st);
+        cudaEventRecord(t1, st);
+        if (s == MXP_OK) s = launch_axpy(n, 1.0, r, d_x, st);
+        if (s != MXP_OK) return done(s);
+        ++trsv_calls;
+        MXP_CUDA(cudaStreamSynchronize(st));
+        ms_trsv += elapsed(t0, t1);
+    }
+    cudaEventRecord(e1, st);
+    mxp_status rs = read_status(ws, st);
+    if (stats) {
+        stats->iterations = it;
+        stats->converged = converged ? 1 : 0;
+        stats->residual = normr;
+        stats->hpl_harness = hpl;
+        stats->norma = norma;
+        stats->normb = normb;
+        stats->normx = normx;
+        stats->ms_total = elapsed(e0, e1);
+        stats->ms_gemv = ms_gemv;
+        stats->ms_trsv = ms_trsv;
+        stats->gemv_calls = gemv_calls;
+        stats->trsv_calls = trsv_calls;
+    }
+    if (s != MXP_OK) return done(s);
+    if (rs != MXP_OK) return done(rs);
+    if (!converged) return done(fail(MXP_NOT_CONVERGED, "IR: maxit reached without convergence"));
+    return done(MXP_OK);
+}
+
+extern "C" mxp_status mxp_solve(int n, int b, uint64_t seed, float *d_A, int64_t lda,
+                                const double *d_d, const double *d_rowsum, const double *d_rhs,
+                                double *d_x, int maxit, int method, mxp_workspace *ws,
+                                void *stream, mxp_lu_stats *lu_stats, mxp_ir_stats *ir_stats) {
+    mxp_status s = mxp_panel_lu(n, b, d_A, lda, ws, stream, lu_stats);
+    if (s != MXP_OK) return s;
+    return mxp_iterative_refinement(n, seed, d_A, lda, d_d, d_rowsum, d_rhs, d_x, 0.0, maxit, method,
+                                    ws, stream, ir_stats);
+}
+
+extern "C" mxp_status mxp_solve_host(int n, int b, uint64_t seed, float *d_A, int64_t lda,
+                                     const double *d_d, const double *d_rowsum,
+                                     const double *h_rhs, double *h_x, int maxit, int method,
+                                     mxp_workspace *ws, void *stream, mxp_lu_stats *lu_stats,
+                                     mxp_ir_stats *ir_stats) {
+    if (!ws || !h_rhs || !h_x) return fail(MXP_INVALID_ARG, "solve_host: NULL argument");
+    if (n > ws->n) return fail(MXP_INVALID_ARG, "solve_host: n larger than the workspace");
+    cudaStream_t st = as_stream(stream);
+    // rhs and x are staged in the workspace's own vector slots: no allocation
+    MXP_CUDA(cudaMemcpyAsync(ws->rhsv, h_rhs, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st));
+    mxp_status s = mxp_solve(n, b, seed, d_A, lda, d_d, d_rowsum, ws->rhsv, ws->xv, maxit, method, ws,
+                             stream, lu_stats, ir_stats);
+    if (s == MXP_OK || s == MXP_NOT_CONVERGED) {
+        cudaError_t e = cudaMemcpyAsync(h_x, ws->xv, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "solve_host: copy of x");
+    }
+    return s;
+}

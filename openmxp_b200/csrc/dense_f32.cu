@@ -1,0 +1,264 @@
+// FP32 dense kernels of the panel factorisation: the diagonal-block no-pivot
+// LU and the two panel TRSMs, blocked by 64 with a shared-memory /
+// register kernel for each 64-wide triangle and a SIMT FP32 GEMM for the
+// rank-64 updates.
+//
+// Reference: GPUSOLVER_SGETRF -> rocsolver_sgetrf_npvt / cusolverDnSgetrf
+// with ipiv = NULL (panel_trf.hpp:547-551, 678-681); GPUBLAS_STRSM
+// (R,U,N,NonUnit) for the L panel (panel_trf.hpp:188-207) and (L,L,N,Unit)
+// for the U panel (panel_trf.hpp:225-246).  The unblocked kernel follows
+// sgetrf_nopiv_naive (sgetrf_nopiv.cpp:27-61): scale the column by the
+// reciprocal pivot, then a rank-1 update.
+#include "mxp_internal.cuh"
+
+namespace mxp {
+
+namespace {
+
+constexpr int kNB = 64;  // inner block of the blocked LU / TRSM
+
+// ---- 64 x 64 no-pivot LU in shared memory ---------------------------------
+__global__ void __launch_bounds__(256)
+getrf_small_kernel(int nb, float *A, int64_t lda, DevStatus *dst, int pivot_base) {
+    __shared__ float a[kNB][kNB + 1];  // a[col][row]
+    const int t = threadIdx.x;
+    for (int idx = t; idx < nb * nb; idx += 256) {
+        const int r = idx % nb, c = idx / nb;
+        a[c][r] = A[(int64_t)c * lda + r];
+    }
+    __syncthreads();
+    for (int k = 0; k < nb; ++k) {
+        const float piv = a[k][k];
+        const bool bad = !(piv != 0.0f) || !isfinite(piv);
+        if (bad && t == 0) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
+        const float inv = 1.0f / piv;
+        if (t > k && t < nb) a[k][t] *= inv;
+        __syncthreads();
+        const int w = nb - k - 1;
+        for (int idx = t; idx < w * w; idx += 256) {
+            const int r = k + 1 + idx % w, c = k + 1 + idx / w;
+            a[c][r] -= a[k][r] * a[c][k];
+        }
+        __syncthreads();
+    }
+    for (int idx = t; idx < nb * nb; idx += 256) {
+        const int r = idx % nb, c = idx / nb;
+        A[(int64_t)c * lda + r] = a[c][r];
+    }
+}
+
+// ---- X = B * U^{-1}, U (nb x nb) upper non-unit; one thread per row -------
+__global__ void __launch_bounds__(128)
+trsm_runn_small_kernel(int m, int nb, const float *U, int64_t ldu, float *B, int64_t ldb) {
+    __shared__ float u[kNB][kNB + 1];  // u[col][row]
+    __shared__ float uinv[kNB];
+    for (int idx = threadIdx.x; idx < nb * nb; idx += 128) {
+        const int r = idx % nb, c = idx / nb;
+        u[c][r] = U[(int64_t)c * ldu + r];
+    }
+    __syncthreads();
+    if (threadIdx.x < nb) uinv[threadIdx.x] = 1.0f / u[threadIdx.x][threadIdx.x];
+    __syncthreads();
+    const int64_t i = (int64_t)blockIdx.x * 128 + threadIdx.x;
+    if (i >= m) return;
+    float x[kNB];
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) x[c] = (c < nb) ? B[(int64_t)c * ldb + i] : 0.0f;
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) {
+        if (c < nb) {
+            float v = x[c];
+#pragma unroll
+            for (int k = 0; k < c; ++k) v -= u[c][k] * x[k];
+            x[c] = v * uinv[c];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kNB; ++c)
+        if (c < nb) B[(int64_t)c * ldb + i] = x[c];
+}
+
+// ---- X = L^{-1} B, L (nb x nb) unit lower; one warp per column ------------
+__global__ void __launch_bounds__(256)
+trsm_llnu_small_kernel(int ncols, int nb, const float *L, int64_t ldl, float *B, int64_t ldb) {
+    __shared__ float l[kNB][kNB + 1];  // l[col][row]
+    for (int idx = threadIdx.x; idx < nb * nb; idx += 256) {
+        const int r = idx % nb, c = idx / nb;
+        l[c][r] = L[(int64_t)c * ldl + r];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t col0 = (int64_t)blockIdx.x * 64;
+    for (int cc = warp; cc < 64; cc += 8) {
+        const int64_t j = col0 + cc;
+        if (j >= ncols) break;
+        float *bj = B + j * ldb;
+        float x0 = (lane < nb) ? bj[lane] : 0.0f;
+        float x1 = (lane + 32 < nb) ? bj[lane + 32] : 0.0f;
+        for (int k = 0; k < nb; ++k) {
+            const float xk = __shfl_sync(0xffffffffu, k < 32 ? x0 : x1, k & 31);
+            if (lane > k) x0 -= l[k][lane] * xk;
+            if (lane + 32 > k && lane + 32 < nb) x1 -= l[k][lane + 32] * xk;
+        }
+        if (lane < nb) bj[lane] = x0;
+        if (lane + 32 < nb) bj[lane + 32] = x1;
+    }
+}
+
+// ---- C -= A * B, FP32 SIMT GEMM, 128 x 128 tiles, 8 x 8 per thread --------
+constexpr int BM = 128, BN = 128, BK = 16;
+
+__global__ void __launch_bounds__(256)
+sgemm_sub_kernel(int m, int n, int k, const float *__restrict__ A, int64_t lda,
+                 const float *__restrict__ B, int64_t ldb, float *__restrict__ C, int64_t ldc) {
+    __shared__ __align__(16) float As[BK][BM];
+    __shared__ __align__(16) float Bs[BK][BN + 4];
+    const int t = threadIdx.x;
+    const int tx = t % 16, ty = t / 16;
+    const int64_t m0 = (int64_t)blockIdx.x * BM, n0 = (int64_t)blockIdx.y * BN;
+
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+
+    float ra[8], rb[8];
+    auto load_tile = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = t + 256 * q;
+            const int kk = idx / BM, r = idx % BM;
+            const int64_t gr = m0 + r;
+            const int gk = k0 + kk;
+            ra[q] = (gr < m && gk < k) ? A[(int64_t)gk * lda + gr] : 0.0f;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = t + 256 * q;
+            const int c = idx / BK, kk = idx % BK;
+            const int64_t gc = n0 + c;
+            const int gk = k0 + kk;
+            rb[q] = (gc < n && gk < k) ? B[gc * ldb + gk] : 0.0f;
+        }
+    };
+    auto store_tile = [&]() {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = t + 256 * q;
+            As[idx / BM][idx % BM] = ra[q];
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = t + 256 * q;
+            Bs[idx % BK][idx / BK] = rb[q];
+        }
+    };
+
+    load_tile(0);
+    for (int k0 = 0; k0 < k; k0 += BK) {
+        __syncthreads();
+        store_tile();
+        __syncthreads();
+        if (k0 + BK < k) load_tile(k0 + BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            const float4 a0 = *reinterpret_cast<const float4 *>(&As[kk][tx * 4]);
+            const float4 a1 = *reinterpret_cast<const float4 *>(&As[kk][64 + tx * 4]);
+            const float4 b0 = *reinterpret_cast<const float4 *>(&Bs[kk][ty * 4]);
+            const float4 b1 = *reinterpret_cast<const float4 *>(&Bs[kk][64 + ty * 4]);
+            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int64_t gc = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
+        if (gc >= n) continue;
+        float *cc = C + gc * ldc;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int64_t gr = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
+            if (gr < m) cc[gr] -= acc[i][j];
+        }
+    }
+}
+
+}  // namespace
+
+mxp_status launch_sgemm_sub(int m, int n, int k, const float *A, int64_t lda, const float *B,
+                            int64_t ldb, float *C, int64_t ldc, cudaStream_t st) {
+    if (m <= 0 || n <= 0 || k <= 0) return MXP_OK;
+    dim3 grid((unsigned)cdiv(m, BM), (unsigned)cdiv(n, BN));
+    if (grid.y > 65535) return fail(MXP_UNSUPPORTED, "sgemm_sub: n too large");
+    sgemm_sub_kernel<<<grid, 256, 0, st>>>(m, n, k, A, lda, B, ldb, C, ldc);
+    MXP_LAUNCHED();
+    return MXP_OK;
+}
+
+mxp_status launch_getrf_blocked(int n, float *A, int64_t lda, DevStatus *dst, int pivot_base,
+                                cudaStream_t st) {
+    if (n <= 0) return MXP_OK;
+    if (lda < n) return fail(MXP_INVALID_ARG, "getrf: lda < n");
+    for (int jb = 0; jb < n; jb += kNB) {
+        const int nbk = n - jb < kNB ? n - jb : kNB;
+        float *Ajj = A + jb + (int64_t)jb * lda;
+        getrf_small_kernel<<<1, 256, 0, st>>>(nbk, Ajj, lda, dst, pivot_base + jb);
+        MXP_LAUNCHED();
+        const int rem = n - jb - nbk;
+        if (rem <= 0) continue;
+        trsm_runn_small_kernel<<<(unsigned)cdiv(rem, 128), 128, 0, st>>>(rem, nbk, Ajj, lda,
+                                                                         Ajj + nbk, lda);
+        MXP_LAUNCHED();
+        trsm_llnu_small_kernel<<<(unsigned)cdiv(rem, 64), 256, 0, st>>>(
+            rem, nbk, Ajj, lda, Ajj + (int64_t)nbk * lda, lda);
+        MXP_LAUNCHED();
+        mxp_status s = launch_sgemm_sub(rem, rem, nbk, Ajj + nbk, lda, Ajj + (int64_t)nbk * lda,
+                                        lda, Ajj + nbk + (int64_t)nbk * lda, lda, st);
+        if (s != MXP_OK) return s;
+    }
+    return MXP_OK;
+}
+
+mxp_status launch_trsm_runn(int m, int n, const float *U, int64_t ldu, float *B, int64_t ldb,
+                            cudaStream_t st) {
+    if (m <= 0 || n <= 0) return MXP_OK;
+    if (ldu < n || ldb < m) return fail(MXP_INVALID_ARG, "trsm_right_upper: bad leading dimension");
+    for (int jb = 0; jb < n; jb += kNB) {
+        const int nbk = n - jb < kNB ? n - jb : kNB;
+        const float *Ujj = U + jb + (int64_t)jb * ldu;
+        float *Bj = B + (int64_t)jb * ldb;
+        trsm_runn_small_kernel<<<(unsigned)cdiv(m, 128), 128, 0, st>>>(m, nbk, Ujj, ldu, Bj, ldb);
+        MXP_LAUNCHED();
+        const int rem = n - jb - nbk;
+        if (rem <= 0) continue;
+        mxp_status s = launch_sgemm_sub(m, rem, nbk, Bj, ldb, Ujj + (int64_t)nbk * ldu, ldu,
+                                        Bj + (int64_t)nbk * ldb, ldb, st);
+        if (s != MXP_OK) return s;
+    }
+    return MXP_OK;
+}
+
+mxp_status launch_trsm_llnu(int m, int n, const float *L, int64_t ldl, float *B, int64_t ldb,
+                            cudaStream_t st) {
+    if (m <= 0 || n <= 0) return MXP_OK;
+    if (ldl < m || ldb < m) return fail(MXP_INVALID_ARG, "trsm_left_lower_unit: bad leading dimension");
+    for (int jb = 0; jb < m; jb += kNB) {
+        const int nbk = m - jb < kNB ? m - jb : kNB;
+        const float *Ljj = L + jb + (int64_t)jb * ldl;
+        trsm_llnu_small_kernel<<<(unsigned)cdiv(n, 64), 256, 0, st>>>(n, nbk, Ljj, ldl, B + jb, ldb);
+        MXP_LAUNCHED();
+        const int rem = m - jb - nbk;
+        if (rem <= 0) continue;
+        mxp_status s = launch_sgemm_sub(rem, n, nbk, Ljj + nbk, ldl, B + jb, ldb, B + jb + nbk,
+                                        ldb, st);
+        if (s != MXP_OK) return s;
+    }
+    return MXP_OK;
+}
+
+}  // namespace mxp

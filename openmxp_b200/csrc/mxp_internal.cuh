@@ -1,0 +1,164 @@
+// Internal declarations shared by the CUDA translation units of libmxp.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/mxp.h"
+
+namespace mxp {
+
+// ---------------------------------------------------------------------------
+// Status plumbing
+// ---------------------------------------------------------------------------
+void set_error(const std::string &msg);
+mxp_status fail(mxp_status st, const std::string &msg);
+mxp_status cuda_fail(cudaError_t e, const char *where);
+void count_launch(int n = 1);
+
+#define MXP_CUDA(call)                                              \
+    do {                                                            \
+        cudaError_t e_ = (call);                                    \
+        if (e_ != cudaSuccess) return ::mxp::cuda_fail(e_, #call);  \
+    } while (0)
+
+#define MXP_LAUNCHED()                                                    \
+    do {                                                                  \
+        cudaError_t e_ = cudaGetLastError();                              \
+        if (e_ != cudaSuccess) return ::mxp::cuda_fail(e_, __func__);     \
+        ::mxp::count_launch();                                            \
+    } while (0)
+
+// Device status word written by kernels (never by traps): code + two
+// integers of detail.  Lives in the workspace.
+struct DevStatus {
+    int code;   // mxp_status
+    int info0;  // e.g. global pivot index
+    int info1;  // e.g. timeout site
+    int pad;
+};
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ void report(DevStatus *st, int code, int i0, int i1) {
+    if (st && atomicCAS(&st->code, 0, code) == 0) {
+        st->info0 = i0;
+        st->info1 = i1;
+    }
+}
+
+// Bounded waits give up after this many nanoseconds of %globaltimer.
+constexpr unsigned long long kWaitTimeoutNs = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+#endif
+
+// ---------------------------------------------------------------------------
+// 64-bit LCG (hpl_rand.hpp:12-78): x <- a*x + c mod 2^64, a = 6364136223846793005.
+// ---------------------------------------------------------------------------
+struct Aff {
+    uint64_t a, c;
+};
+
+constexpr uint64_t kLcgA = 6364136223846793005ull;
+constexpr uint64_t kLcgC = 1ull;
+
+__host__ __device__ __forceinline__ Aff aff_mul(Aff f, Aff g) {  // f o g
+    return Aff{f.a * g.a, f.a * g.c + f.c};
+}
+
+__host__ __device__ __forceinline__ Aff aff_pow(Aff f, uint64_t n) {
+    Aff r{1ull, 0ull};
+    while (n) {
+        if (n & 1ull) r = aff_mul(r, f);
+        f = aff_mul(f, f);
+        n >>= 1;
+    }
+    return r;
+}
+
+__host__ __device__ __forceinline__ uint64_t aff_apply(Aff f, uint64_t x) { return f.a * x + f.c; }
+
+__host__ __device__ __forceinline__ Aff lcg_inc1() { return Aff{kLcgA, kLcgC}; }
+
+// RandStat::initialize(seed) (hpl_rand.hpp:54-57)
+__host__ __device__ __forceinline__ uint64_t lcg_stat00(uint64_t seed) {
+    return aff_apply(lcg_inc1(), seed);
+}
+
+#if defined(__CUDACC__)
+// Exact round-to-nearest int64 -> double without the 64-bit converter:
+// both 32-bit halves are exact doubles (built by the 2^52 bias trick), and
+// hi*2^32 + lo is formed by one fused multiply-add, i.e. a single rounding
+// of the exact integer.  Bitwise equal to a correctly rounded conversion.
+__device__ __forceinline__ double i64_to_double_rn(uint64_t x) {
+    const uint32_t lo = (uint32_t)x;
+    const uint32_t hi = (uint32_t)(x >> 32) ^ 0x80000000u;  // signed hi, biased by 2^31
+    const double dlo = __hiloint2double(0x43300000, (int)lo) - 4503599627370496.0;   // 2^52
+    const double dhi = __hiloint2double(0x43300000, (int)hi) - 4503601774854144.0;   // 2^52 + 2^31
+    return __fma_rn(dhi, 4294967296.0, dlo);
+}
+
+// RandStat -> double in [-0.5, 0.5] (hpl_rand.hpp:64-66)
+__device__ __forceinline__ double lcg_to_double(uint64_t x) {
+    return __dmul_rn(i64_to_double_rn(x), 0x1.fffffffffffffP-65);
+}
+#endif
+
+// ---------------------------------------------------------------------------
+// Small helpers
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+__host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Launchers implemented in the individual translation units ---------------
+mxp_status launch_matgen(int n, uint64_t seed, int diag_rule, float *A, int64_t lda, double *d,
+                         double *rowsum, double *rhs, cudaStream_t st);
+
+mxp_status launch_getrf_blocked(int n, float *A, int64_t lda, DevStatus *dst, int pivot_base,
+                                cudaStream_t st);
+mxp_status launch_trsm_runn(int m, int n, const float *U, int64_t ldu, float *B, int64_t ldb,
+                            cudaStream_t st);
+mxp_status launch_trsm_llnu(int m, int n, const float *L, int64_t ldl, float *B, int64_t ldb,
+                            cudaStream_t st);
+mxp_status launch_sgemm_sub(int m, int n, int k, const float *A, int64_t lda, const float *B,
+                            int64_t ldb, float *C, int64_t ldc, cudaStream_t st);
+
+mxp_status launch_cast_left(int form, int m, int b, const float *A, int64_t lda, void *out,
+                            int64_t ldk, uint8_t *scales, cudaStream_t st);
+mxp_status launch_cast_right(int form, int m, int b, const float *A, int64_t lda, void *out,
+                             int64_t ldk, uint8_t *scales, cudaStream_t st);
+mxp_status launch_half_left_ref(const float *C, int m, int b, int64_t plda, uint16_t *lp,
+                                int64_t lplda, cudaStream_t st);
+mxp_status launch_half_right_trans_ref(const float *C, int b, int m, int64_t plda, uint16_t *rp,
+                                       int64_t rplda, cudaStream_t st);
+
+mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ldl,
+                        const uint8_t *lsc, const void *R, int64_t ldr, const uint8_t *rsc,
+                        float *C, int64_t ldc, DevStatus *dst, cudaStream_t st);
+
+mxp_status launch_otf_gemv(int n, uint64_t seed, const double *d, double alpha, const double *x,
+                           double beta, double *y, double *partials, int max_splits,
+                           cudaStream_t st);
+mxp_status launch_lu_solve(int n, const float *LU, int64_t lda, double *x, int *flags,
+                           DevStatus *dst, cudaStream_t st);
+size_t lu_solve_flag_ints(int n);
+
+mxp_status launch_infnorm(int n, const double *x, double *out, cudaStream_t st);
+mxp_status launch_ir_init(int n, const double *rhs, const double *d, double *x, cudaStream_t st);
+mxp_status launch_copy(int n, const double *src, double *dst, cudaStream_t st);
+mxp_status launch_axpy(int n, double alpha, const double *x, double *y, cudaStream_t st);
+mxp_status launch_norma(int n, const double *d, const double *rowsum, double *out,
+                        cudaStream_t st);
+
+int num_sms();
+
+}  // namespace mxp

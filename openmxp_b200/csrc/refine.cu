@@ -1,0 +1,339 @@
+// FP64 kernels of the iterative refinement.
+//
+//  * otf_gemv: y = beta*y + alpha*A*x with a_ij regenerated from the LCG in
+//    FP64 (otf_gemv_h / otf_gemv_d / otf_gemv_diag_d, panel_gemv.hpp:13-117).
+//    The reference launches one <<<b,256>>> kernel per b x b block pair and
+//    synchronises after each; here one launch covers the matrix: each thread
+//    owns two rows (two independent LCG chains) over a column range and
+//    steps the state with J_n = INC1^n per column.  The state -> double
+//    conversion uses the exact split-integer route (no 64-bit converter),
+//    and the 2^-64 scale of RandStat::operator double is folded into x.
+//    Column splits write partial sums to the workspace and a second kernel
+//    reduces them in a fixed order, so the result is deterministic.
+//  * lu_solve: x <- U^{-1} L^{-1} x with the FP32 factors (trsvL_h /
+//    trsvU_h, panel_trsv.hpp:308-597).  One persistent launch per triangle:
+//    row blocks of 64 are claimed in order through an atomic ticket; a row
+//    block streams its part of the factor against the already-solved blocks
+//    (waiting, bounded, on per-block completion flags), then solves its 64 x
+//    64 diagonal triangle in FP64 and publishes.  Claim order guarantees every
+//    awaited block is owned by a CTA that is already running.
+//  * infnorm / vector ops (panel_norm.hpp:11-58, panel.hpp:525-623).
+#include "mxp_internal.cuh"
+
+namespace mxp {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// on-the-fly GEMV
+// ---------------------------------------------------------------------------
+constexpr int kGemvThreads = 128;
+constexpr int kGemvRowsPerThread = 2;
+constexpr int kGemvRows = kGemvThreads * kGemvRowsPerThread;  // 256 rows per CTA
+constexpr int kGemvXChunk = 1024;
+constexpr double kLcgScale = 0x1.fffffffffffffP-65;
+
+__global__ void __launch_bounds__(kGemvThreads)
+otf_gemv_kernel(int n, uint64_t s00, Aff jn, const double *__restrict__ d,
+                const double *__restrict__ x, int64_t cols_per_split, double alpha, double beta,
+                double *__restrict__ y, double *__restrict__ partials) {
+    __shared__ double xs[kGemvXChunk];
+    const int64_t r0 = (int64_t)blockIdx.x * kGemvRows + threadIdx.x;
+    const int64_t r1 = r0 + kGemvThreads;
+    const int64_t j_begin = (int64_t)blockIdx.y * cols_per_split;
+    const int64_t j_end = imin64(n, j_begin + cols_per_split);
+
+    const Aff inc1 = lcg_inc1();
+    // states of (r0, j_begin) and (r1, j_begin)
+    uint64_t s0 = aff_apply(aff_pow(inc1, (uint64_t)r0 + (uint64_t)n * (uint64_t)j_begin), s00);
+    uint64_t s1 = aff_apply(aff_pow(inc1, (uint64_t)kGemvThreads), s0);
+    double acc0 = 0.0, acc1 = 0.0;
+    for (int64_t jc = j_begin; jc < j_end; jc += kGemvXChunk) {
+        const int len = (int)imin64(kGemvXChunk, j_end - jc);
+        __syncthreads();
+        for (int q = threadIdx.x; q < len; q += kGemvThreads) xs[q] = x[jc + q] * kLcgScale;
+        __syncthreads();
+#pragma unroll 4
+        for (int q = 0; q < len; ++q) {
+            const int64_t j = jc + q;
+            const double xq = xs[q];
+            double v0 = i64_to_double_rn(s0);
+            double v1 = i64_to_double_rn(s1);
+            v0 = (j == r0) ? 0.0 : v0;
+            v1 = (j == r1) ? 0.0 : v1;
+            acc0 = __fma_rn(v0, xq, acc0);
+            acc1 = __fma_rn(v1, xq, acc1);
+            s0 = aff_apply(jn, s0);
+            s1 = aff_apply(jn, s1);
+        }
+    }
+    // diagonal entries come from d (otf_gemv_diag_d, panel_gemv.hpp:26)
+    if (r0 < n && r0 >= j_begin && r0 < j_end) acc0 += d[r0] * x[r0];
+    if (r1 < n && r1 >= j_begin && r1 < j_end) acc1 += d[r1] * x[r1];
+    if (partials) {
+        double *p = partials + (int64_t)blockIdx.y * n;
+        if (r0 < n) p[r0] = acc0;
+        if (r1 < n) p[r1] = acc1;
+    } else {
+        if (r0 < n) y[r0] = (beta == 0.0 ? 0.0 : beta * y[r0]) + alpha * acc0;
+        if (r1 < n) y[r1] = (beta == 0.0 ? 0.0 : beta * y[r1]) + alpha * acc1;
+    }
+}
+
+__global__ void gemv_reduce_kernel(int n, int splits, const double *__restrict__ partials,
+                                   double alpha, double beta, double *__restrict__ y) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double t = 0.0;
+    for (int s = 0; s < splits; ++s) t += partials[(int64_t)s * n + i];
+    y[i] = (beta == 0.0 ? 0.0 : beta * y[i]) + alpha * t;
+}
+
+// ---------------------------------------------------------------------------
+// sync-free block triangular solves
+// ---------------------------------------------------------------------------
+constexpr int kRB = 64;
+constexpr int kTrsvThreads = 256;
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(int *p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// flags[0..nrb) : block done; flags[nrb] : ticket
+template <bool LOWER>
+__global__ void __launch_bounds__(kTrsvThreads)
+trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *flags,
+            DevStatus *dst) {
+    __shared__ float tri[kRB][kRB + 1];  // tri[col][row] of the diagonal block
+    __shared__ double part[kTrsvThreads / kRB][kRB];
+    __shared__ double zs[kRB];
+    __shared__ int s_ticket;
+    const int nrb = (n + kRB - 1) / kRB;
+    const int tid = threadIdx.x;
+    if (tid == 0) s_ticket = atomicAdd(&flags[nrb], 1);
+    __syncthreads();
+    const int rb = LOWER ? s_ticket : nrb - 1 - s_ticket;
+    const int64_t row0 = (int64_t)rb * kRB;
+    const int nrows = (int)imin64(kRB, n - row0);
+    const int r = tid % kRB, cph = tid / kRB;  // 4 column phases of 16
+
+    // diagonal block into shared memory
+    for (int idx = tid; idx < kRB * kRB; idx += kTrsvThreads) {
+        const int rr = idx % kRB, cc = idx / kRB;
+        tri[cc][rr] = (rr < nrows && cc < nrows) ? LU[(row0 + cc) * lda + row0 + rr] : 0.0f;
+    }
+
+    double acc = 0.0;
+    int known = LOWER ? -1 : nrb;  // furthest block known complete
+    bool timed_out = false;
+    const int64_t grow = row0 + r;
+    const bool row_ok = r < nrows;
+    const int ncb = LOWER ? rb : nrb - 1 - rb;
+    for (int q = 0; q < ncb && !timed_out; ++q) {
+        const int cb = LOWER ? q : nrb - 1 - q;
+        const bool need = LOWER ? (cb > known) : (cb < known);
+        if (need) {
+            const int latest = LOWER ? rb - 1 : rb + 1;
+            if (ld_acquire(&flags[latest])) {
+                known = latest;
+            } else {
+                const unsigned long long t0 = globaltimer_ns();
+                uint32_t it = 0;
+                while (!ld_acquire(&flags[cb])) {
+                    if ((++it & 255u) == 0u && globaltimer_ns() - t0 > kWaitTimeoutNs) {
+                        timed_out = true;
+                        break;
+                    }
+                }
+                known = cb;
+            }
+        }
+        if (timed_out) break;
+        const int64_t c0 = (int64_t)cb * kRB + cph * 16;
+        const int clen = (int)imin64(16, n - c0);
+        if (row_ok) {
+            const float *col = LU + c0 * lda + grow;
+#pragma unroll 16
+            for (int cc = 0; cc < clen; ++cc) acc = __fma_rn((double)col[cc * lda], __ldcg(x + c0 + cc), acc);
+        }
+    }
+    if (timed_out) report(dst, MXP_TIMEOUT, 10 + (LOWER ? 0 : 1), rb);
+    part[cph][r] = acc;
+    __syncthreads();
+    if (tid < kRB) {
+        double s = part[0][tid] + part[1][tid] + part[2][tid] + part[3][tid];
+        zs[tid] = (tid < nrows) ? __ldcg(x + row0 + tid) - s : 0.0;
+    }
+    __syncthreads();
+    if (tid < 32) {
+        // 64 x 64 triangle in FP64 by one warp; lane holds rows lane, lane+32
+        double z0 = zs[tid], z1 = zs[tid + 32];
+        if (LOWER) {
+            for (int k = 0; k < nrows; ++k) {
+                const double zk = __shfl_sync(0xffffffffu, k < 32 ? z0 : z1, k & 31);
+                if (tid > k) z0 -= (double)tri[k][tid] * zk;
+                if (tid + 32 > k) z1 -= (double)tri[k][tid + 32] * zk;
+            }
+        } else {
+            for (int k = nrows - 1; k >= 0; --k) {
+                double dk = (double)tri[k][k];
+                if (k < 32) {
+                    if (tid == k) z0 = z0 / dk;
+                } else {
+                    if (tid + 32 == k) z1 = z1 / dk;
+                }
+                const double zk = __shfl_sync(0xffffffffu, k < 32 ? z0 : z1, k & 31);
+                if (tid < k) z0 -= (double)tri[k][tid] * zk;
+                if (tid + 32 < k) z1 -= (double)tri[k][tid + 32] * zk;
+            }
+        }
+        if (tid < nrows) __stcg(x + row0 + tid, z0);
+        if (tid + 32 < nrows) __stcg(x + row0 + tid + 32, z1);
+        __threadfence();
+        __syncwarp();
+        if (tid == 0) st_release(&flags[rb], 1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// norms and vector ops
+// ---------------------------------------------------------------------------
+__global__ void infnorm_kernel(int n, const double *__restrict__ x, unsigned long long *out) {
+    double m = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(x[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ double red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+        // non-negative doubles order like their bit patterns; NaN sorts high
+        atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+__global__ void norma_kernel(int n, const double *__restrict__ d, const double *__restrict__ rs,
+                             unsigned long long *out) {
+    double m = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        m = fmax(m, rs ? rs[i] + d[i] : 2.0 * d[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ double red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+        atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+__global__ void ir_init_kernel(int n, const double *__restrict__ rhs, const double *__restrict__ d,
+                               double *__restrict__ x) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = rhs[i] / d[i];
+}
+
+__global__ void copy_kernel(int n, const double *__restrict__ s, double *__restrict__ t) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) t[i] = s[i];
+}
+
+__global__ void axpy_kernel(int n, double alpha, const double *__restrict__ x, double *__restrict__ y) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] += alpha * x[i];
+}
+
+}  // namespace
+
+mxp_status launch_otf_gemv(int n, uint64_t seed, const double *d, double alpha, const double *x,
+                           double beta, double *y, double *partials, int max_splits,
+                           cudaStream_t st) {
+    if (n <= 0) return MXP_OK;
+    const int row_blocks = (int)cdiv(n, kGemvRows);
+    const int target = 4 * num_sms();
+    int splits = (target + row_blocks - 1) / row_blocks;
+    if (splits > max_splits) splits = max_splits;
+    if (!partials) splits = 1;
+    int64_t cols = cdiv(n, splits);
+    cols = cdiv(cols, 64) * 64;
+    splits = (int)cdiv(n, cols);
+    if (splits < 1) splits = 1;
+    const uint64_t s00 = lcg_stat00(seed);
+    const Aff jn = aff_pow(lcg_inc1(), (uint64_t)n);
+    dim3 grid((unsigned)row_blocks, (unsigned)splits);
+    otf_gemv_kernel<<<grid, kGemvThreads, 0, st>>>(n, s00, jn, d, x, cols, alpha, beta, y,
+                                                   splits > 1 ? partials : nullptr);
+    MXP_LAUNCHED();
+    if (splits > 1) {
+        gemv_reduce_kernel<<<(unsigned)cdiv(n, 256), 256, 0, st>>>(n, splits, partials, alpha, beta, y);
+        MXP_LAUNCHED();
+    }
+    return MXP_OK;
+}
+
+size_t lu_solve_flag_ints(int n) { return 2 * ((size_t)cdiv(n, kRB) + 1); }
+
+mxp_status launch_lu_solve(int n, const float *LU, int64_t lda, double *x, int *flags,
+                           DevStatus *dst, cudaStream_t st) {
+    if (n <= 0) return MXP_OK;
+    if (lda < n) return fail(MXP_INVALID_ARG, "lu_solve: lda < n");
+    const int nrb = (int)cdiv(n, kRB);
+    MXP_CUDA(cudaMemsetAsync(flags, 0, lu_solve_flag_ints(n) * sizeof(int), st));
+    trsv_kernel<true><<<nrb, kTrsvThreads, 0, st>>>(n, LU, lda, x, flags, dst);
+    MXP_LAUNCHED();
+    trsv_kernel<false><<<nrb, kTrsvThreads, 0, st>>>(n, LU, lda, x, flags + nrb + 1, dst);
+    MXP_LAUNCHED();
+    return MXP_OK;
+}
+
+mxp_status launch_infnorm(int n, const double *x, double *out, cudaStream_t st) {
+    MXP_CUDA(cudaMemsetAsync(out, 0, sizeof(double), st));
+    if (n <= 0) return MXP_OK;
+    const int blocks = (int)imin64(cdiv(n, 256), 2 * num_sms());
+    infnorm_kernel<<<blocks, 256, 0, st>>>(n, x, reinterpret_cast<unsigned long long *>(out));
+    MXP_LAUNCHED();
+    return MXP_OK;
+}
+
+mxp_status launch_norma(int n, const double *d, const double *rowsum, double *out, cudaStream_t st) {
+    MXP_CUDA(cudaMemsetAsync(out, 0, sizeof(double), st));
+    if (n <= 0) return MXP_OK;
+    const int blocks = (int)imin64(cdiv(n, 256), 2 * num_sms());
+    norma_kernel<<<blocks, 256, 0, st>>>(n, d, rowsum, reinterpret_cast<unsigned long long *>(out));
+    MXP_LAUNCHED();
+    return MXP_OK;
+}
+
+mxp_status launch_ir_init(int n, const double *rhs, const double *d, double *x, cudaStream_t st) {
+    if (n <= 0) return MXP_OK;
+    ir_init_kernel<<<(unsigned)cdiv(n, 256), 256, 0, st>>>(n, rhs, d, x);
+    MXP_LAUNCHED();
+    return MXP_OK;
+}
+
+mxp_status launch_copy(int n, const double *src, double *dst, cudaStream_t st) {
+    if (n <= 0) return MXP_OK;
+    copy_kernel<<<(unsigned)cdiv(n, 256), 256, 0, st>>>(n, src, dst);
+    MXP_LAUNCHED();
+    return MXP_OK;
+}
+
+mxp_status launch_axpy(int n, double alpha, const double *x, double *y, cudaStream_t st) {
+    if (n <= 0) return MXP_OK;
+    axpy_kernel<<<(unsigned)cdiv(n, 256), 256, 0, st>>>(n, alpha, x, y);
+    MXP_LAUNCHED();
+    return MXP_OK;
+}
+
+}  // namespace mxp

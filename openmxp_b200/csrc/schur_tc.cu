@@ -1,0 +1,432 @@
+// Schur update C -= L * R^T on the 5th-generation tensor cores (tcgen05).
+//
+// Reference: the FP16 gemm_ex calls of the LU loop (GPUBLAS_SGEMM_EX with
+// OP_N, OP_T, alpha = -1, beta = 1, FP16 inputs, FP32 C and compute;
+// panel_trf.hpp:661-665, 710-715, 734-740, 828-834; rocm_device_macros.h:
+// 267-268).  The reference reaches matrix cores only through that library
+// call; this is a hand-written sm_100a kernel.
+//
+// Design (one CTA per SM, persistent over output tiles):
+//   * tile 128 (rows of L) x 256 (rows of R), K step 64 (2-byte types),
+//     4-stage shared-memory ring filled by TMA (cp.async.bulk.tensor, 128-byte
+//     swizzle, no multicast), synchronised with mbarriers;
+//   * warp 0: TMA producer; warp 1: allocates 512 TMEM columns and issues
+//     tcgen05.mma (kind::f16, M=128, N=256, K=16) from one lane, committing
+//     each stage back to the producer and each finished accumulator to the
+//     epilogue;
+//   * warps 2..9: epilogue.  Two TMEM accumulators (2 x 256 columns) let the
+//     epilogue of tile t overlap the main loop of tile t+1.  Each epilogue
+//     warp reads its 32-lane quarter of the accumulator (tcgen05.ld 32x32b),
+//     and applies C -= acc to FP32 C in place with 128-byte coalesced
+//     accesses (lanes = consecutive rows of the column-major C);
+//   * every mbarrier wait is bounded (%globaltimer); on timeout the kernel
+//     records MXP_TIMEOUT in the status word, drains, frees TMEM and returns.
+//
+// Operands are K-major (row i of the panel holds its K values contiguously),
+// as written by the panel-cast kernels.  Out-of-range rows / K columns are
+// zero-filled by TMA; C is masked in the epilogue.
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "mxp_internal.cuh"
+
+namespace mxp {
+
+namespace {
+
+constexpr int kBM = 128;
+constexpr int kBN = 256;
+constexpr int kStages = 4;
+constexpr int kStageBytesA = kBM * 128;  // 128 rows x 128 bytes of K
+constexpr int kStageBytesB = kBN * 128;
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 64 + 32 * kEpiWarps;  // 2 control warps + epilogue
+constexpr int kTmemCols = 512;
+constexpr int kSmemBytes = 1024 /*align slack*/ + kStages * (kStageBytesA + kStageBytesB) + 256;
+
+// ---- PTX wrappers ----------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false when the deadline passed or another role aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 63u) == 0u) {
+            if (*abort_flag) return false;
+            if (globaltimer_ns() - t0 > kWaitTimeoutNs) return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                           uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// 32 lanes x 32 consecutive 32-bit columns -> 32 registers per thread.
+__device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor: K-major operand tile, 128-byte swizzle,
+// 8-row core groups 1024 bytes apart (SBO), descriptor version 1 (sm_100).
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);     // start address  [0,14)
+    d |= (uint64_t)1 << 16;                        // LBO (unused with swizzle) [16,30)
+    d |= (uint64_t)(1024 >> 4) << 32;              // SBO [32,46)
+    d |= (uint64_t)1 << 46;                        // version [46,48)
+    d |= (uint64_t)2 << 61;                        // SWIZZLE_128B [61,64)
+    return d;
+}
+
+// Instruction descriptor, kind::f16: D = F32, A/B = F16 (0) or BF16 (1),
+// both K-major, M = 128, N = 256.
+__host__ __device__ constexpr uint32_t idesc_f16(uint32_t ab_fmt) {
+    return (1u << 4) | (ab_fmt << 7) | (ab_fmt << 10) | ((uint32_t)(kBN >> 3) << 17) |
+           ((uint32_t)(kBM >> 4) << 24);
+}
+
+struct TileMap {
+    int tiles_m, tiles_n, group_m;
+    __device__ __forceinline__ void get(int t, int &tm, int &tn) const {
+        const int per_group = group_m * tiles_n;
+        const int g = t / per_group;
+        const int local = t - g * per_group;
+        const int gm = min(group_m, tiles_m - g * group_m);
+        tm = g * group_m + local % gm;
+        tn = local / gm;
+    }
+};
+
+__global__ void __launch_bounds__(kThreads, 1)
+schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                    int M, int N, int K, float *__restrict__ C, int64_t ldc, uint32_t idesc,
+                    TileMap tiles, DevStatus *dst) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                                ~uintptr_t(1023));
+    uint8_t *sA = smem;
+    uint8_t *sB = smem + kStages * kStageBytesA;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sB + kStages * kStageBytesB);
+    uint64_t *full = bars;                     // [kStages]
+    uint64_t *empty = bars + kStages;          // [kStages]
+    uint64_t *tfull = bars + 2 * kStages;      // [2]
+    uint64_t *tempty = bars + 2 * kStages + 2; // [2]
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 4);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_holder + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int total_tiles = tiles.tiles_m * tiles.tiles_n;
+    const int nk = (K + 63) / 64;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(smem_u32(&tfull[a]), 1);
+            mbar_init(smem_u32(&tempty[a]), kEpiWarps);
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_holder)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_holder;
+
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
+                int tm, tn;
+                tiles.get(t, tm, tn);
+                for (int kb = 0; kb < nk; ++kb) {
+                    if (!mbar_wait(smem_u32(&empty[stage]), phase ^ 1u, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t fb = smem_u32(&full[stage]);
+                    mbar_expect_tx(fb, kStageBytesA + kStageBytesB);
+                    tma_load_2d(smem_u32(sA + stage * kStageBytesA), &tmA, kb * 64, tm * kBM, fb);
+                    tma_load_2d(smem_u32(sB + stage * kStageBytesB), &tmB, kb * 64, tn * kBN, fb);
+                    if (++stage == kStages) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                report(dst, MXP_TIMEOUT, 1, blockIdx.x);
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            uint32_t it = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x, ++it) {
+                const uint32_t acc = it & 1u, acc_phase = (it >> 1) & 1u;
+                if (!mbar_wait(smem_u32(&tempty[acc]), acc_phase ^ 1u, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d_tmem = tmem_base + acc * kBN;
+                for (int kb = 0; kb < nk; ++kb) {
+                    if (!mbar_wait(smem_u32(&full[stage]), phase, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a0 = smem_u32(sA + stage * kStageBytesA);
+                    const uint32_t b0 = smem_u32(sB + stage * kStageBytesB);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        tc_mma_f16(d_tmem, smem_desc_sw128(a0 + 32 * k), smem_desc_sw128(b0 + 32 * k),
+                                   idesc, (kb > 0 || k > 0) ? 1u : 0u);
+                    }
+                    tc_commit(smem_u32(&empty[stage]));
+                    if (++stage == kStages) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                tc_commit(smem_u32(&tfull[acc]));
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                report(dst, MXP_TIMEOUT, 2, blockIdx.x);
+            }
+        }
+    } else {
+        // ---------------- epilogue ----------------
+        const int ew = warp - 2;             // 0..7
+        const int quarter = warp & 3;        // TMEM lane quarter this warp may access
+        const int col_half = ew >> 2;        // which 128 columns of the 256
+        uint32_t it = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
+            int tm, tn;
+            tiles.get(t, tm, tn);
+            const uint32_t acc = it & 1u, acc_phase = (it >> 1) & 1u;
+            if (!mbar_wait(smem_u32(&tfull[acc]), acc_phase, abort_flag)) {
+                ok = false;
+                break;
+            }
+            __syncwarp();
+            tc_fence_after();
+            const int64_t row = (int64_t)tm * kBM + quarter * 32 + lane;
+            const bool row_ok = row < M;
+#pragma unroll 1
+            for (int c0 = col_half * 128; c0 < col_half * 128 + 128; c0 += 32) {
+                uint32_t r[32];
+                tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quarter * 32) << 16) + acc * kBN + c0, r);
+                const int64_t col0 = (int64_t)tn * kBN + c0;
+                if (row_ok) {
+                    float *cp = C + col0 * ldc + row;
+                    float cv[32];
+                    const int ncol = (int)imin64(32, (int64_t)N - col0);
+                    if (ncol >= 32) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) cv[j] = __ldcs(cp + j * ldc);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) __stcs(cp + j * ldc, cv[j] - __uint_as_float(r[j]));
+                    } else {
+                        for (int j = 0; j < ncol; ++j) cp[j * ldc] = cp[j * ldc] - __uint_as_float(r[j]);
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&tempty[acc]));
+        }
+        if (!ok && lane == 0) {
+            *abort_flag = 1;
+            report(dst, MXP_TIMEOUT, 3, blockIdx.x);
+        }
+    }
+
+    __syncthreads();
+    if (*abort_flag) {
+        // Let any TMA copy / MMA still in flight land before TMEM and shared
+        // memory are released (bounded: ~50 us).
+        if (threadIdx.x == 0) {
+            const unsigned long long t0 = globaltimer_ns();
+            while (globaltimer_ns() - t0 < 50000ull) {
+            }
+        }
+        __syncthreads();
+    }
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(kTmemCols)
+                     : "memory");
+    }
+}
+
+// ---- host side ---------------------------------------------------------------
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// 2-D K-major map: dim0 = K (contiguous), dim1 = rows; box = box_k x box_rows.
+mxp_status make_kmajor_map(CUtensorMap *map, CUtensorMapDataType dt, int esize, const void *base,
+                           int64_t K, int64_t rows, int64_t ld, int box_k, int box_rows) {
+    auto fn = get_encode_fn();
+    if (!fn) return fail(MXP_CUDA_ERROR, "cuTensorMapEncodeTiled unavailable");
+    if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0)
+        return fail(MXP_INVALID_ARG, "schur: panel base must be 16-byte aligned");
+    if ((ld * esize) % 16 != 0) return fail(MXP_INVALID_ARG, "schur: panel ld*esize must be a multiple of 16");
+    cuuint64_t gdim[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    cuuint64_t gstride[1] = {(cuuint64_t)(ld * esize)};
+    cuuint32_t box[2] = {(cuuint32_t)box_k, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, dt, 2, const_cast<void *>(base), gdim, gstride, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(MXP_CUDA_ERROR, "cuTensorMapEncodeTiled failed");
+    return MXP_OK;
+}
+
+}  // namespace
+
+mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ldl,
+                        const uint8_t *lsc, const void *R, int64_t ldr, const uint8_t *rsc,
+                        float *C, int64_t ldc, DevStatus *dst, cudaStream_t st) {
+    (void)lsc;
+    (void)rsc;
+    if (m < 0 || n < 0 || k < 0) return fail(MXP_INVALID_ARG, "schur: negative size");
+    if (m == 0 || n == 0 || k == 0) return MXP_OK;
+    if (ldc < m) return fail(MXP_INVALID_ARG, "schur: ldc < m");
+    if (form == MXP_FORM_FP8) return fail(MXP_UNSUPPORTED, "schur: FP8 form not built yet");
+    if (form != MXP_FORM_FP16 && form != MXP_FORM_BF16X2)
+        return fail(MXP_INVALID_ARG, "schur: unknown form");
+    if (m > (1 << 30) || n > (1 << 30)) return fail(MXP_INVALID_ARG, "schur: size too large");
+    const int64_t K = (form == MXP_FORM_BF16X2) ? 3 * (int64_t)k : k;
+    if (ldl < K || ldr < K) return fail(MXP_INVALID_ARG, "schur: panel ld smaller than K");
+    const CUtensorMapDataType dt =
+        form == MXP_FORM_FP16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    CUtensorMap mapA, mapB;
+    mxp_status s = make_kmajor_map(&mapA, dt, 2, L, K, m, ldl, 64, kBM);
+    if (s != MXP_OK) return s;
+    s = make_kmajor_map(&mapB, dt, 2, R, K, n, ldr, 64, kBN);
+    if (s != MXP_OK) return s;
+
+    static bool attr_done = false;
+    if (!attr_done) {
+        MXP_CUDA(cudaFuncSetAttribute(schur_tc_f16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      kSmemBytes));
+        attr_done = true;
+    }
+    TileMap tiles;
+    tiles.tiles_m = (int)cdiv(m, kBM);
+    tiles.tiles_n = (int)cdiv(n, kBN);
+    tiles.group_m = 16;
+    const int64_t total = (int64_t)tiles.tiles_m * tiles.tiles_n;
+    if (total > (int64_t)1 << 31) return fail(MXP_INVALID_ARG, "schur: too many tiles");
+    const int grid = (int)(total < num_sms() ? total : num_sms());
+    const uint32_t idesc = idesc_f16(form == MXP_FORM_FP16 ? 0u : 1u);
+    schur_tc_f16_kernel<<<grid, kThreads, kSmemBytes, st>>>(mapA, mapB, m, n, (int)K, C, ldc, idesc,
+                                                            tiles, dst);
+    MXP_LAUNCHED();
+    return MXP_OK;
+}
+
+}  // namespace mxp

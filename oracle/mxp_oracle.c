@@ -1,0 +1,732 @@
+/*
+ * mxp_oracle.c -- CPU restatement of OpenMxP's single-process solve path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA library in
+ * openmxp_b200/csrc: only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg load it.  The product path never calls into it.
+ *
+ * Parity pinning: the generator functions below are checked bit-for-bit
+ * against the reference's own hpl_rand.hpp compiled in place
+ * (oracle/build_ref.sh -> oracle/_ref/libmxpref.so) and against the committed
+ * fixtures in tests/golden/.  The LU/Schur/TRSM/IR restatements follow the
+ * reference's algorithm; the reference's numbers at that boundary come from
+ * rocBLAS/rocSOLVER, which are not part of the reference tree, so factor
+ * parity is a tolerance check (relative Frobenius) rather than bitwise.
+ *
+ * Every function cites the reference file:line it restates.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_EXPORT __attribute__((visibility("default")))
+
+/* ------------------------------------------------------------------------ */
+/* 64-bit LCG: x <- a*x + c (mod 2^64)                hpl_rand.hpp:12-78      */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    uint64_t a, c;
+} orc_aff;
+
+static const orc_aff ORC_INC1 = {6364136223846793005ULL, 1ULL}; /* hpl_rand.hpp:16 */
+
+/* f o g : x -> f.a*(g.a*x+g.c)+f.c                     hpl_rand.hpp:18-20 */
+static inline orc_aff aff_mul(orc_aff f, orc_aff g) {
+    orc_aff r;
+    r.a = f.a * g.a;
+    r.c = f.a * g.c + f.c;
+    return r;
+}
+
+/* f^n by binary powering                               hpl_rand.hpp:31-48 */
+static orc_aff aff_pow(orc_aff f, uint64_t n) {
+    orc_aff r = {1ULL, 0ULL};
+    orc_aff t = f;
+    while (n) {
+        if (n & 1ULL) r = aff_mul(r, t);
+        t = aff_mul(t, t);
+        n >>= 1;
+    }
+    return r;
+}
+
+static inline uint64_t aff_apply(orc_aff f, uint64_t x) { return f.a * x + f.c; }
+
+/* state -> double in [-0.5, 0.5]                       hpl_rand.hpp:64-73 */
+static inline double state_to_double(uint64_t x) {
+    return (double)(int64_t)x * 0x1.fffffffffffffP-65;
+}
+
+/* RandStat::initialize(seed) = INC1 * {seed}           hpl_rand.hpp:54-57 */
+static inline uint64_t stat00(uint64_t seed) { return aff_apply(ORC_INC1, seed); }
+
+/* Stream index of element (i, j) is i + n*j            hpl_rand.hpp:249-254 */
+ORC_EXPORT double orc_elem(int n, uint64_t seed, int64_t i, int64_t j) {
+    orc_aff jmp = aff_pow(ORC_INC1, (uint64_t)i + (uint64_t)n * (uint64_t)j);
+    return state_to_double(aff_apply(jmp, stat00(seed)));
+}
+
+ORC_EXPORT uint64_t orc_state(int n, uint64_t seed, int64_t i, int64_t j) {
+    orc_aff jmp = aff_pow(ORC_INC1, (uint64_t)i + (uint64_t)n * (uint64_t)j);
+    return aff_apply(jmp, stat00(seed));
+}
+
+ORC_EXPORT void orc_aff_pow(uint64_t a, uint64_t c, uint64_t n, uint64_t *out_a, uint64_t *out_c) {
+    orc_aff f = {a, c};
+    orc_aff r = aff_pow(f, n);
+    *out_a = r.a;
+    *out_c = r.c;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Matrix generation                                                         */
+/* ------------------------------------------------------------------------ */
+
+/* Diagonal rules.  0 = the reference's rule (diag = off-diagonal row sum of
+ * |a_ij|, matgen.hpp:26-62).  1 = 0.55*rowsum + 1 (weaker dominance stress
+ * form; not a reference feature). */
+enum { ORC_DIAG_ROWSUM = 0, ORC_DIAG_055_PLUS1 = 1 };
+
+/* Row sum of |a_ij| (j != i) in the pinned GPU reduction order of
+ * fill_panel_diag_dev (matgen.hpp:26-62): 512 strided partials, thread t
+ * summing columns t, t+512, ... in ascending order; tree 512 -> 4
+ * (matgen.hpp:39-57); then ((s0+s1)+s2)+s3 (matgen.hpp:61). */
+static double rowsum_gpu_order(int n, uint64_t seed, int64_t row, const orc_aff *pn_t,
+                               orc_aff j512) {
+    double part[512];
+    uint64_t s00 = stat00(seed);
+    orc_aff ri = aff_pow(ORC_INC1, (uint64_t)row);
+    uint64_t srow = aff_apply(ri, s00);
+    for (int t = 0; t < 512; ++t) {
+        double acc = 0.0;
+        if (t < n) {
+            uint64_t s = aff_apply(pn_t[t], srow); /* element (row, t) */
+            for (int64_t j = t; j < n; j += 512) {
+                if (j != row) acc += fabs(state_to_double(s));
+                s = aff_apply(j512, s);
+            }
+        }
+        part[t] = acc;
+    }
+    for (int w = 256; w >= 4; w >>= 1)
+        for (int t = 0; t < w; ++t) part[t] += part[t + w];
+    return ((part[0] + part[1]) + part[2]) + part[3];
+}
+
+/* Full N x N FP32 matrix, FP64 diagonal d, FP64 row sums, FP64 RHS.
+ *   A(i,j) = float(elem(i,j))                  matgen.hpp:67-82 (fill_panel_dev)
+ *   A(i,i) = float(d_i)                        matgen.hpp:59-63
+ *   rhs_i  = elem(i, n)  (stream column n)     matgen.hpp:419-436 -> hpl_rand.hpp:80-129
+ * Any of d / rowsum / rhs may be NULL. */
+ORC_EXPORT void orc_matgen(int n, uint64_t seed, int diag_rule, float *A, int64_t lda, double *d,
+                           double *rowsum, double *rhs) {
+    uint64_t s00 = stat00(seed);
+    orc_aff jn = aff_pow(ORC_INC1, (uint64_t)n);
+    if (A) {
+#pragma omp parallel for schedule(static)
+        for (int64_t j = 0; j < n; ++j) {
+            uint64_t s = aff_apply(aff_pow(ORC_INC1, (uint64_t)n * (uint64_t)j), s00);
+            float *col = A + j * lda;
+            for (int64_t i = 0; i < n; ++i) {
+                col[i] = (float)state_to_double(s);
+                s = aff_apply(ORC_INC1, s);
+            }
+        }
+    }
+    orc_aff pn_t[512];
+    pn_t[0].a = 1;
+    pn_t[0].c = 0;
+    for (int t = 1; t < 512; ++t) pn_t[t] = aff_mul(jn, pn_t[t - 1]);
+    orc_aff j512 = aff_pow(jn, 512);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t i = 0; i < n; ++i) {
+        double s = rowsum_gpu_order(n, seed, i, pn_t, j512);
+        double dv = (diag_rule == ORC_DIAG_055_PLUS1) ? (0.55 * s + 1.0) : s;
+        if (rowsum) rowsum[i] = s;
+        if (d) d[i] = dv;
+        if (A) A[i * lda + i] = (float)dv;
+    }
+    if (rhs) {
+        uint64_t s = aff_apply(aff_pow(ORC_INC1, (uint64_t)n * (uint64_t)n), s00);
+        for (int64_t i = 0; i < n; ++i) {
+            rhs[i] = state_to_double(s);
+            s = aff_apply(ORC_INC1, s);
+        }
+    }
+}
+
+/* One row sum in the pinned GPU order (for spot checks at large n). */
+ORC_EXPORT double orc_rowsum_row(int n, uint64_t seed, int64_t i) {
+    orc_aff jn = aff_pow(ORC_INC1, (uint64_t)n);
+    orc_aff pn_t[512];
+    pn_t[0].a = 1;
+    pn_t[0].c = 0;
+    for (int t = 1; t < 512; ++t) pn_t[t] = aff_mul(jn, pn_t[t - 1]);
+    return rowsum_gpu_order(n, seed, i, pn_t, aff_pow(jn, 512));
+}
+
+/* FP64 matrix with the FP64 generator values off the diagonal and d on it:
+ * the matrix the refinement's residual uses (otf_gemv_d regenerates a_ij in
+ * FP64, panel_gemv.hpp:49-81; the diagonal comes from d, :13-47).  Used for
+ * the FP64 forward-error oracle. */
+ORC_EXPORT void orc_matgen_f64(int n, uint64_t seed, const double *d, double *A, int64_t lda) {
+    uint64_t s00 = stat00(seed);
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < n; ++j) {
+        uint64_t s = aff_apply(aff_pow(ORC_INC1, (uint64_t)n * (uint64_t)j), s00);
+        double *col = A + j * lda;
+        for (int64_t i = 0; i < n; ++i) {
+            col[i] = (i == j) ? d[i] : state_to_double(s);
+            s = aff_apply(ORC_INC1, s);
+        }
+    }
+}
+
+/* Row sum in the reference CPU order (calc_diag, hpl_rand.hpp:200-214):
+ * one sequential sum over j ascending.  Used only to document that the CPU
+ * and GPU orders agree in FP32 and may differ in the last FP64 bit. */
+ORC_EXPORT double orc_rowsum_cpu_order(int n, uint64_t seed, int64_t i) {
+    uint64_t s = aff_apply(aff_pow(ORC_INC1, (uint64_t)i), stat00(seed));
+    orc_aff jn = aff_pow(ORC_INC1, (uint64_t)n);
+    double sum = 0.0;
+    for (int64_t j = 0; j < n; ++j) {
+        if (j != i) sum += fabs(state_to_double(s));
+        s = aff_apply(jn, s);
+    }
+    return sum;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Low-precision conversions (bit-exact restatements)                        */
+/* ------------------------------------------------------------------------ */
+static inline uint32_t f2u(float f) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return u;
+}
+static inline float u2f(uint32_t u) {
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+/* FP32 -> FP16 round-to-nearest-even, subnormals kept, overflow -> inf.
+ * Semantics of __float2half in copyCoalesced / transposeCoalesced
+ * (fp16_gpu_kernels.cpp:11-36,158-176) and of _cvtss_sh(x, 0) in
+ * fp16sim.hpp:119. */
+ORC_EXPORT uint16_t orc_f2h(float f) {
+    uint32_t x = f2u(f);
+    uint32_t sign = (x >> 16) & 0x8000u;
+    uint32_t ax = x & 0x7fffffffu;
+    if (ax > 0x7f800000u) return (uint16_t)(sign | 0x7e00u | ((ax >> 13) & 0x3ffu));
+    if (ax == 0x7f800000u) return (uint16_t)(sign | 0x7c00u);
+    int e = (int)(ax >> 23) - 127 + 15;
+    if (e >= 1) {
+        uint32_t m = ax & 0x7fffffu;
+        uint32_t h = ((uint32_t)e << 10) | (m >> 13);
+        uint32_t rem = m & 0x1fffu;
+        if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) h += 1u;
+        if (h >= 0x7c00u) h = 0x7c00u; /* overflow (also e >= 31) */
+        return (uint16_t)(sign | h);
+    }
+    /* half subnormal or zero */
+    int shift = 14 - e;
+    if (shift > 40) return (uint16_t)sign;
+    uint64_t mm = (uint64_t)((ax & 0x7fffffu) | ((ax >> 23) ? 0x800000u : 0u));
+    uint64_t h = mm >> shift;
+    uint64_t rem = mm & ((1ULL << shift) - 1ULL);
+    uint64_t half = 1ULL << (shift - 1);
+    if (rem > half || (rem == half && (h & 1ULL))) h += 1ULL;
+    return (uint16_t)(sign | (uint32_t)h);
+}
+
+ORC_EXPORT float orc_h2f(uint16_t h) {
+    uint32_t sign = ((uint32_t)h & 0x8000u) << 16;
+    uint32_t e = (h >> 10) & 0x1fu;
+    uint32_t m = h & 0x3ffu;
+    if (e == 0) {
+        float v = (float)m * 0x1p-24f;
+        return sign ? -v : v;
+    }
+    if (e == 31) return u2f(sign | 0x7f800000u | (m << 13));
+    return u2f(sign | ((e - 15 + 127) << 23) | (m << 13));
+}
+
+/* FP32 -> BF16 round-to-nearest-even (split hi+lo form). */
+ORC_EXPORT uint16_t orc_f2bf(float f) {
+    uint32_t x = f2u(f);
+    if ((x & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((x >> 16) | 0x40u);
+    uint32_t r = x + 0x7fffu + ((x >> 16) & 1u);
+    return (uint16_t)(r >> 16);
+}
+ORC_EXPORT float orc_bf2f(uint16_t b) { return u2f((uint32_t)b << 16); }
+
+/* FP32 -> FP8 E4M3 (OCP "fn": bias 7, max 448, no inf), round to nearest
+ * even, saturating to +-448 (satfinite); NaN -> 0x7f. */
+ORC_EXPORT uint8_t orc_f2e4m3(float f) {
+    uint32_t x = f2u(f);
+    uint8_t sign = (uint8_t)((x >> 24) & 0x80u);
+    uint32_t ax = x & 0x7fffffffu;
+    if (ax > 0x7f800000u) return 0x7f;
+    float a = u2f(ax);
+    if (a > 448.0f) return (uint8_t)(sign | 0x7e);
+    int E = (int)(ax >> 23) - 127;
+    if (E >= -6) {
+        /* normal: 3 mantissa bits */
+        uint32_t m = (ax & 0x7fffffu) | 0x800000u; /* 24-bit significand */
+        uint32_t q = m >> 20;                       /* 4 bits: 1.xxx */
+        uint32_t rem = m & 0xfffffu;
+        if (rem > 0x80000u || (rem == 0x80000u && (q & 1u))) q += 1u;
+        if (q == 16u) {
+            q = 8u;
+            E += 1;
+        }
+        if (E > 8 || (E == 8 && q > 14u)) return (uint8_t)(sign | 0x7e);
+        return (uint8_t)(sign | (uint8_t)(((uint32_t)(E + 7) << 3) | (q - 8u)));
+    }
+    /* subnormal: value = q * 2^-9, q in [0, 8] */
+    double v = (double)a * 512.0; /* exact */
+    double fl = floor(v);
+    double rem = v - fl;
+    uint32_t q = (uint32_t)fl;
+    if (rem > 0.5 || (rem == 0.5 && (q & 1u))) q += 1u;
+    return (uint8_t)(sign | (uint8_t)q); /* q == 8 encodes 2^-6 (e=1,m=0) */
+}
+
+ORC_EXPORT float orc_e4m32f(uint8_t b) {
+    uint32_t sign = (b & 0x80u) ? 1u : 0u;
+    uint32_t e = (b >> 3) & 0xfu;
+    uint32_t m = b & 0x7u;
+    float v;
+    if (e == 15 && m == 7) return u2f(0x7fc00000u);
+    if (e == 0)
+        v = (float)m * 0x1p-9f;
+    else
+        v = ldexpf(1.0f + (float)m / 8.0f, (int)e - 7);
+    return sign ? -v : v;
+}
+
+/* Per-tile power-of-two scale exponent for E4M3: the largest e with
+ * amax * 2^e <= 448.  amax == 0 (or non-finite) -> 0. */
+ORC_EXPORT int orc_e4m3_scale_exp(float amax) {
+    if (!(amax > 0.0f) || !(amax < 3.0e38f)) return 0;
+    int ea = (int)((f2u(amax) >> 23) & 0xffu) - 127;
+    if (ea < -126) ea = -126; /* subnormal amax: treat as 2^-126 range */
+    int e = 8 - ea;
+    if (ldexpf(amax, e) > 448.0f) e -= 1;
+    if (e > 126) e = 126;
+    if (e < -126) e = -126;
+    return e;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Dense kernels of the LU                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Unblocked right-looking no-pivot LU, FP32 (sgetrf_nopiv.cpp:27-61). */
+ORC_EXPORT int orc_getrf_nopiv(int m, int n, float *a, int64_t lda) {
+    int kend = n < m ? n : m;
+    for (int k = 0; k < kend; ++k) {
+        float piv = a[k + lda * k];
+        if (piv == 0.0f || !isfinite(piv)) return k + 1;
+        float inv = 1.0f / piv;
+        for (int i = k + 1; i < m; ++i) a[i + lda * k] *= inv;
+        for (int j = k + 1; j < n; ++j) {
+            float akj = a[k + lda * j];
+            float *aj = a + lda * j;
+            const float *ak = a + lda * k;
+            for (int i = k + 1; i < m; ++i) aj[i] -= ak[i] * akj;
+        }
+    }
+    return 0;
+}
+
+/* B <- B * U^{-1}, U upper non-unit (STRSM R/U/N/N, panel_trf.hpp:188-207;
+ * getrf_nopiv.hpp:13-16).  BLAS reference order: column j gets the
+ * contributions of columns k<j, then is scaled by 1/U(j,j). */
+ORC_EXPORT void orc_trsm_runn(int m, int n, const float *u, int64_t ldu, float *b, int64_t ldb) {
+#pragma omp parallel for schedule(static)
+    for (int i0 = 0; i0 < m; i0 += 256) {
+        int i1 = i0 + 256 < m ? i0 + 256 : m;
+        for (int j = 0; j < n; ++j) {
+            float *bj = b + ldb * j;
+            for (int k = 0; k < j; ++k) {
+                float ukj = u[k + ldu * j];
+                const float *bk = b + ldb * k;
+                for (int i = i0; i < i1; ++i) bj[i] -= ukj * bk[i];
+            }
+            float t = 1.0f / u[j + ldu * j];
+            for (int i = i0; i < i1; ++i) bj[i] *= t;
+        }
+    }
+}
+
+/* B <- L^{-1} B, L unit lower (STRSM L/L/N/U, panel_trf.hpp:225-246;
+ * getrf_nopiv.hpp:21-24). */
+ORC_EXPORT void orc_trsm_llnu(int m, int n, const float *l, int64_t ldl, float *b, int64_t ldb) {
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < n; ++j) {
+        float *bj = b + ldb * j;
+        for (int k = 0; k < m; ++k) {
+            float bkj = bj[k];
+            const float *lk = l + ldl * k;
+            for (int i = k + 1; i < m; ++i) bj[i] -= bkj * lk[i];
+        }
+    }
+}
+
+/* C(i,j) -= sum_k Lf(i,k) * Rf(j,k) with FP32 accumulation; Lf/Rf are the
+ * dequantised panel values (column-major m x K and n x K here).  Semantics
+ * of the FP16 Schur gemm_ex (OP_N, OP_T, alpha=-1, beta=1), panel_trf.hpp:
+ * 828-834 / rocm_device_macros.h:267-268, and of shgemm (fp16sim.hpp:232-241):
+ * FP16 products are exact in FP32, only the accumulation rounds. */
+static void schur_f32(int m, int n, int K, const float *Lf, int64_t ldl, const float *Rf,
+                      int64_t ldr, float *C, int64_t ldc) {
+    const int MB = 128, NB = 64, KB = 256;
+#pragma omp parallel for collapse(2) schedule(dynamic, 1)
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        for (int i0 = 0; i0 < m; i0 += MB) {
+            int i1 = i0 + MB < m ? i0 + MB : m;
+            int j1 = j0 + NB < n ? j0 + NB : n;
+            float acc[64][128];
+            for (int j = j0; j < j1; ++j)
+                for (int i = 0; i < MB; ++i) acc[j - j0][i] = 0.0f;
+            for (int k0 = 0; k0 < K; k0 += KB) {
+                int k1 = k0 + KB < K ? k0 + KB : K;
+                for (int j = j0; j < j1; ++j) {
+                    float *aj = acc[j - j0];
+                    for (int k = k0; k < k1; ++k) {
+                        float r = Rf[j + ldr * k];
+                        const float *lk = Lf + ldl * k + i0;
+                        for (int i = 0; i < i1 - i0; ++i) aj[i] += lk[i] * r;
+                    }
+                }
+            }
+            for (int j = j0; j < j1; ++j) {
+                float *cj = C + ldc * j;
+                for (int i = i0; i < i1; ++i) cj[i] -= acc[j - j0][i - i0];
+            }
+        }
+    }
+}
+
+/* Precision forms of the Schur update. */
+enum { ORC_FORM_FP16 = 0, ORC_FORM_BF16X2 = 1, ORC_FORM_FP8 = 2, ORC_FORM_FP32 = 3 };
+
+/* Quantise an m x K FP32 block (column-major, ld) to the dequantised FP32
+ * values the tensor cores see.  out is m x Kout column-major (ld = m).
+ * FP16: RN cast (fp16_gpu_kernels.cpp:11-36).  BF16X2: hi,lo split laid out
+ * as three K segments (hi|hi|lo for the left panel, hi|lo|hi for the right),
+ * so one K'=3K product gives hi*hi + hi*lo + lo*hi.  FP8: E4M3 with a
+ * power-of-two scale per 128 x 128 tile. */
+static void quantise_panel(int form, int is_right, int m, int K, const float *src, int64_t ld,
+                           float *out) {
+    if (form == ORC_FORM_FP32) {
+        for (int k = 0; k < K; ++k)
+            for (int i = 0; i < m; ++i) out[(int64_t)k * m + i] = src[i + ld * k];
+    } else if (form == ORC_FORM_FP16) {
+#pragma omp parallel for schedule(static)
+        for (int k = 0; k < K; ++k)
+            for (int i = 0; i < m; ++i) out[(int64_t)k * m + i] = orc_h2f(orc_f2h(src[i + ld * k]));
+    } else if (form == ORC_FORM_BF16X2) {
+#pragma omp parallel for schedule(static)
+        for (int k = 0; k < K; ++k)
+            for (int i = 0; i < m; ++i) {
+                float x = src[i + ld * k];
+                float hi = orc_bf2f(orc_f2bf(x));
+                float lo = orc_bf2f(orc_f2bf(x - hi));
+                out[(int64_t)k * m + i] = hi;
+                out[(int64_t)(K + k) * m + i] = is_right ? lo : hi;
+                out[(int64_t)(2 * K + k) * m + i] = is_right ? hi : lo;
+            }
+    } else { /* FP8 */
+        int mt = (m + 127) / 128, kt = (K + 127) / 128;
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int ti = 0; ti < mt; ++ti)
+            for (int tk = 0; tk < kt; ++tk) {
+                int i0 = ti * 128, i1 = i0 + 128 < m ? i0 + 128 : m;
+                int k0 = tk * 128, k1 = k0 + 128 < K ? k0 + 128 : K;
+                float amax = 0.0f;
+                for (int k = k0; k < k1; ++k)
+                    for (int i = i0; i < i1; ++i) {
+                        float a = fabsf(src[i + ld * k]);
+                        if (a > amax) amax = a;
+                    }
+                int e = orc_e4m3_scale_exp(amax);
+                float up = ldexpf(1.0f, e), down = ldexpf(1.0f, -e);
+                for (int k = k0; k < k1; ++k)
+                    for (int i = i0; i < i1; ++i)
+                        out[(int64_t)k * m + i] = orc_e4m32f(orc_f2e4m3(src[i + ld * k] * up)) * down;
+            }
+    }
+}
+
+static int form_kmul(int form) { return form == ORC_FORM_BF16X2 ? 3 : 1; }
+
+/* Exported single Schur update on FP32 sources (quantise both panels then
+ * C -= L * R^T): L is m x K (column-major, ldl), U is K x n (the U row
+ * panel, column-major, ldu), C is m x n.  This is the oracle of
+ * mxp_panel_cast_{l,r} + mxp_schur_update for one step. */
+ORC_EXPORT void orc_schur_update(int form, int m, int n, int K, const float *L, int64_t ldl,
+                                 const float *U, int64_t ldu, float *C, int64_t ldc) {
+    int Kq = K * form_kmul(form);
+    float *Lf = (float *)malloc(sizeof(float) * (size_t)m * Kq);
+    float *Rf = (float *)malloc(sizeof(float) * (size_t)n * Kq);
+    float *Ut = (float *)malloc(sizeof(float) * (size_t)n * K);
+    for (int j = 0; j < n; ++j)
+        for (int k = 0; k < K; ++k) Ut[(int64_t)k * n + j] = U[k + ldu * j];
+    quantise_panel(form, 0, m, K, L, ldl, Lf);
+    quantise_panel(form, 1, n, K, Ut, n, Rf);
+    schur_f32(m, n, Kq, Lf, m, Rf, n, C, ldc);
+    free(Lf);
+    free(Rf);
+    free(Ut);
+}
+
+/* Blocked right-looking no-pivot LU (panel_lu_async_wGPU, panel_trf.hpp:
+ * 470-867, at a 1x1 grid).  The reference's look-ahead applies step k-1's
+ * update to panel k before the rest of the trailing matrix; every element
+ * still receives its updates in k order, which is what this loop does.
+ * Per step: getrf of the diagonal block (panel_trf.hpp:678-681), STRSM of
+ * the L column (:723, body :188-207) and the U row (:747, body :225-246),
+ * casts (:724,:748), Schur update (:825-837).  Returns 0, or 1 + the global
+ * index of the first zero / non-finite pivot. */
+ORC_EXPORT int orc_panel_lu(int n, int b, float *A, int64_t lda, int form) {
+    int nb = n / b;
+    int kmul = form_kmul(form);
+    float *Lf = NULL, *Rf = NULL, *Ut = NULL;
+    for (int k = 0; k < nb; ++k) {
+        int64_t kk = (int64_t)k * b;
+        float *Akk = A + kk + lda * kk;
+        int info = orc_getrf_nopiv(b, b, Akk, lda);
+        if (info) {
+            free(Lf);
+            free(Rf);
+            free(Ut);
+            return (int)kk + info;
+        }
+        int m = n - (int)kk - b;
+        if (m <= 0) break;
+        float *Lcol = A + (kk + b) + lda * kk;
+        float *Urow = A + kk + lda * (kk + b);
+        orc_trsm_runn(m, b, Akk, lda, Lcol, lda);
+        orc_trsm_llnu(b, m, Akk, lda, Urow, lda);
+        if (!Lf) {
+            Lf = (float *)malloc(sizeof(float) * (size_t)(n - b) * b * kmul);
+            Rf = (float *)malloc(sizeof(float) * (size_t)(n - b) * b * kmul);
+            Ut = (float *)malloc(sizeof(float) * (size_t)(n - b) * b);
+        }
+        /* U row panel transposed to m x b (the reference's R panel is U^T,
+         * fp16_gpu_kernels.cpp:158-176). */
+#pragma omp parallel for schedule(static)
+        for (int j = 0; j < m; ++j)
+            for (int q = 0; q < b; ++q) Ut[(int64_t)q * m + j] = Urow[q + lda * j];
+        quantise_panel(form, 0, m, b, Lcol, lda, Lf);
+        quantise_panel(form, 1, m, b, Ut, m, Rf);
+        schur_f32(m, m, b * kmul, Lf, m, Rf, m, A + (kk + b) + lda * (kk + b), lda);
+    }
+    free(Lf);
+    free(Rf);
+    free(Ut);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* FP64 pieces of the refinement                                             */
+/* ------------------------------------------------------------------------ */
+
+/* y = beta*y + alpha*A*x with A regenerated from the LCG in FP64 and the
+ * diagonal taken from d (otf_gemv_diag_d / otf_gemv_d, panel_gemv.hpp:
+ * 13-117; CPU otf_gemv, panel_gemv.hpp:310-338).  A is never read. */
+ORC_EXPORT void orc_otf_gemv(int n, uint64_t seed, const double *d, double alpha, const double *x,
+                             double beta, double *y) {
+    uint64_t s00 = stat00(seed);
+    orc_aff jn = aff_pow(ORC_INC1, (uint64_t)n);
+#pragma omp parallel for schedule(static, 64)
+    for (int64_t i = 0; i < n; ++i) {
+        uint64_t s = aff_apply(aff_pow(ORC_INC1, (uint64_t)i), s00);
+        double t = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            double a = (j == i) ? d[i] : state_to_double(s);
+            t += a * x[j];
+            s = aff_apply(jn, s);
+        }
+        y[i] = beta * y[i] + alpha * t;
+    }
+}
+
+/* x <- U^{-1} L^{-1} x with the FP32 factors upcast to FP64, exact
+ * substitution (the column-oriented tttrsvL / tttrsvU loops of
+ * panel_trsv.hpp:710-747 applied to the whole matrix; a block substitution
+ * with FP64 diagonal solves as in trsvL_h / trsvU_h, panel_trsv.hpp:308-597,
+ * computes the same quantity). */
+ORC_EXPORT void orc_lu_solve(int n, const float *LU, int64_t lda, double *x) {
+    for (int64_t j = 0; j + 1 < n; ++j) {
+        double xj = x[j];
+        const float *c = LU + lda * j;
+        for (int64_t i = j + 1; i < n; ++i) x[i] -= xj * (double)c[i];
+    }
+    for (int64_t j = n - 1; j >= 0; --j) {
+        const float *c = LU + lda * j;
+        x[j] /= (double)c[j];
+        double xj = x[j];
+        for (int64_t i = 0; i < j; ++i) x[i] -= xj * (double)c[i];
+    }
+}
+
+/* The reference's 1 x 1 block substitution as written (trsvL_h / trsvU_h,
+ * panel_trsv.hpp:308-597 with grid.ncol == 1): the running partial sums are
+ * sent to MPI_PROC_NULL and the wr/ws buffers swap every block column, so
+ * row block r only receives the contributions of block columns c with
+ * c == r (mod 2).  Kept to measure the effect of that behaviour; the product
+ * path uses the exact substitution above. */
+ORC_EXPORT void orc_lu_solve_ref1x1(int n, int b, const float *LU, int64_t lda, double *x) {
+    int nb = n / b;
+    double *w[2];
+    w[0] = (double *)calloc((size_t)n, sizeof(double));
+    w[1] = (double *)calloc((size_t)n, sizeof(double));
+    for (int pj = 0; pj < nb; ++pj) {
+        double *wr = w[pj & 1];
+        int64_t o = (int64_t)pj * b;
+        for (int q = 0; q < b; ++q) x[o + q] -= wr[o + q];
+        for (int q = 0; q < b; ++q) { /* unit lower solve of the block */
+            double xq = x[o + q];
+            const float *c = LU + lda * (o + q);
+            for (int i = q + 1; i < b; ++i) x[o + i] -= xq * (double)c[o + i];
+        }
+        for (int q = 0; q < b; ++q) {
+            double xq = x[o + q];
+            const float *c = LU + lda * (o + q);
+            for (int64_t i = o + b; i < n; ++i) wr[i] += (double)c[i] * xq;
+        }
+    }
+    memset(w[0], 0, sizeof(double) * (size_t)n);
+    memset(w[1], 0, sizeof(double) * (size_t)n);
+    for (int pj = nb - 1, it = 0; pj >= 0; --pj, ++it) {
+        double *wr = w[it & 1];
+        int64_t o = (int64_t)pj * b;
+        for (int q = 0; q < b; ++q) x[o + q] -= wr[o + q];
+        for (int q = b - 1; q >= 0; --q) {
+            const float *c = LU + lda * (o + q);
+            x[o + q] /= (double)c[o + q];
+            double xq = x[o + q];
+            for (int i = 0; i < q; ++i) x[o + i] -= xq * (double)c[o + i];
+        }
+        for (int q = 0; q < b; ++q) {
+            double xq = x[o + q];
+            const float *c = LU + lda * (o + q);
+            for (int64_t i = 0; i < o; ++i) wr[i] += (double)c[i] * xq;
+        }
+    }
+    free(w[0]);
+    free(w[1]);
+}
+
+ORC_EXPORT double orc_infnorm(int n, const double *x) {
+    double m = 0.0;
+    for (int i = 0; i < n; ++i) {
+        double a = fabs(x[i]);
+        m = m >= a ? m : a;
+    }
+    return m;
+}
+
+/* Classic iterative refinement, GPU branch of iterative_refinement2
+ * (iterative_refinement.hpp:141-171):
+ *   x0 = b ./ d; repeat: r = b - A x (A regenerated in FP64);
+ *   hpl = |r|inf / (|A|inf |x|inf + |b|inf) / (n eps/2); stop when < 16;
+ *   x += U^{-1} L^{-1} r.
+ * norma: 2*max(d) for the row-sum rule (hpl_infnorm, panel_norm.hpp:129-135),
+ * max(rowsum + d) otherwise.  Returns the number of corrections applied
+ * before the residual test passed (the reference's "step"), or -1 when maxit
+ * evaluations did not converge (iterative_refinement.hpp:173).  hist (may be
+ * NULL) receives the scaled residual of every evaluation. */
+ORC_EXPORT int orc_ir_classic(int n, int b, uint64_t seed, const float *LU, int64_t lda,
+                              const double *d, const double *rowsum, const double *rhs,
+                              double *x, int maxit, int ref1x1, double *out_resid,
+                              double *out_hpl, double *hist) {
+    double *r = (double *)malloc(sizeof(double) * (size_t)n);
+    double norma = 0.0;
+    for (int i = 0; i < n; ++i) {
+        double v = rowsum ? rowsum[i] + d[i] : 2.0 * d[i];
+        norma = norma >= v ? norma : v;
+    }
+    double normb = orc_infnorm(n, rhs);
+    for (int i = 0; i < n; ++i) x[i] = rhs[i] / d[i];
+    const double eps = 0x1p-53; /* DBL_EPSILON / 2 */
+    int ret = -1;
+    for (int it = 0; it < maxit; ++it) {
+        memcpy(r, rhs, sizeof(double) * (size_t)n);
+        double normx = orc_infnorm(n, x);
+        orc_otf_gemv(n, seed, d, -1.0, x, 1.0, r);
+        double normr = orc_infnorm(n, r);
+        double hpl = normr / (norma * normx + normb) * 1.0 / ((double)n * eps);
+        if (hist) hist[it] = hpl;
+        if (out_resid) *out_resid = normr;
+        if (out_hpl) *out_hpl = hpl;
+        if (hpl < 16.0) {
+            ret = it;
+            break;
+        }
+        if (ref1x1)
+            orc_lu_solve_ref1x1(n, b, LU, lda, r);
+        else
+            orc_lu_solve(n, LU, lda, r);
+        for (int i = 0; i < n; ++i) x[i] += r[i];
+    }
+    free(r);
+    return ret;
+}
+
+/* Whole solve (generation excluded from the timing as in main.cpp:617-657):
+ * matgen, LU, classic IR.  t_lu / t_ir are wall seconds.  Used as the CPU
+ * baseline and by the tests.  Returns the IR step count (>= 0), -1 when IR
+ * did not converge, -2 on a zero pivot. */
+static double wall(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+ORC_EXPORT int orc_solve(int n, int b, uint64_t seed, int diag_rule, int form, int maxit,
+                         double *x, double *out_stats /* [t_lu, t_ir, resid, hpl, iters] */) {
+    float *A = (float *)malloc(sizeof(float) * (size_t)n * n);
+    double *d = (double *)malloc(sizeof(double) * (size_t)n);
+    double *rs = (double *)malloc(sizeof(double) * (size_t)n);
+    double *rhs = (double *)malloc(sizeof(double) * (size_t)n);
+    orc_matgen(n, seed, diag_rule, A, n, d, rs, rhs);
+    double t0 = wall();
+    int info = orc_panel_lu(n, b, A, n, form);
+    double t1 = wall();
+    int ret = -1;
+    double resid = -1.0, hpl = -1.0;
+    if (info == 0)
+        ret = orc_ir_classic(n, b, seed, A, n, d, diag_rule ? rs : NULL, rhs, x, maxit, 0, &resid,
+                             &hpl, NULL);
+    double t2 = wall();
+    if (out_stats) {
+        out_stats[0] = t1 - t0;
+        out_stats[1] = t2 - t1;
+        out_stats[2] = resid;
+        out_stats[3] = hpl;
+        out_stats[4] = (double)ret;
+    }
+    free(A);
+    free(d);
+    free(rs);
+    free(rhs);
+    return info ? -2 : ret;
+}
+
+ORC_EXPORT int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

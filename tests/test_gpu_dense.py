@@ -1,0 +1,66 @@
+"""FP32 diagonal LU and panel TRSMs vs the oracle (tolerance: FP32 rounding
+of a different but equivalent summation order)."""
+import numpy as np
+import pytest
+
+from tests.gpu_util import from_np_colmajor, to_np_colmajor, rel_fro
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n,pad", [(64, 0), (200, 7), (512, 0), (1000, 24)])
+def test_getrf_nopiv(mxp, orc, torch_cuda, n, pad):
+    torch = torch_cuda
+    A, _, _, _ = orc.matgen(n, 5)
+    dA = from_np_colmajor(torch, A, ld=n + pad)
+    ws = mxp.Workspace(n, n, 0)
+    mxp.getrf_nopiv(dA, n, n + pad, ws)
+    got = to_np_colmajor(dA, n, n, n + pad)
+    ref = A.copy(order="F")
+    assert orc.lib().orc_getrf_nopiv(n, n, ref.ctypes.data, n) == 0
+    assert rel_fro(got, ref) < 1e-6
+
+
+def test_getrf_zero_pivot_reported(mxp, orc, torch_cuda):
+    torch = torch_cuda
+    n = 128
+    A, _, _, _ = orc.matgen(n, 5)
+    A[70, 70] = 0.0
+    A[70, :] = 0.0           # row 70 all zero -> pivot 70 is exactly zero
+    dA = from_np_colmajor(torch, A)
+    ws = mxp.Workspace(n, n, 0)
+    with pytest.raises(mxp.MxpError) as e:
+        mxp.getrf_nopiv(dA, n, n, ws)
+    assert e.value.status == mxp.ZERO_PIVOT
+
+
+@pytest.mark.parametrize("m,n", [(1000, 64), (333, 200), (4096, 256)])
+def test_trsm_right_upper(mxp, orc, torch_cuda, m, n):
+    torch = torch_cuda
+    U, _, _, _ = orc.matgen(n, 9)
+    assert orc.lib().orc_getrf_nopiv(n, n, U.ctypes.data, n) == 0
+    rng = np.random.default_rng(m)
+    B = rng.uniform(-0.5, 0.5, (m, n)).astype(np.float32)
+    dU = from_np_colmajor(torch, U)
+    dB = from_np_colmajor(torch, B, ld=m + 1)
+    mxp.trsm_right_upper(m, n, dU, n, dB, m + 1)
+    got = to_np_colmajor(dB, m, n, m + 1)
+    ref = np.asfortranarray(B.copy())
+    orc.lib().orc_trsm_runn(m, n, U.ctypes.data, n, ref.ctypes.data, m)
+    assert rel_fro(got, ref) < 1e-6
+
+
+@pytest.mark.parametrize("m,n", [(64, 1000), (200, 333), (256, 4096)])
+def test_trsm_left_lower_unit(mxp, orc, torch_cuda, m, n):
+    torch = torch_cuda
+    Lm, _, _, _ = orc.matgen(m, 9)
+    assert orc.lib().orc_getrf_nopiv(m, m, Lm.ctypes.data, m) == 0
+    rng = np.random.default_rng(n)
+    B = rng.uniform(-0.5, 0.5, (m, n)).astype(np.float32)
+    dL = from_np_colmajor(torch, Lm)
+    dB = from_np_colmajor(torch, B)
+    mxp.trsm_left_lower_unit(m, n, dL, m, dB, m)
+    got = to_np_colmajor(dB, m, n, m)
+    ref = np.asfortranarray(B.copy())
+    orc.lib().orc_trsm_llnu(m, n, Lm.ctypes.data, m, ref.ctypes.data, m)
+    assert rel_fro(got, ref) < 1e-6
