@@ -217,10 +217,11 @@ def cpu_baseline_sample_text(cores):
 
 def workload_config(args):
     return {"workload": (f"HPL-MxP solve N={args.n} B={args.b} seed={args.seed} "
-                         f"{args.form}-Schur + FP64 classic IR to scaled residual<16"),
+                         f"{args.form}-Schur + FP64 {args.ir} IR to scaled residual<16"),
             "n": args.n, "b": args.b, "seed": args.seed, "form": args.form,
             "diag_rule": "rowsum" if args.diag_rule == 0 else "0.55*rowsum+1",
-            "ir": "classic", "parallelism": "replicas (one independent system per GPU)",
+            "ir": args.ir, "trsm": args.trsm,
+            "parallelism": "replicas (one independent system per GPU)",
             "l2": f"inputs larger than L2 (A = {args.n * args.n * 4 / 1e9:.1f} GB per GPU)"}
 
 
@@ -242,7 +243,8 @@ def run_gpu(args):
     seed = args.seed + (rank if args.distinct_seeds else 0)
 
     p = mxp.panel_matgen(n, seed, args.diag_rule)
-    ws = mxp.Workspace(n, b, form, device=local)
+    ws = mxp.Workspace(n, b, form, device=local, trsm_tensor=(args.trsm == "tensor"))
+    method = mxp.IR_GMRES if args.ir == "gmres" else mxp.IR_CLASSIC
     x = torch.empty(n, dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream()
 
@@ -253,7 +255,7 @@ def run_gpu(args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        _, lst, ist = mxp.solve(p, b, ws, x=x, maxit=args.maxit)
+        _, lst, ist = mxp.solve(p, b, ws, x=x, maxit=args.maxit, method=method)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier(dist)
@@ -303,7 +305,7 @@ def run_gpu(args):
             torch.cuda.synchronize()
             barrier(dist)
             t0 = time.perf_counter()
-            mxp.solve_host(p, b, ws, h_rhs, h_x, maxit=args.maxit)
+            mxp.solve_host(p, b, ws, h_rhs, h_x, maxit=args.maxit, method=method)
             t1 = time.perf_counter()
             barrier(dist)
             e2e_s.append(t1 - t0)
@@ -327,7 +329,8 @@ def run_gpu(args):
             "config": workload_config(args),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": launches,
-            "ir": {"iterations": last_ir["iterations"], "hpl_harness": last_ir["hpl_harness"],
+            "ir": {"iterations": last_ir["iterations"], "inner": last_ir["inner_iterations"],
+                   "hpl_harness": last_ir["hpl_harness"],
                    "residual": last_ir["residual"], "converged": last_ir["converged"]},
             "phases_ms": {k: sum(l[k] for l in lus) / len(lus)
                           for k in ("ms_total", "ms_diag_lu", "ms_trsm", "ms_cast", "ms_schur")},
@@ -338,6 +341,66 @@ def run_gpu(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# kernel micro-benchmarks (few launches: used for ncu captures)
+# ---------------------------------------------------------------------------
+def run_micro(args):
+    import torch
+
+    import openmxp_b200 as mxp
+    torch.cuda.set_device(0)
+    form = mxp.FORMS[args.form]
+    m, b = args.n, args.b
+    kmul = 3 if form == mxp.FORM_BF16X2 else 1
+    es = 1 if form == mxp.FORM_FP8 else 2
+    ldk = -(-b * kmul // (16 // es)) * (16 // es)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    out = {"micro": args.micro, "m": m, "b": b, "form": args.form}
+    if args.micro == "schur":
+        L = (torch.randn(m * b, device="cuda", generator=g) * 1e-3).float()
+        U = (torch.randn(b * m, device="cuda", generator=g) * 0.5).float()
+        Cm = torch.randn(m * m, device="cuda", generator=g).float()
+        dt = torch.uint8 if es == 1 else torch.int16
+        Lp = torch.empty(m * ldk, dtype=dt, device="cuda")
+        Rp = torch.empty(m * ldk, dtype=dt, device="cuda")
+        nsc = (-(-m // 128)) * (-(-b // 128))
+        ls = torch.empty(nsc, dtype=torch.uint8, device="cuda")
+        rs = torch.empty(nsc, dtype=torch.uint8, device="cuda")
+        ws = mxp.Workspace(m + b, b, form)
+        mxp.panel_cast_left(form, m, b, L, m, Lp, ldk, ls if es == 1 else None)
+        mxp.panel_cast_right(form, m, b, U, b, Rp, ldk, rs if es == 1 else None)
+
+        def launch():
+            mxp.schur_update(form, m, m, b, Lp, ldk, Rp, ldk, Cm, m, ws,
+                             ls if es == 1 else None, rs if es == 1 else None)
+        flops = 2.0 * m * m * b * kmul
+    elif args.micro == "otf_gemv":
+        d = torch.full((m,), m / 4.0, dtype=torch.float64, device="cuda")
+        x = torch.randn(m, dtype=torch.float64, device="cuda", generator=g)
+        y = torch.zeros(m, dtype=torch.float64, device="cuda")
+        ws = mxp.Workspace(m, min(b, m), 0)
+
+        def launch():
+            mxp.otf_gemv(m, 7, d, -1.0, x, 1.0, y, ws)
+        flops = 2.0 * m * m
+    else:
+        raise SystemExit(f"unknown micro benchmark {args.micro}")
+    for _ in range(args.warmup):
+        launch()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        launch()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    out.update(ms_per_launch=ms, tflops=flops / (ms / 1e3) / 1e12)
+    print(json.dumps(out), flush=True)
     return 0
 
 
@@ -353,9 +416,13 @@ def parse(argv=None):
     ap.add_argument("--form", choices=["fp16", "bf16x2", "fp8"], default="fp16")
     ap.add_argument("--diag-rule", type=int, default=0)
     ap.add_argument("--maxit", type=int, default=50)
+    ap.add_argument("--ir", choices=["classic", "gmres"], default="classic")
+    ap.add_argument("--trsm", choices=["tensor", "simt"], default="tensor")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--micro", choices=["schur", "otf_gemv"], default=None,
+                    help="time one kernel alone at m=--n, k=--b (for profiler captures)")
     ap.add_argument("--distinct-seeds", action="store_true",
                     help="rank r solves seed+r instead of the same system")
     return ap.parse_args(argv)
@@ -367,6 +434,8 @@ def main(argv=None):
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":
         return run_reference(args)
+    if args.micro:
+        return run_micro(args)
     return run_gpu(args)
 
 

@@ -72,6 +72,7 @@ typedef struct {
     double norma, normb, normx;
     double ms_total, ms_gemv, ms_trsv;
     int gemv_calls, trsv_calls;
+    int inner_iterations; /* GMRES Arnoldi steps over all corrections (0 for classic) */
     double history[64];  /* scaled residual of every evaluation */
 } mxp_ir_stats;
 
@@ -87,6 +88,19 @@ const char *mxp_last_error_string(void);
  * word.  All device memory the hot calls use is allocated here, once.
  * device: CUDA ordinal the workspace lives on. */
 mxp_status mxp_workspace_create(int n, int b, int form, int device, mxp_workspace **out);
+
+/* Workspace options (no reference counterpart: execution choices of this
+ * implementation).  MXP_OPT_TRSM_TENSOR: 1 (default) solves the two panel
+ * TRSMs of each LU step as split-BF16 tensor-core products against FP32
+ * triangular inverses; 0 uses the FP32 SIMT blocked substitution. */
+typedef enum {
+    MXP_OPT_TRSM_TENSOR = 1,
+    MXP_OPT_GMRES_RESTART = 2,  /* Arnoldi steps per GMRES correction, 1..30 (default 30) */
+    MXP_OPT_GMRES_TOL_EXP = 3,  /* inner tolerance 10^-value on the preconditioned residual (default 10) */
+    MXP_OPT_MERGE_PANELS = 4    /* 1 (default): update panel k+1 with step k, factor it, then apply
+                                   panels k and k+1 to the trailing matrix in one K = 2b pass */
+} mxp_option;
+mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int value);
 mxp_status mxp_workspace_destroy(mxp_workspace *ws);
 size_t mxp_workspace_bytes(int n, int b, int form);
 
@@ -180,7 +194,10 @@ mxp_status mxp_lu_solve(int n, const float *d_LU, int64_t lda, double *d_x, mxp_
  * x0 = rhs ./ d, then refine until the scaled residual
  * ||r||inf / (norma ||x||inf + normb) / (n eps/2) < 16 or maxit.
  * norma <= 0 selects 2*max(d) (hpl_infnorm, panel_norm.hpp:129-135) or,
- * with d_rowsum != NULL, max(rowsum + d).  Blocking: returns when done. */
+ * with d_rowsum != NULL, max(rowsum + d).  method MXP_IR_CLASSIC corrects
+ * with x += U^{-1} L^{-1} r; MXP_IR_GMRES solves the correction equation
+ * with GMRES preconditioned by the LU (FP64 Arnoldi, CGS2, Givens on the GPU).
+ * Blocking: returns when done. */
 mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float *d_LU, int64_t lda,
                                     const double *d_d, const double *d_rowsum,
                                     const double *d_rhs, double *d_x, double norma, int maxit,

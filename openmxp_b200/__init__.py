@@ -46,7 +46,7 @@ class IrStats(C.Structure):
                 ("hpl_harness", C.c_double), ("norma", C.c_double), ("normb", C.c_double),
                 ("normx", C.c_double), ("ms_total", C.c_double), ("ms_gemv", C.c_double),
                 ("ms_trsv", C.c_double), ("gemv_calls", C.c_int), ("trsv_calls", C.c_int),
-                ("history", C.c_double * 64)]
+                ("inner_iterations", C.c_int), ("history", C.c_double * 64)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "history"}
@@ -64,6 +64,7 @@ _SIGS = {
     "mxp_workspace_create": (_i32, [_i32, _i32, _i32, _i32, C.POINTER(_vp)]),
     "mxp_workspace_destroy": (_i32, [_vp]),
     "mxp_workspace_bytes": (C.c_size_t, [_i32, _i32, _i32]),
+    "mxp_workspace_set_option": (_i32, [_vp, _i32, _i32]),
     "mxp_matgen": (_i32, [_i32, _u64, _i32, _vp, _i64, _vp, _vp, _vp, _vp]),
     "mxp_getrf_nopiv": (_i32, [_i32, _vp, _i64, _vp, _vp]),
     "mxp_trsm_right_upper": (_i32, [_i32, _i32, _vp, _i64, _vp, _i64, _vp]),
@@ -123,14 +124,26 @@ def _stream(stream=None) -> int:
 # ---------------------------------------------------------------------------
 # workspace (LRPanels / Workspace of the reference, panel.hpp:169-187, 321-454)
 # ---------------------------------------------------------------------------
+OPT_TRSM_TENSOR = 1
+OPT_GMRES_RESTART = 2
+OPT_GMRES_TOL_EXP = 3
+OPT_MERGE_PANELS = 4
+
+
 class Workspace:
-    def __init__(self, n: int, b: int, form: int | str = FORM_FP16, device: int = 0):
+    def __init__(self, n: int, b: int, form: int | str = FORM_FP16, device: int = 0,
+                 trsm_tensor: bool = True, merge_panels: bool = True):
         if isinstance(form, str):
             form = FORMS[form]
         self.n, self.b, self.form, self.device = n, b, form, device
         h = _vp()
         check(lib().mxp_workspace_create(n, b, form, device, C.byref(h)))
         self.handle = h
+        self.set_option(OPT_TRSM_TENSOR, int(trsm_tensor))
+        self.set_option(OPT_MERGE_PANELS, int(merge_panels))
+
+    def set_option(self, key: int, value: int) -> None:
+        check(lib().mxp_workspace_set_option(self.handle, key, value))
 
     def close(self):
         if self.handle:

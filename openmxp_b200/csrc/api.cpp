@@ -56,12 +56,32 @@ int num_sms() {
 
 using namespace mxp;
 
+namespace mxp {
+int gmres_dot_blocks(int n);
+mxp_status launch_mdot(int n, int nv, const double *V, int64_t ldv, const double *w,
+                       double *partial, double *out, int accumulate, cudaStream_t st);
+mxp_status launch_vsub(int n, int nv, const double *V, int64_t ldv, const double *h, double *w,
+                       cudaStream_t st);
+mxp_status launch_vadd(int n, int nv, const double *V, int64_t ldv, const double *c, double *y,
+                       cudaStream_t st);
+mxp_status launch_vdiv(int n, const double *src, const double *den, double *dst, cudaStream_t st);
+mxp_status launch_givens(int j, double *H, int ldh, const double *hcol, const double *hnext,
+                         double *cs, double *sn, double *g, double *resid_out, cudaStream_t st);
+mxp_status launch_backsolve(int k, const double *H, int ldh, const double *g, double *y,
+                            cudaStream_t st);
+mxp_status launch_set_g0(int m, double *g, const double *beta, cudaStream_t st);
+mxp_status launch_sqrt(const double *in, double *out, cudaStream_t st);
+}  // namespace mxp
+
 // ---------------------------------------------------------------------------
 // workspace
 // ---------------------------------------------------------------------------
 struct mxp_workspace {
     int n = 0, b = 0, form = 0, device = 0;
-    int64_t ldk = 0;         // K-major panel leading dimension (elements)
+    int64_t ldk = 0;         // K-major panel row stride (elements): two panels side by side
+    int64_t kp = 0;          // K extent of one panel (b, or 3b for BF16X2)
+    int sc_ld = 0;           // FP8 scale-table row stride (tiles): two panels side by side
+    int merge = 1;           // merged look-ahead: two panels per trailing pass
     size_t esize = 2;        // panel element size
     void *lpanel[2] = {nullptr, nullptr};
     void *rpanel[2] = {nullptr, nullptr};
@@ -73,6 +93,15 @@ struct mxp_workspace {
     double *partials = nullptr, *scal = nullptr;
     int max_splits = 16;
     int *flags = nullptr;
+    // tensor-core panel TRSM: FP32 triangular inverses and split-BF16 operands
+    int trsm_tc = 1;
+    int64_t ldk3 = 0;
+    float *tinv_u = nullptr, *tinv_l = nullptr;
+    void *split_big = nullptr, *split_u = nullptr, *split_l = nullptr;
+    // GMRES-IR: basis V ((m+1) x n), Hessenberg H ((m+1) x m), rotations, scalars
+    int gm_m = 30;
+    double gm_tol = 1e-10;
+    double *gV = nullptr, *gH = nullptr, *gsmall = nullptr, *gpart = nullptr;
     double *h_scal = nullptr;  // pinned host scalars
     std::vector<void *> allocs;
 };
@@ -84,16 +113,24 @@ static int64_t panel_ldk(int b, int form) {
     return (K + align - 1) / align * align;
 }
 
+static size_t trsm_bytes(int n, int b) {
+    const int64_t ldk3 = panel_ldk(b, MXP_FORM_BF16X2);
+    const int64_t rows = n > b ? n - b : 1;
+    return 2 * (size_t)b * b * 4 + (size_t)(rows + 2 * (int64_t)b) * ldk3 * 2 + 4096;
+}
+
 static size_t ws_layout(int n, int b, int form, size_t *panel_bytes, size_t *scale_bytes,
                         size_t *vec_doubles, size_t *flag_ints) {
     const int64_t ldk = panel_ldk(b, form);
     const int64_t esize = form == MXP_FORM_FP8 ? 1 : 2;
     const int64_t rows = n > b ? n - b : 1;
-    *panel_bytes = (size_t)(rows * ldk * esize + 1024) / 256 * 256 + 256;
-    *scale_bytes = (size_t)(cdiv(rows, 128) * cdiv(b, 128) + 256) / 256 * 256 + 256;
+    *panel_bytes = (size_t)(rows * 2 * ldk * esize + 1024) / 256 * 256 + 256;
+    *scale_bytes = (size_t)(cdiv(rows, 128) * 2 * cdiv(b, 128) + 256) / 256 * 256 + 256;
     *vec_doubles = (size_t)n * (4 + 16) + 64;
     *flag_ints = lu_solve_flag_ints(n) + 64;
-    return 4 * *panel_bytes + 4 * *scale_bytes + *vec_doubles * 8 + *flag_ints * 4 + 256;
+    *vec_doubles += (size_t)31 * n + 64 * 32 + 2 * 31 * 64 + 31 * (size_t)(2 * 148 + 2) + 1024;
+    return 2 * *panel_bytes + 2 * *scale_bytes + *vec_doubles * 8 + *flag_ints * 4 + 256 +
+           trsm_bytes(n, b);
 }
 
 extern "C" size_t mxp_workspace_bytes(int n, int b, int form) {
@@ -128,7 +165,9 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
     ws->b = b;
     ws->form = form;
     ws->device = device;
-    ws->ldk = panel_ldk(b, form);
+    ws->kp = form == MXP_FORM_BF16X2 ? 3 * (int64_t)b : b;
+    ws->ldk = 2 * panel_ldk(b, form);
+    ws->sc_ld = 2 * (int)cdiv(b, 128);
     ws->esize = form == MXP_FORM_FP8 ? 1 : 2;
     size_t pb, sb, vd, fi;
     ws_layout(n, b, form, &pb, &sb, &vd, &fi);
@@ -139,13 +178,20 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
         return p;
     };
     bool ok = true;
-    for (int i = 0; i < 2 && ok; ++i) {
-        ok = (ws->lpanel[i] = alloc(pb)) && (ws->rpanel[i] = alloc(pb)) &&
-             (ws->lscale[i] = (uint8_t *)alloc(sb)) && (ws->rscale[i] = (uint8_t *)alloc(sb));
-    }
+    ok = (ws->lpanel[0] = alloc(pb)) && (ws->rpanel[0] = alloc(pb)) &&
+         (ws->lscale[0] = (uint8_t *)alloc(sb)) && (ws->rscale[0] = (uint8_t *)alloc(sb));
     ok = ok && (ws->status = (DevStatus *)alloc(sizeof(DevStatus) * 4));
     ok = ok && (ws->vec = (double *)alloc(vd * sizeof(double)));
     ok = ok && (ws->flags = (int *)alloc(fi * sizeof(int)));
+    ws->ldk3 = panel_ldk(b, MXP_FORM_BF16X2);
+    {
+        const int64_t rows = n > b ? n - b : 1;
+        ok = ok && (ws->tinv_u = (float *)alloc((size_t)b * b * 4));
+        ok = ok && (ws->tinv_l = (float *)alloc((size_t)b * b * 4));
+        ok = ok && (ws->split_big = alloc((size_t)rows * ws->ldk3 * 2 + 1024));
+        ok = ok && (ws->split_u = alloc((size_t)b * ws->ldk3 * 2 + 1024));
+        ok = ok && (ws->split_l = alloc((size_t)b * ws->ldk3 * 2 + 1024));
+    }
     if (ok) ok = cudaMallocHost(&ws->h_scal, 64 * sizeof(double)) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
@@ -159,12 +205,38 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
     ws->rhsv = ws->vec + 3 * (size_t)n;
     ws->partials = ws->vec + 4 * (size_t)n;
     ws->scal = ws->vec + 20 * (size_t)n;
+    ws->gV = ws->vec + 20 * (size_t)n + 64;
+    ws->gH = ws->gV + 31 * (size_t)n;             // 31 x 30 (ldh 31), padded to 64*32
+    ws->gsmall = ws->gH + 64 * 32;                 // cs, sn, g, y, hcol, hcol2, scalars
+    ws->gpart = ws->gsmall + 2 * 31 * 64;          // dot partials
     cudaMemset(ws->status, 0, sizeof(DevStatus) * 4);
     cudaMemset(ws->flags, 0, fi * sizeof(int));
     cudaDeviceSynchronize();
     cudaSetDevice(cur);
     *out = ws;
     return MXP_OK;
+}
+
+extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int value) {
+    if (!ws) return fail(MXP_INVALID_ARG, "set_option: workspace is NULL");
+    switch (key) {
+        case MXP_OPT_TRSM_TENSOR:
+            ws->trsm_tc = value ? 1 : 0;
+            return MXP_OK;
+        case MXP_OPT_MERGE_PANELS:
+            ws->merge = value ? 1 : 0;
+            return MXP_OK;
+        case MXP_OPT_GMRES_RESTART:
+            if (value < 1 || value > 30) return fail(MXP_INVALID_ARG, "set_option: GMRES restart must be 1..30");
+            ws->gm_m = value;
+            return MXP_OK;
+        case MXP_OPT_GMRES_TOL_EXP:
+            if (value < 1 || value > 15) return fail(MXP_INVALID_ARG, "set_option: GMRES tolerance exponent must be 1..15");
+            ws->gm_tol = std::pow(10.0, -value);
+            return MXP_OK;
+        default:
+            return fail(MXP_INVALID_ARG, "set_option: unknown key");
+    }
 }
 
 // Read and clear the device status word; synchronises the stream.
@@ -289,30 +361,92 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
     pt.st = st;
     int schur_launches = 0;
     mxp_status s = MXP_OK;
-    for (int k = 0; k < nb && s == MXP_OK; ++k) {
-        const int64_t kk = (int64_t)k * b;
+    const int64_t ldk = ws->ldk, kp = ws->kp;
+    const size_t es = ws->esize;
+    uint8_t *Lb = (uint8_t *)ws->lpanel[0], *Rb = (uint8_t *)ws->rpanel[0];
+    uint8_t *Ls = ws->lscale[0], *Rs = ws->rscale[0];
+    const int scl = ws->sc_ld;
+    const bool fp8 = form == MXP_FORM_FP8;
+    // merged schedule needs FP8 scale tiles aligned to the block size
+    const bool merge = ws->merge && (!fp8 || b % 128 == 0);
+    auto schur = [&](int64_t mrows, int64_t ncols, int kfac, int64_t lrow, int64_t rrow, float *C,
+                     int store) -> mxp_status {
+        ++schur_launches;
+        return launch_schur(form, (int)mrows, (int)ncols, b * kfac, Lb + lrow * ldk * es, ldk,
+                            fp8 ? Ls + (lrow / 128) * scl : nullptr, Rb + rrow * ldk * es, ldk,
+                            fp8 ? Rs + (rrow / 128) * scl : nullptr, C, lda, ws->status, st, store,
+                            scl, scl);
+    };
+    // Factor the diagonal block of step kk, solve its two panels, and cast them
+    // into panel slot `slot` (0 or 1) of the buffers at buffer row `row0`.
+    auto factor_panel = [&](int64_t kk, int slot, int64_t row0) -> mxp_status {
         float *Akk = d_A + kk + kk * lda;
         pt.mark(PH_DIAG);
-        s = launch_getrf_blocked(b, Akk, lda, ws->status, (int)kk, st);
-        if (s != MXP_OK) break;
+        mxp_status q = launch_getrf_blocked(b, Akk, lda, ws->status, (int)kk, st);
         const int m = n - (int)kk - b;
-        if (m <= 0) break;
+        if (q != MXP_OK || m <= 0) return q;
         float *Lcol = Akk + b;
         float *Urow = Akk + (int64_t)b * lda;
         pt.mark(PH_TRSM);
-        s = launch_trsm_runn(m, b, Akk, lda, Lcol, lda, st);
-        if (s == MXP_OK) s = launch_trsm_llnu(b, m, Akk, lda, Urow, lda, st);
-        if (s != MXP_OK) break;
-        const int buf = k & 1;
+        if (ws->trsm_tc) {
+            // X_L = A21 * U11^{-1} and X_U = L11^{-1} * A12 as split-BF16 (hi*hi + hi*lo +
+            // lo*hi) tensor-core products against FP32 triangular inverses; the same
+            // TRSM-by-inverse idea as the reference's -alt path (panel_trf_gdirect.hpp:73-142)
+            // at near-FP32 accuracy instead of FP16.
+            const int bf = MXP_FORM_BF16X2;
+            q = launch_tri_inv_upper(b, Akk, lda, ws->tinv_u, b, st);
+            if (q == MXP_OK) q = launch_tri_inv_lower_unit(b, Akk, lda, ws->tinv_l, b, st);
+            if (q == MXP_OK) q = launch_cast_left(bf, m, b, Lcol, lda, ws->split_big, ws->ldk3, nullptr, st);
+            if (q == MXP_OK) q = launch_cast_right(bf, b, b, ws->tinv_u, b, ws->split_u, ws->ldk3, nullptr, st);
+            if (q == MXP_OK)
+                q = launch_schur(bf, m, b, b, ws->split_big, ws->ldk3, nullptr, ws->split_u, ws->ldk3,
+                                 nullptr, Lcol, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/1);
+            if (q == MXP_OK) q = launch_cast_left(bf, b, b, ws->tinv_l, b, ws->split_l, ws->ldk3, nullptr, st);
+            if (q == MXP_OK) q = launch_cast_right(bf, m, b, Urow, lda, ws->split_big, ws->ldk3, nullptr, st);
+            if (q == MXP_OK)
+                q = launch_schur(bf, b, m, b, ws->split_l, ws->ldk3, nullptr, ws->split_big, ws->ldk3,
+                                 nullptr, Urow, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/2);
+        } else {
+            q = launch_trsm_runn(m, b, Akk, lda, Lcol, lda, st);
+            if (q == MXP_OK) q = launch_trsm_llnu(b, m, Akk, lda, Urow, lda, st);
+        }
+        if (q != MXP_OK) return q;
         pt.mark(PH_CAST);
-        s = launch_cast_left(form, m, b, Lcol, lda, ws->lpanel[buf], ws->ldk, ws->lscale[buf], st);
-        if (s == MXP_OK)
-            s = launch_cast_right(form, m, b, Urow, lda, ws->rpanel[buf], ws->ldk, ws->rscale[buf], st);
+        const int64_t koff = slot * kp;
+        const int64_t soff = slot * (int64_t)cdiv(b, 128);
+        q = launch_cast_left(form, m, b, Lcol, lda, Lb + (row0 * ldk + koff) * es, ldk,
+                             fp8 ? Ls + (row0 / 128) * scl + soff : nullptr, st, scl);
+        if (q == MXP_OK)
+            q = launch_cast_right(form, m, b, Urow, lda, Rb + (row0 * ldk + koff) * es, ldk,
+                                  fp8 ? Rs + (row0 / 128) * scl + soff : nullptr, st, scl);
+        return q;
+    };
+
+    int k = 0;
+    while (k < nb && s == MXP_OK) {
+        const int64_t kk = (int64_t)k * b;
+        const int64_t base = kk + b;            // global row of buffer row 0
+        const int64_t m = n - base;
+        s = factor_panel(kk, 0, 0);
+        if (s != MXP_OK || m <= 0) break;
+        if (!merge || m == b) {
+            // one panel per trailing pass (the reference's step structure)
+            pt.mark(PH_SCHUR);
+            s = schur(m, m, 1, 0, 0, d_A + base + base * lda, 0);
+            ++k;
+            continue;
+        }
+        // merged look-ahead: bring panel k+1 up to date with step k, factor it,
+        // then apply both panels to the rest of the trailing matrix in one pass.
+        pt.mark(PH_SCHUR);
+        s = schur(m, b, 1, 0, 0, d_A + base + base * lda, 0);                     // column block k+1
+        if (s == MXP_OK) s = schur(b, m - b, 1, 0, b, d_A + base + (base + b) * lda, 0);  // row block k+1
+        if (s != MXP_OK) break;
+        s = factor_panel(base, 1, b);
         if (s != MXP_OK) break;
         pt.mark(PH_SCHUR);
-        s = launch_schur(form, m, m, b, ws->lpanel[buf], ws->ldk, ws->lscale[buf], ws->rpanel[buf],
-                         ws->ldk, ws->rscale[buf], Akk + b + (int64_t)b * lda, lda, ws->status, st);
-        ++schur_launches;
+        s = schur(m - b, m - b, 2, b, b, d_A + (base + b) + (base + b) * lda, 0);
+        k += 2;
     }
     pt.mark(PH_END);
     if (s != MXP_OK) {
@@ -374,6 +508,85 @@ static double elapsed(cudaEvent_t a, cudaEvent_t b) {
     return t;
 }
 
+// Correction d = (approx) A^{-1} r by GMRES on M^{-1} A d = M^{-1} r, M = LU,
+// zero initial guess, at most ws->gm_m Arnoldi steps, stop when the
+// preconditioned residual estimate |g_{k}| <= gm_tol * beta.  r is
+// overwritten by d.  Host reads one scalar per Arnoldi step.
+static mxp_status gmres_correction(int n, uint64_t seed, const float *LU, int64_t lda, const double *dd,
+                                   double *r, mxp_workspace *ws, cudaStream_t st, int *inner_iters,
+                                   double *ms_gemv, double *ms_trsv) {
+    const int m = ws->gm_m;
+    const int ldh = 31;
+    double *V = ws->gV, *H = ws->gH;
+    double *cs = ws->gsmall, *sn = cs + 31, *g = sn + 31, *y = g + 32, *hcol = y + 31, *hcol2 = hcol + 31;
+    double *sc = hcol2 + 31;  // [0] dot scratch [1] beta [2] hnext [3] resid
+    double *w = ws->w;
+    double *h = ws->h_scal + 8;
+    mxp_status s;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    auto timed = [&](double *acc, auto &&fn) -> mxp_status {
+        cudaEventRecord(a, st);
+        mxp_status q = fn();
+        cudaEventRecord(b, st);
+        cudaEventSynchronize(b);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        *acc += t;
+        return q;
+    };
+    // z = M^{-1} r -> V_0 after normalisation
+    s = launch_copy(n, r, V, st);
+    if (s == MXP_OK) s = timed(ms_trsv, [&] { return launch_lu_solve(n, LU, lda, V, ws->flags, ws->status, st); });
+    if (s == MXP_OK) s = launch_mdot(n, 1, V, n, V, ws->gpart, sc + 0, 0, st);
+    if (s == MXP_OK) s = launch_sqrt(sc + 0, sc + 1, st);
+    if (s == MXP_OK) s = launch_vdiv(n, V, sc + 1, V, st);
+    if (s == MXP_OK) s = launch_set_g0(m, g, sc + 1, st);
+    if (s != MXP_OK) goto out;
+    {
+        MXP_CUDA(cudaMemcpyAsync(h, sc + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+        MXP_CUDA(cudaStreamSynchronize(st));
+        const double beta = h[0];
+        int k = 0;
+        if (!(beta > 0.0) || !std::isfinite(beta)) {
+            MXP_CUDA(cudaMemsetAsync(r, 0, (size_t)n * sizeof(double), st));
+            goto out;
+        }
+        for (int j = 0; j < m; ++j) {
+            double *vj = V + (int64_t)j * n;
+            s = timed(ms_gemv, [&] { return launch_otf_gemv(n, seed, dd, 1.0, vj, 0.0, w, ws->partials, ws->max_splits, st); });
+            if (s == MXP_OK) s = timed(ms_trsv, [&] { return launch_lu_solve(n, LU, lda, w, ws->flags, ws->status, st); });
+            // classical Gram-Schmidt, twice
+            if (s == MXP_OK) s = launch_mdot(n, j + 1, V, n, w, ws->gpart, hcol, 0, st);
+            if (s == MXP_OK) s = launch_vsub(n, j + 1, V, n, hcol, w, st);
+            if (s == MXP_OK) s = launch_mdot(n, j + 1, V, n, w, ws->gpart, hcol2, 0, st);
+            if (s == MXP_OK) s = launch_vsub(n, j + 1, V, n, hcol2, w, st);
+            if (s == MXP_OK) s = launch_axpy(j + 1, 1.0, hcol2, hcol, st);
+            if (s == MXP_OK) s = launch_mdot(n, 1, w, n, w, ws->gpart, sc + 0, 0, st);
+            if (s == MXP_OK) s = launch_sqrt(sc + 0, sc + 2, st);
+            if (s == MXP_OK) s = launch_givens(j, H, ldh, hcol, sc + 2, cs, sn, g, sc + 3, st);
+            if (s == MXP_OK) s = launch_vdiv(n, w, sc + 2, V + (int64_t)(j + 1) * n, st);
+            if (s != MXP_OK) goto out;
+            MXP_CUDA(cudaMemcpyAsync(h + 1, sc + 3, sizeof(double), cudaMemcpyDeviceToHost, st));
+            MXP_CUDA(cudaStreamSynchronize(st));
+            k = j + 1;
+            if (!(h[1] > ws->gm_tol * beta)) break;
+        }
+        *inner_iters += k;
+        s = launch_backsolve(k, H, ldh, g, y, st);
+        if (s == MXP_OK) {
+            cudaError_t e = cudaMemsetAsync(r, 0, (size_t)n * sizeof(double), st);
+            if (e != cudaSuccess) s = cuda_fail(e, "gmres: memset");
+        }
+        if (s == MXP_OK) s = launch_vadd(n, k, V, n, y, r, st);
+    }
+out:
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return s;
+}
+
 extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float *d_LU, int64_t lda,
                                                const double *d_d, const double *d_rowsum,
                                                const double *d_rhs, double *d_x, double norma,
@@ -382,7 +595,7 @@ extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float
     if (!ws || !d_LU || !d_d || !d_rhs || !d_x) return fail(MXP_INVALID_ARG, "IR: NULL argument");
     if (n > ws->n || lda < n) return fail(MXP_INVALID_ARG, "IR: bad n / lda");
     if (maxit < 1) return fail(MXP_INVALID_ARG, "IR: maxit < 1");
-    if (method != MXP_IR_CLASSIC) return fail(MXP_UNSUPPORTED, "IR: GMRES refinement not built yet");
+    if (method != MXP_IR_CLASSIC && method != MXP_IR_GMRES) return fail(MXP_INVALID_ARG, "IR: unknown method");
     cudaStream_t st = as_stream(stream);
     double *r = ws->r;
     double *sc = ws->scal;  // [0] normx [1] normr [2] norma [3] normb
@@ -423,7 +636,7 @@ extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float
     int it = 0;
     bool converged = false;
     double normr = -1.0, hpl = -1.0, normx = 0.0;
-    int gemv_calls = 0, trsv_calls = 0;
+    int gemv_calls = 0, trsv_calls = 0, inner = 0;
     for (it = 0; it < maxit; ++it) {
         s = launch_copy(n, d_rhs, r, st);
         if (s == MXP_OK) s = launch_infnorm(n, d_x, sc + 0, st);
@@ -448,14 +661,26 @@ extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float
             converged = true;
             break;
         }
-        cudaEventRecord(t0, st);
-        s = launch_lu_solve(n, d_LU, lda, r, ws->flags, ws->status, st);
-        cudaEventRecord(t1, st);
-        if (s == MXP_OK) s = launch_axpy(n, 1.0, r, d_x, st);
-        if (s != MXP_OK) return done(s);
-        ++trsv_calls;
-        MXP_CUDA(cudaStreamSynchronize(st));
-        ms_trsv += elapsed(t0, t1);
+        if (method == MXP_IR_GMRES) {
+            double mg = 0.0, mt = 0.0;
+            const int before = inner;
+            s = gmres_correction(n, seed, d_LU, lda, d_d, r, ws, st, &inner, &mg, &mt);
+            ms_gemv += mg;
+            ms_trsv += mt;
+            gemv_calls += inner - before;
+            trsv_calls += inner - before + 1;
+            if (s == MXP_OK) s = launch_axpy(n, 1.0, r, d_x, st);
+            if (s != MXP_OK) return done(s);
+        } else {
+            cudaEventRecord(t0, st);
+            s = launch_lu_solve(n, d_LU, lda, r, ws->flags, ws->status, st);
+            cudaEventRecord(t1, st);
+            if (s == MXP_OK) s = launch_axpy(n, 1.0, r, d_x, st);
+            if (s != MXP_OK) return done(s);
+            ++trsv_calls;
+            MXP_CUDA(cudaStreamSynchronize(st));
+            ms_trsv += elapsed(t0, t1);
+        }
     }
     cudaEventRecord(e1, st);
     mxp_status rs = read_status(ws, st);
@@ -472,6 +697,7 @@ extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float
         stats->ms_trsv = ms_trsv;
         stats->gemv_calls = gemv_calls;
         stats->trsv_calls = trsv_calls;
+        stats->inner_iterations = inner;
     }
     if (s != MXP_OK) return done(s);
     if (rs != MXP_OK) return done(rs);

@@ -127,7 +127,7 @@ constexpr int kF8Tile = 128;
 // L panel, FP8: one CTA per 128 (rows) x 128 (k) tile.
 __global__ void __launch_bounds__(kCastThreads)
 cast_left_fp8_kernel(int m, int b, const float *__restrict__ A, int64_t lda, uint8_t *out,
-                     int64_t ldk, uint8_t *scales) {
+                     int64_t ldk, uint8_t *scales, int sc_ld) {
     __shared__ uint32_t tile[kF8Tile][kF8Tile / 4 + 1];
     __shared__ float red[kCastThreads / 32];
     const int i0 = blockIdx.x * kF8Tile, k0 = blockIdx.y * kF8Tile;
@@ -152,7 +152,7 @@ cast_left_fp8_kernel(int m, int b, const float *__restrict__ A, int64_t lda, uin
         for (int r = 0; r < 4; ++r) w |= (uint32_t)to_e4m3(__fmul_rn(v[q + r], up)) << (8 * r);
         tile[ii][(kh * 64 + q) / 4] = w;
     }
-    if (t == 0) scales[(int64_t)blockIdx.x * gridDim.y + blockIdx.y] = (uint8_t)(127 - e);
+    if (t == 0) scales[(int64_t)blockIdx.x * sc_ld + blockIdx.y] = (uint8_t)(127 - e);
     __syncthreads();
     // write out: row ri = t / 2, 64 bytes (16 words) per thread
     const int ri = t / 2, half = t % 2;
@@ -180,7 +180,7 @@ cast_left_fp8_kernel(int m, int b, const float *__restrict__ A, int64_t lda, uin
 // R panel (U^T rows), FP8: one CTA per 128 (rows j) x 128 (k) tile.
 __global__ void __launch_bounds__(kCastThreads)
 cast_right_fp8_kernel(int m, int b, const float *__restrict__ A, int64_t lda, uint8_t *out,
-                      int64_t ldk, uint8_t *scales) {
+                      int64_t ldk, uint8_t *scales, int sc_ld) {
     __shared__ float red[kCastThreads / 32];
     const int j0 = blockIdx.x * kF8Tile, k0 = blockIdx.y * kF8Tile;
     const int t = threadIdx.x;
@@ -198,7 +198,7 @@ cast_right_fp8_kernel(int m, int b, const float *__restrict__ A, int64_t lda, ui
     amax = block_max_256(amax, red);
     const int e = e4m3_scale_exp(amax);
     const float up = __int_as_float((e + 127) << 23);
-    if (t == 0) scales[(int64_t)blockIdx.x * gridDim.y + blockIdx.y] = (uint8_t)(127 - e);
+    if (t == 0) scales[(int64_t)blockIdx.x * sc_ld + blockIdx.y] = (uint8_t)(127 - e);
     if (j >= m) return;
     uint8_t *dst = out + j * ldk + k0 + half * 64;
     const int kvalid = min(64, b - (k0 + half * 64));
@@ -267,7 +267,7 @@ static mxp_status check_cast_args(int form, int m, int b, int64_t lda, int64_t l
 }
 
 mxp_status launch_cast_left(int form, int m, int b, const float *A, int64_t lda, void *out,
-                            int64_t ldk, uint8_t *scales, cudaStream_t st) {
+                            int64_t ldk, uint8_t *scales, cudaStream_t st, int sc_ld) {
     mxp_status s = check_cast_args(form, m, b, lda, ldk);
     if (s != MXP_OK) return s;
     if (m == 0) return MXP_OK;
@@ -275,7 +275,7 @@ mxp_status launch_cast_left(int form, int m, int b, const float *A, int64_t lda,
         if (!scales) return fail(MXP_INVALID_ARG, "FP8 cast needs a scale buffer");
         dim3 grid((unsigned)cdiv(m, kF8Tile), (unsigned)cdiv(b, kF8Tile));
         cast_left_fp8_kernel<<<grid, kCastThreads, 0, st>>>(m, b, A, lda, (uint8_t *)out, ldk,
-                                                            scales);
+                                                            scales, sc_ld > 0 ? sc_ld : (int)grid.y);
     } else {
         dim3 grid((unsigned)cdiv(m, kTile), (unsigned)cdiv(b, kTile));
         if (form == MXP_FORM_FP16)
@@ -288,7 +288,7 @@ mxp_status launch_cast_left(int form, int m, int b, const float *A, int64_t lda,
 }
 
 mxp_status launch_cast_right(int form, int m, int b, const float *A, int64_t lda, void *out,
-                             int64_t ldk, uint8_t *scales, cudaStream_t st) {
+                             int64_t ldk, uint8_t *scales, cudaStream_t st, int sc_ld) {
     mxp_status s = check_cast_args(form, m, b, lda, ldk);
     if (s != MXP_OK) return s;
     if (m == 0) return MXP_OK;
@@ -296,7 +296,7 @@ mxp_status launch_cast_right(int form, int m, int b, const float *A, int64_t lda
         if (!scales) return fail(MXP_INVALID_ARG, "FP8 cast needs a scale buffer");
         dim3 grid((unsigned)cdiv(m, kF8Tile), (unsigned)cdiv(b, kF8Tile));
         cast_right_fp8_kernel<<<grid, kCastThreads, 0, st>>>(m, b, A, lda, (uint8_t *)out, ldk,
-                                                             scales);
+                                                             scales, sc_ld > 0 ? sc_ld : (int)grid.y);
     } else {
         const int64_t threads = (int64_t)m * ((b + 7) / 8);
         const unsigned blocks = (unsigned)cdiv(threads, kCastThreads);

@@ -17,33 +17,42 @@ namespace {
 
 constexpr int kNB = 64;  // inner block of the blocked LU / TRSM
 
-// ---- 64 x 64 no-pivot LU in shared memory ---------------------------------
-__global__ void __launch_bounds__(256)
+// ---- 64 x 64 no-pivot LU, one row per thread in registers -----------------
+// Step k: the owner of row k publishes it to shared memory; every row below
+// scales its column-k entry by the reciprocal pivot and applies the rank-1
+// update (sgetrf_nopiv_naive order, sgetrf_nopiv.cpp:27-61).  One barrier
+// per step.
+__global__ void __launch_bounds__(kNB)
 getrf_small_kernel(int nb, float *A, int64_t lda, DevStatus *dst, int pivot_base) {
-    __shared__ float a[kNB][kNB + 1];  // a[col][row]
-    const int t = threadIdx.x;
-    for (int idx = t; idx < nb * nb; idx += 256) {
-        const int r = idx % nb, c = idx / nb;
-        a[c][r] = A[(int64_t)c * lda + r];
-    }
-    __syncthreads();
-    for (int k = 0; k < nb; ++k) {
-        const float piv = a[k][k];
-        const bool bad = !(piv != 0.0f) || !isfinite(piv);
-        if (bad && t == 0) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
-        const float inv = 1.0f / piv;
-        if (t > k && t < nb) a[k][t] *= inv;
-        __syncthreads();
-        const int w = nb - k - 1;
-        for (int idx = t; idx < w * w; idx += 256) {
-            const int r = k + 1 + idx % w, c = k + 1 + idx / w;
-            a[c][r] -= a[k][r] * a[c][k];
+    __shared__ float prow[2][kNB];
+    const int i = threadIdx.x;
+    float a[kNB];
+#pragma unroll
+    for (int j = 0; j < kNB; ++j) a[j] = (i < nb && j < nb) ? A[(int64_t)j * lda + i] : 0.0f;
+#pragma unroll
+    for (int k = 0; k < kNB; ++k) {
+        if (k < nb) {
+            if (i == k) {
+#pragma unroll
+                for (int j = 0; j < kNB; ++j)
+                    if (j >= k) prow[k & 1][j] = a[j];
+            }
+            __syncthreads();
+            const float piv = prow[k & 1][k];
+            if (i == k && (!(piv != 0.0f) || !isfinite(piv))) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
+            if (i > k && i < nb) {
+                const float l = a[k] * (1.0f / piv);
+                a[k] = l;
+#pragma unroll
+                for (int j = 0; j < kNB; ++j)
+                    if (j > k) a[j] -= l * prow[k & 1][j];
+            }
         }
-        __syncthreads();
     }
-    for (int idx = t; idx < nb * nb; idx += 256) {
-        const int r = idx % nb, c = idx / nb;
-        A[(int64_t)c * lda + r] = a[c][r];
+    if (i < nb) {
+#pragma unroll
+        for (int j = 0; j < kNB; ++j)
+            if (j < nb) A[(int64_t)j * lda + i] = a[j];
     }
 }
 
@@ -188,7 +197,59 @@ sgemm_sub_kernel(int m, int n, int k, const float *__restrict__ A, int64_t lda,
     }
 }
 
+__global__ void set_identity_kernel(int n, float *X, int64_t ldx) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t j = blockIdx.y;
+    if (i < n) X[j * ldx + i] = (i == j) ? 1.0f : 0.0f;
+}
+
 }  // namespace
+
+// X = U^{-1} for an n x n upper non-unit triangle (the TRSM of the identity,
+// X * U = I, as the reference's -alt 1 path builds its inverse with STRSM on
+// an identity, panel_trf_gdirect.hpp:73-92).  Blocked by 64 with the row
+// range restricted to the non-zero part of X, so the cost is n^3/3.
+mxp_status launch_tri_inv_upper(int n, const float *U, int64_t ldu, float *X, int64_t ldx,
+                                cudaStream_t st) {
+    if (n <= 0) return MXP_OK;
+    set_identity_kernel<<<dim3((unsigned)cdiv(n, 256), (unsigned)n), 256, 0, st>>>(n, X, ldx);
+    MXP_LAUNCHED();
+    for (int jb = 0; jb < n; jb += kNB) {
+        const int nbk = n - jb < kNB ? n - jb : kNB;
+        const int rows = jb + nbk;  // X(:, jb:jb+nbk) is zero below row jb+nbk
+        const float *Ujj = U + jb + (int64_t)jb * ldu;
+        float *Xj = X + (int64_t)jb * ldx;
+        trsm_runn_small_kernel<<<(unsigned)cdiv(rows, 128), 128, 0, st>>>(rows, nbk, Ujj, ldu, Xj, ldx);
+        MXP_LAUNCHED();
+        const int rem = n - jb - nbk;
+        if (rem <= 0) continue;
+        mxp_status s = launch_sgemm_sub(rows, rem, nbk, Xj, ldx, Ujj + (int64_t)nbk * ldu, ldu,
+                                        Xj + (int64_t)nbk * ldx, ldx, st);
+        if (s != MXP_OK) return s;
+    }
+    return MXP_OK;
+}
+
+// X = L^{-1} for an n x n unit lower triangle (L X = I), blocked by row
+// blocks with the column range restricted to the non-zero part of X.
+mxp_status launch_tri_inv_lower_unit(int n, const float *L, int64_t ldl, float *X, int64_t ldx,
+                                     cudaStream_t st) {
+    if (n <= 0) return MXP_OK;
+    set_identity_kernel<<<dim3((unsigned)cdiv(n, 256), (unsigned)n), 256, 0, st>>>(n, X, ldx);
+    MXP_LAUNCHED();
+    for (int jb = 0; jb < n; jb += kNB) {
+        const int nbk = n - jb < kNB ? n - jb : kNB;
+        const int cols = jb + nbk;  // X(jb:jb+nbk, :) is zero right of column jb+nbk
+        const float *Ljj = L + jb + (int64_t)jb * ldl;
+        trsm_llnu_small_kernel<<<(unsigned)cdiv(cols, 64), 256, 0, st>>>(cols, nbk, Ljj, ldl, X + jb, ldx);
+        MXP_LAUNCHED();
+        const int rem = n - jb - nbk;
+        if (rem <= 0) continue;
+        mxp_status s = launch_sgemm_sub(rem, cols, nbk, Ljj + nbk, ldl, X + jb, ldx, X + jb + nbk, ldx, st);
+        if (s != MXP_OK) return s;
+    }
+    return MXP_OK;
+}
 
 mxp_status launch_sgemm_sub(int m, int n, int k, const float *A, int64_t lda, const float *B,
                             int64_t ldb, float *C, int64_t ldc, cudaStream_t st) {
@@ -207,7 +268,7 @@ mxp_status launch_getrf_blocked(int n, float *A, int64_t lda, DevStatus *dst, in
     for (int jb = 0; jb < n; jb += kNB) {
         const int nbk = n - jb < kNB ? n - jb : kNB;
         float *Ajj = A + jb + (int64_t)jb * lda;
-        getrf_small_kernel<<<1, 256, 0, st>>>(nbk, Ajj, lda, dst, pivot_base + jb);
+        getrf_small_kernel<<<1, kNB, 0, st>>>(nbk, Ajj, lda, dst, pivot_base + jb);
         MXP_LAUNCHED();
         const int rem = n - jb - nbk;
         if (rem <= 0) continue;

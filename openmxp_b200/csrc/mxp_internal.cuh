@@ -129,13 +129,19 @@ mxp_status launch_trsm_runn(int m, int n, const float *U, int64_t ldu, float *B,
                             cudaStream_t st);
 mxp_status launch_trsm_llnu(int m, int n, const float *L, int64_t ldl, float *B, int64_t ldb,
                             cudaStream_t st);
+mxp_status launch_tri_inv_upper(int n, const float *U, int64_t ldu, float *X, int64_t ldx,
+                                cudaStream_t st);
+mxp_status launch_tri_inv_lower_unit(int n, const float *L, int64_t ldl, float *X, int64_t ldx,
+                                     cudaStream_t st);
 mxp_status launch_sgemm_sub(int m, int n, int k, const float *A, int64_t lda, const float *B,
                             int64_t ldb, float *C, int64_t ldc, cudaStream_t st);
 
+// sc_ld: stride (in tiles) between the scale rows of consecutive 128-row
+// tiles; <= 0 means ceil(b / 128) (a dense table).
 mxp_status launch_cast_left(int form, int m, int b, const float *A, int64_t lda, void *out,
-                            int64_t ldk, uint8_t *scales, cudaStream_t st);
+                            int64_t ldk, uint8_t *scales, cudaStream_t st, int sc_ld = 0);
 mxp_status launch_cast_right(int form, int m, int b, const float *A, int64_t lda, void *out,
-                             int64_t ldk, uint8_t *scales, cudaStream_t st);
+                             int64_t ldk, uint8_t *scales, cudaStream_t st, int sc_ld = 0);
 mxp_status launch_half_left_ref(const float *C, int m, int b, int64_t plda, uint16_t *lp,
                                 int64_t lplda, cudaStream_t st);
 mxp_status launch_half_right_trans_ref(const float *C, int b, int m, int64_t plda, uint16_t *rp,
@@ -143,7 +149,8 @@ mxp_status launch_half_right_trans_ref(const float *C, int b, int m, int64_t pld
 
 mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ldl,
                         const uint8_t *lsc, const void *R, int64_t ldr, const uint8_t *rsc,
-                        float *C, int64_t ldc, DevStatus *dst, cudaStream_t st);
+                        float *C, int64_t ldc, DevStatus *dst, cudaStream_t st, int store = 0,
+                        int lsc_ld = 0, int rsc_ld = 0, int tri_mode = 0);
 
 mxp_status launch_otf_gemv(int n, uint64_t seed, const double *d, double alpha, const double *x,
                            double beta, double *y, double *partials, int max_splits,

@@ -169,7 +169,7 @@ struct TileMap {
 __global__ void __launch_bounds__(kThreads, 1)
 schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                     int M, int N, int K, float *__restrict__ C, int64_t ldc, uint32_t idesc,
-                    TileMap tiles, DevStatus *dst) {
+                    TileMap tiles, int store, int tri_mode, int seg, DevStatus *dst) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                 ~uintptr_t(1023));
@@ -186,6 +186,14 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total_tiles = tiles.tiles_m * tiles.tiles_n;
     const int nk = (K + 63) / 64;
+    // Triangular operand (panel solves against a triangular inverse): a tile
+    // only needs the K stages, within each of the K segments of length seg,
+    // below its column (tri_mode 1) or row (tri_mode 2) extent.
+    auto needed = [&](int kb, int tm, int tn) -> bool {
+        if (tri_mode == 0) return true;
+        const int off = (kb * 64) % seg;
+        return off < (tri_mode == 1 ? (tn + 1) * kBN : (tm + 1) * kBM);
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -222,6 +230,7 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                 int tm, tn;
                 tiles.get(t, tm, tn);
                 for (int kb = 0; kb < nk; ++kb) {
+                    if (!needed(kb, tm, tn)) continue;
                     if (!mbar_wait(smem_u32(&empty[stage]), phase ^ 1u, abort_flag)) {
                         ok = false;
                         break;
@@ -249,6 +258,8 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             uint32_t it = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x, ++it) {
+                int tm, tn;
+                tiles.get(t, tm, tn);
                 const uint32_t acc = it & 1u, acc_phase = (it >> 1) & 1u;
                 if (!mbar_wait(smem_u32(&tempty[acc]), acc_phase ^ 1u, abort_flag)) {
                     ok = false;
@@ -256,7 +267,9 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                 }
                 tc_fence_after();
                 const uint32_t d_tmem = tmem_base + acc * kBN;
+                bool first = true;
                 for (int kb = 0; kb < nk; ++kb) {
+                    if (!needed(kb, tm, tn)) continue;
                     if (!mbar_wait(smem_u32(&full[stage]), phase, abort_flag)) {
                         ok = false;
                         break;
@@ -267,8 +280,9 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         tc_mma_f16(d_tmem, smem_desc_sw128(a0 + 32 * k), smem_desc_sw128(b0 + 32 * k),
-                                   idesc, (kb > 0 || k > 0) ? 1u : 0u);
+                                   idesc, (!first || k > 0) ? 1u : 0u);
                     }
+                    first = false;
                     tc_commit(smem_u32(&empty[stage]));
                     if (++stage == kStages) {
                         stage = 0;
@@ -311,13 +325,19 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                     float *cp = C + col0 * ldc + row;
                     float cv[32];
                     const int ncol = (int)imin64(32, (int64_t)N - col0);
-                    if (ncol >= 32) {
+                    if (store) {  // C = acc (panel solves)
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (j < ncol) __stcs(cp + j * ldc, __uint_as_float(r[j]));
+                    } else if (ncol >= 32) {
 #pragma unroll
                         for (int j = 0; j < 32; ++j) cv[j] = __ldcs(cp + j * ldc);
 #pragma unroll
                         for (int j = 0; j < 32; ++j) __stcs(cp + j * ldc, cv[j] - __uint_as_float(r[j]));
                     } else {
-                        for (int j = 0; j < ncol; ++j) cp[j * ldc] = cp[j * ldc] - __uint_as_float(r[j]);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (j < ncol) cp[j * ldc] = cp[j * ldc] - __uint_as_float(r[j]);
                     }
                 }
             }
@@ -335,6 +355,269 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
     if (*abort_flag) {
         // Let any TMA copy / MMA still in flight land before TMEM and shared
         // memory are released (bounded: ~50 us).
+        if (threadIdx.x == 0) {
+            const unsigned long long t0 = globaltimer_ns();
+            while (globaltimer_ns() - t0 < 50000ull) {
+            }
+        }
+        __syncthreads();
+    }
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(kTmemCols)
+                     : "memory");
+    }
+}
+
+// ---- FP8 E4M3, block-scaled (kind::mxf8f6f4.block_scale) ---------------------
+//
+// Same pipeline with 128-byte K stages (128 FP8 values).  Each 128 x 128 tile
+// of a panel carries one UE8M0 scale (2^-e, e from the tile amax); a stage of
+// K = 128 covers exactly one scale tile, so the stage's scale factors are
+// uniform per 128 rows.  Warp 0 writes them to shared memory in the MX
+// scale-factor atom layout (32 rows x 16 bytes, row r / k-block kb at byte
+// (r%32)*16 + (r/32)*4 + kb) next to the TMA tiles; the MMA lane moves them to
+// TMEM with tcgen05.cp (32x128b, replicated to the four lane quarters) and
+// issues tcgen05.mma ... kind::mxf8f6f4.block_scale, which applies the scales
+// inside the MMA.  TMEM: one 256-column accumulator (cols 0..255) plus a
+// 4-slot scale-factor ring (cols 256..319).  The epilogue copies the whole
+// accumulator to registers first and releases TMEM, so its C update overlaps
+// the next tile's main loop.
+constexpr int kF8BN = 256;
+constexpr int kF8StageA = kBM * 128;
+constexpr int kF8StageB = kF8BN * 128;
+constexpr int kF8StageSF = 2048;  // SFA 512 B + SFB 1024 B, padded
+constexpr int kF8StageBytes = kF8StageA + kF8StageB + kF8StageSF;
+constexpr int kF8Stages = 4;
+constexpr int kF8SmemBytes = 1024 + kF8Stages * kF8StageBytes + 256;
+constexpr int kF8SfCol0 = 256;
+
+__device__ __forceinline__ void tc_cp_32x128b_x4(uint32_t taddr, uint64_t sdesc) {
+    asm volatile("tcgen05.cp.cta_group::1.32x128b.warpx4 [%0], %1;" ::"r"(taddr), "l"(sdesc)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_mma_mxf8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                            uint32_t idesc, uint32_t sfa, uint32_t sfb,
+                                            uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::mxf8f6f4.block_scale [%0], %1, %2, %3, [%5], [%6], p;\n\t}" ::"r"(
+            d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(sfa), "r"(sfb)
+        : "memory");
+}
+
+// Scale-factor tile: 32 rows x 16 bytes, no swizzle; 8-row core matrices 128 B apart.
+__device__ __forceinline__ uint64_t smem_desc_sf(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)1 << 16;           // LBO: a single core matrix along K
+    d |= (uint64_t)(128 >> 4) << 32;  // SBO
+    d |= (uint64_t)1 << 46;           // version
+    return d;                         // layout type 0 = no swizzle
+}
+
+// Block-scaled instruction descriptor: A, B = E4M3, K-major, UE8M0 scales,
+// M = 128, N = 256, dense K = 32; sf_id picks the byte (k-block) of the scale words.
+__host__ __device__ constexpr uint32_t idesc_mxf8(uint32_t sf_id) {
+    return (sf_id << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(kF8BN >> 3) << 17) | (1u << 23) |
+           ((uint32_t)(kBM >> 4) << 24) | (sf_id << 29);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                    int M, int N, int K, const uint8_t *__restrict__ lsc,
+                    const uint8_t *__restrict__ rsc, int lsc_ld, int rsc_ld, float *__restrict__ C,
+                    int64_t ldc, TileMap tiles, DevStatus *dst) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                                ~uintptr_t(1023));
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kF8Stages * kF8StageBytes);
+    uint64_t *full = bars;
+    uint64_t *empty = bars + kF8Stages;
+    uint64_t *tfull = bars + 2 * kF8Stages;
+    uint64_t *tempty = bars + 2 * kF8Stages + 1;
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + 2 * kF8Stages + 2);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_holder + 1);
+    auto stA = [&](int s) { return smem + s * kF8StageBytes; };
+    auto stB = [&](int s) { return smem + s * kF8StageBytes + kF8StageA; };
+    auto stSF = [&](int s) { return smem + s * kF8StageBytes + kF8StageA + kF8StageB; };
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int total_tiles = tiles.tiles_m * tiles.tiles_n;
+    const int nk = (K + 127) / 128;
+    const int rtiles = (N + 127) / 128;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kF8Stages; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        mbar_init(smem_u32(tfull), 1);
+        mbar_init(smem_u32(tempty), kEpiWarps);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_holder)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_holder;
+
+    if (warp == 0) {
+        // ---------------- producer: scale factors (whole warp) + TMA (lane 0) ----------------
+        int stage = 0;
+        uint32_t phase = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
+            int tm, tn;
+            tiles.get(t, tm, tn);
+            for (int kb = 0; kb < nk; ++kb) {
+                int got = 1;
+                if (lane == 0) got = mbar_wait(smem_u32(&empty[stage]), phase ^ 1u, abort_flag) ? 1 : 0;
+                got = __shfl_sync(0xffffffffu, got, 0);
+                if (!got) {
+                    ok = false;
+                    break;
+                }
+                const uint32_t sa = lsc[(int64_t)tm * lsc_ld + kb];
+                const uint32_t sb0 = rsc[(int64_t)(2 * tn) * rsc_ld + kb];
+                const uint32_t sb1 = (2 * tn + 1 < rtiles) ? rsc[(int64_t)(2 * tn + 1) * rsc_ld + kb] : 127u;
+                const uint32_t wa = sa * 0x01010101u, wb0 = sb0 * 0x01010101u, wb1 = sb1 * 0x01010101u;
+                uint4 *sf = reinterpret_cast<uint4 *>(stSF(stage));
+                sf[lane] = make_uint4(wa, wa, wa, wa);             // SFA: rows 0..127
+                sf[32 + lane] = make_uint4(wb0, wb0, wb0, wb0);    // SFB atom 0: rows 0..127
+                sf[64 + lane] = make_uint4(wb1, wb1, wb1, wb1);    // SFB atom 1: rows 128..255
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                    const uint32_t fb = smem_u32(&full[stage]);
+                    mbar_expect_tx(fb, kF8StageA + kF8StageB);
+                    tma_load_2d(smem_u32(stA(stage)), &tmA, kb * 128, tm * kBM, fb);
+                    tma_load_2d(smem_u32(stB(stage)), &tmB, kb * 128, tn * kF8BN, fb);
+                }
+                if (++stage == kF8Stages) {
+                    stage = 0;
+                    phase ^= 1u;
+                }
+            }
+        }
+        if (!ok && lane == 0) {
+            *abort_flag = 1;
+            report(dst, MXP_TIMEOUT, 4, blockIdx.x);
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            uint32_t it = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x, ++it) {
+                if (!mbar_wait(smem_u32(tempty), (it & 1u) ^ 1u, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                for (int kb = 0; kb < nk; ++kb) {
+                    if (!mbar_wait(smem_u32(&full[stage]), phase, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sfa_t = tmem_base + kF8SfCol0 + 16u * stage;
+                    const uint32_t sfb_t = sfa_t + 4u;
+                    const uint32_t sf0 = smem_u32(stSF(stage));
+                    tc_cp_32x128b_x4(sfa_t, smem_desc_sf(sf0));
+                    tc_cp_32x128b_x4(sfb_t, smem_desc_sf(sf0 + 512));
+                    tc_cp_32x128b_x4(sfb_t + 4u, smem_desc_sf(sf0 + 1024));
+                    const uint32_t a0 = smem_u32(stA(stage));
+                    const uint32_t b0 = smem_u32(stB(stage));
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        tc_mma_mxf8(tmem_base, smem_desc_sw128(a0 + 32 * k), smem_desc_sw128(b0 + 32 * k),
+                                    idesc_mxf8((uint32_t)k), sfa_t, sfb_t, (kb > 0 || k > 0) ? 1u : 0u);
+                    }
+                    tc_commit(smem_u32(&empty[stage]));
+                    if (++stage == kF8Stages) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                tc_commit(smem_u32(tfull));
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                report(dst, MXP_TIMEOUT, 5, blockIdx.x);
+            }
+        }
+    } else {
+        // ---------------- epilogue ----------------
+        const int ew = warp - 2;
+        const int quarter = warp & 3;
+        const int col_half = ew >> 2;
+        uint32_t it = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
+            int tm, tn;
+            tiles.get(t, tm, tn);
+            if (!mbar_wait(smem_u32(tfull), it & 1u, abort_flag)) {
+                ok = false;
+                break;
+            }
+            __syncwarp();
+            tc_fence_after();
+            uint32_t r[4][32];
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quarter * 32) << 16) + col_half * 128 + 32 * c, r[c]);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(tempty));  // accumulator free: next tile may start
+            const int64_t row = (int64_t)tm * kBM + quarter * 32 + lane;
+            if (row < M) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const int64_t col0 = (int64_t)tn * kF8BN + col_half * 128 + 32 * c;
+                    const int ncol = (int)imin64(32, (int64_t)N - col0);
+                    float *cp = C + col0 * ldc + row;
+                    if (ncol >= 32) {
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            float cv[16];
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) cv[j] = __ldcs(cp + (16 * h + j) * ldc);
+#pragma unroll
+                            for (int j = 0; j < 16; ++j)
+                                __stcs(cp + (16 * h + j) * ldc, cv[j] - __uint_as_float(r[c][16 * h + j]));
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (j < ncol) cp[j * ldc] = cp[j * ldc] - __uint_as_float(r[c][j]);
+                    }
+                }
+            }
+        }
+        if (!ok && lane == 0) {
+            *abort_flag = 1;
+            report(dst, MXP_TIMEOUT, 6, blockIdx.x);
+        }
+    }
+
+    __syncthreads();
+    if (*abort_flag) {
         if (threadIdx.x == 0) {
             const unsigned long long t0 = globaltimer_ns();
             while (globaltimer_ns() - t0 < 50000ull) {
@@ -389,42 +672,61 @@ mxp_status make_kmajor_map(CUtensorMap *map, CUtensorMapDataType dt, int esize, 
 
 mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ldl,
                         const uint8_t *lsc, const void *R, int64_t ldr, const uint8_t *rsc,
-                        float *C, int64_t ldc, DevStatus *dst, cudaStream_t st) {
-    (void)lsc;
-    (void)rsc;
+                        float *C, int64_t ldc, DevStatus *dst, cudaStream_t st, int store,
+                        int lsc_ld, int rsc_ld, int tri_mode) {
     if (m < 0 || n < 0 || k < 0) return fail(MXP_INVALID_ARG, "schur: negative size");
     if (m == 0 || n == 0 || k == 0) return MXP_OK;
     if (ldc < m) return fail(MXP_INVALID_ARG, "schur: ldc < m");
-    if (form == MXP_FORM_FP8) return fail(MXP_UNSUPPORTED, "schur: FP8 form not built yet");
-    if (form != MXP_FORM_FP16 && form != MXP_FORM_BF16X2)
+    if (form != MXP_FORM_FP16 && form != MXP_FORM_BF16X2 && form != MXP_FORM_FP8)
         return fail(MXP_INVALID_ARG, "schur: unknown form");
     if (m > (1 << 30) || n > (1 << 30)) return fail(MXP_INVALID_ARG, "schur: size too large");
     const int64_t K = (form == MXP_FORM_BF16X2) ? 3 * (int64_t)k : k;
     if (ldl < K || ldr < K) return fail(MXP_INVALID_ARG, "schur: panel ld smaller than K");
+    TileMap tiles;
+    tiles.tiles_m = (int)cdiv(m, kBM);
+    tiles.tiles_n = (int)cdiv(n, form == MXP_FORM_FP8 ? kF8BN : kBN);
+    tiles.group_m = 16;
+    const int64_t total = (int64_t)tiles.tiles_m * tiles.tiles_n;
+    if (total > (int64_t)1 << 31) return fail(MXP_INVALID_ARG, "schur: too many tiles");
+    const int grid = (int)(total < num_sms() ? total : num_sms());
+    CUtensorMap mapA, mapB;
+    if (form == MXP_FORM_FP8) {
+        if (!lsc || !rsc) return fail(MXP_INVALID_ARG, "schur: FP8 form needs both scale tables");
+        if (store || tri_mode) return fail(MXP_UNSUPPORTED, "schur: store / triangular modes are FP16/BF16 only");
+        mxp_status s = make_kmajor_map(&mapA, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, L, K, m, ldl, 128, kBM);
+        if (s != MXP_OK) return s;
+        s = make_kmajor_map(&mapB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, R, K, n, ldr, 128, kF8BN);
+        if (s != MXP_OK) return s;
+        static bool attr8 = false;
+        if (!attr8) {
+            MXP_CUDA(cudaFuncSetAttribute(schur_tc_fp8_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kF8SmemBytes));
+            attr8 = true;
+        }
+        const int kt = (int)cdiv(K, 128);
+        schur_tc_fp8_kernel<<<grid, kThreads, kF8SmemBytes, st>>>(
+            mapA, mapB, m, n, (int)K, lsc, rsc, lsc_ld > 0 ? lsc_ld : kt, rsc_ld > 0 ? rsc_ld : kt, C,
+            ldc, tiles, dst);
+        MXP_LAUNCHED();
+        return MXP_OK;
+    }
     const CUtensorMapDataType dt =
         form == MXP_FORM_FP16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
-    CUtensorMap mapA, mapB;
     mxp_status s = make_kmajor_map(&mapA, dt, 2, L, K, m, ldl, 64, kBM);
     if (s != MXP_OK) return s;
     s = make_kmajor_map(&mapB, dt, 2, R, K, n, ldr, 64, kBN);
     if (s != MXP_OK) return s;
-
     static bool attr_done = false;
     if (!attr_done) {
         MXP_CUDA(cudaFuncSetAttribute(schur_tc_f16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       kSmemBytes));
         attr_done = true;
     }
-    TileMap tiles;
-    tiles.tiles_m = (int)cdiv(m, kBM);
-    tiles.tiles_n = (int)cdiv(n, kBN);
-    tiles.group_m = 16;
-    const int64_t total = (int64_t)tiles.tiles_m * tiles.tiles_n;
-    if (total > (int64_t)1 << 31) return fail(MXP_INVALID_ARG, "schur: too many tiles");
-    const int grid = (int)(total < num_sms() ? total : num_sms());
     const uint32_t idesc = idesc_f16(form == MXP_FORM_FP16 ? 0u : 1u);
+    // the triangular skip needs whole stages inside one K segment
+    if (tri_mode != 0 && (k % 64 != 0)) tri_mode = 0;
     schur_tc_f16_kernel<<<grid, kThreads, kSmemBytes, st>>>(mapA, mapB, m, n, (int)K, C, ldc, idesc,
-                                                            tiles, dst);
+                                                            tiles, store, tri_mode, k, dst);
     MXP_LAUNCHED();
     return MXP_OK;
 }

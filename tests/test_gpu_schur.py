@@ -8,7 +8,7 @@ from tests.gpu_util import from_np_colmajor, to_np_colmajor
 
 pytestmark = pytest.mark.gpu
 
-FORMS = [0, 1]  # FP16, BF16X2 (FP8 joins when its kernel lands)
+FORMS = [0, 1, 2]  # FP16, BF16X2, FP8 (block-scaled)
 
 
 def _run(mxp, torch, form, m, n, K, seed=0):
@@ -70,6 +70,44 @@ def test_schur_exact_small_integers(mxp, orc, torch_cuda):
     torch.cuda.synchronize()
     got = to_np_colmajor(dC, m, n, m)
     want = Cm - L @ U
+    assert np.array_equal(got, want)
+
+
+def _tiles(rng, rows, cols, scales):
+    """Integer-valued blocks in [-7, 7] times a per-128x128-tile power of two."""
+    a = rng.integers(-7, 8, (rows, cols)).astype(np.float32)
+    for ti in range(-(-rows // 128)):
+        for tk in range(-(-cols // 128)):
+            a[ti * 128:(ti + 1) * 128, tk * 128:(tk + 1) * 128] *= np.float32(scales[(ti + tk) % len(scales)])
+    return a
+
+
+def test_schur_fp8_exact_tile_scales(mxp, orc, torch_cuda):
+    """FP8 with different power-of-two scales per 128x128 tile: every value is
+    exact in E4M3 after scaling, every product and sum exact in FP32, so the
+    block-scaled MMA must reproduce C - L U^T bit for bit.  Pins the scale-
+    factor layout (rows, k-blocks, both operands)."""
+    torch = torch_cuda
+    rng = np.random.default_rng(3)
+    m, n, K = 384, 512, 384
+    L = _tiles(rng, m, K, [1.0, 0.125, 0.25, 2.0])
+    Ut = _tiles(rng, n, K, [0.5, 1.0, 4.0])      # R = U^T, rows n
+    U = np.asfortranarray(Ut.T)
+    Cm = rng.integers(-1000, 1000, (m, n)).astype(np.float32)
+    dL = from_np_colmajor(torch, L)
+    dU = from_np_colmajor(torch, U)
+    dC = from_np_colmajor(torch, Cm)
+    Lp = torch.zeros(m * K, dtype=torch.uint8, device="cuda")
+    Rp = torch.zeros(n * K, dtype=torch.uint8, device="cuda")
+    ls = torch.zeros(3 * 3 + 16, dtype=torch.uint8, device="cuda")
+    rs = torch.zeros(4 * 3 + 16, dtype=torch.uint8, device="cuda")
+    ws = mxp.Workspace(1024, 128, 2)
+    mxp.panel_cast_left(2, m, K, dL, m, Lp, K, ls)
+    mxp.panel_cast_right(2, n, K, dU, K, Rp, K, rs)
+    mxp.schur_update(2, m, n, K, Lp, K, Rp, K, dC, m, ws, ls, rs)
+    torch.cuda.synchronize()
+    got = to_np_colmajor(dC, m, n, m)
+    want = Cm - (L.astype(np.float64) @ U.astype(np.float64)).astype(np.float32)
     assert np.array_equal(got, want)
 
 
