@@ -184,6 +184,19 @@ mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_workspace *ws
 mxp_status mxp_otf_gemv(int n, uint64_t seed, const double *d_d, double alpha, const double *d_x,
                         double beta, double *d_y, mxp_workspace *ws, void *stream);
 
+/* No counterpart in the reference.  mxp_otf_gemv for callers that cannot
+ * allocate device memory or own a workspace (code placed inside an existing
+ * refinement loop that only holds raw vector pointers, or applications that
+ * forbid device allocation after start-up because cudaMalloc / cudaFree can
+ * synchronise the whole device).  Same result as mxp_otf_gemv within FP64
+ * rounding; the split partial sums live in a fixed 4 MiB device array inside
+ * the library, reserved on every GPU that loads it until the process exits.
+ * Limit: n <= 262144, larger n returns MXP_INVALID_ARG.  The first call on a
+ * device resolves the array's address (make it before any stream capture).
+ * All calls share the array: calls that overlap on the GPU race. */
+mxp_status mxp_otf_gemv_noalloc(int n, uint64_t seed, const double *d_d, double alpha,
+                                const double *d_x, double beta, double *d_y, void *stream);
+
 /* trsvL_h + trsvU_h (panel_trsv.hpp:308-597): x <- U^{-1} L^{-1} x with
  * the FP32 factors of mxp_panel_lu, vectors in FP64, exact block
  * substitution. */
