@@ -333,7 +333,8 @@ def run_gpu(args):
                    "hpl_harness": last_ir["hpl_harness"],
                    "residual": last_ir["residual"], "converged": last_ir["converged"]},
             "phases_ms": {k: sum(l[k] for l in lus) / len(lus)
-                          for k in ("ms_total", "ms_diag_lu", "ms_trsm", "ms_cast", "ms_schur")},
+                          for k in ("ms_total", "ms_diag_lu", "ms_trsm", "ms_trsm_inv", "ms_trsm_gemm",
+                                    "ms_cast", "ms_schur")},
             "ir_ms": sum(i["ms_total"] for i in irs) / len(irs),
         }
         print(json.dumps(line), flush=True)

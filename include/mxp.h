@@ -58,10 +58,12 @@ typedef struct {
     double ms_total;
     double ms_diag_lu;   /* DIAG_LU */
     double ms_trsm;      /* TRSM_L + TRSM_R */
-    double ms_cast;      /* CONV_L + CONV_R */
+    double ms_cast;      /* CONV_L + CONV_R, and the split-BF16 operand casts of the TRSM */
     double ms_schur;     /* GEMM_UPDATE */
     int info;            /* 0, or 1 + global index of the first bad pivot */
     int schur_launches;  /* tcgen05 Schur kernel launches */
+    double ms_trsm_inv;  /* part of ms_trsm: FP32 triangular inverses */
+    double ms_trsm_gemm; /* part of ms_trsm: tensor-core products against the inverses */
 } mxp_lu_stats;
 
 typedef struct {

@@ -35,7 +35,7 @@ class MxpError(RuntimeError):
 class LuStats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_diag_lu", C.c_double), ("ms_trsm", C.c_double),
                 ("ms_cast", C.c_double), ("ms_schur", C.c_double), ("info", C.c_int),
-                ("schur_launches", C.c_int)]
+                ("schur_launches", C.c_int), ("ms_trsm_inv", C.c_double), ("ms_trsm_gemm", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

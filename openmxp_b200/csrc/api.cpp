@@ -96,7 +96,7 @@ struct mxp_workspace {
     // tensor-core panel TRSM: FP32 triangular inverses and split-BF16 operands
     int trsm_tc = 1;
     int64_t ldk3 = 0;
-    float *tinv_u = nullptr, *tinv_l = nullptr;
+    float *tinv_u = nullptr, *tinv_l = nullptr, *tinv_tmp = nullptr;
     void *split_big = nullptr, *split_u = nullptr, *split_l = nullptr;
     // GMRES-IR: basis V ((m+1) x n), Hessenberg H ((m+1) x m), rotations, scalars
     int gm_m = 30;
@@ -116,7 +116,8 @@ static int64_t panel_ldk(int b, int form) {
 static size_t trsm_bytes(int n, int b) {
     const int64_t ldk3 = panel_ldk(b, MXP_FORM_BF16X2);
     const int64_t rows = n > b ? n - b : 1;
-    return 2 * (size_t)b * b * 4 + (size_t)(rows + 2 * (int64_t)b) * ldk3 * 2 + 4096;
+    return 2 * (size_t)b * b * 4 + ((size_t)b * b / 4 + 64 * (size_t)b) * 4 +
+           (size_t)(rows + 2 * (int64_t)b) * ldk3 * 2 + 4096;
 }
 
 static size_t ws_layout(int n, int b, int form, size_t *panel_bytes, size_t *scale_bytes,
@@ -188,6 +189,7 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
         const int64_t rows = n > b ? n - b : 1;
         ok = ok && (ws->tinv_u = (float *)alloc((size_t)b * b * 4));
         ok = ok && (ws->tinv_l = (float *)alloc((size_t)b * b * 4));
+        ok = ok && (ws->tinv_tmp = (float *)alloc(((size_t)b * b / 4 + 64 * (size_t)b) * 4));
         ok = ok && (ws->split_big = alloc((size_t)rows * ws->ldk3 * 2 + 1024));
         ok = ok && (ws->split_u = alloc((size_t)b * ws->ldk3 * 2 + 1024));
         ok = ok && (ws->split_l = alloc((size_t)b * ws->ldk3 * 2 + 1024));
@@ -343,7 +345,7 @@ struct PhaseTimer {
         marks.clear();
     }
 };
-enum { PH_DIAG = 0, PH_TRSM = 1, PH_CAST = 2, PH_SCHUR = 3, PH_END = 4 };
+enum { PH_DIAG = 0, PH_TRSM = 1, PH_CAST = 2, PH_SCHUR = 3, PH_TINV = 4, PH_TGEMM = 5, PH_END = 6 };
 }  // namespace
 
 extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_workspace *ws,
@@ -394,15 +396,20 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
             // TRSM-by-inverse idea as the reference's -alt path (panel_trf_gdirect.hpp:73-142)
             // at near-FP32 accuracy instead of FP16.
             const int bf = MXP_FORM_BF16X2;
-            q = launch_tri_inv_upper(b, Akk, lda, ws->tinv_u, b, st);
-            if (q == MXP_OK) q = launch_tri_inv_lower_unit(b, Akk, lda, ws->tinv_l, b, st);
+            pt.mark(PH_TINV);
+            q = launch_tri_inv_upper(b, Akk, lda, ws->tinv_u, b, ws->tinv_tmp, st);
+            if (q == MXP_OK) q = launch_tri_inv_lower_unit(b, Akk, lda, ws->tinv_l, b, ws->tinv_tmp, st);
+            pt.mark(PH_CAST);
             if (q == MXP_OK) q = launch_cast_left(bf, m, b, Lcol, lda, ws->split_big, ws->ldk3, nullptr, st);
             if (q == MXP_OK) q = launch_cast_right(bf, b, b, ws->tinv_u, b, ws->split_u, ws->ldk3, nullptr, st);
+            pt.mark(PH_TGEMM);
             if (q == MXP_OK)
                 q = launch_schur(bf, m, b, b, ws->split_big, ws->ldk3, nullptr, ws->split_u, ws->ldk3,
                                  nullptr, Lcol, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/1);
+            pt.mark(PH_CAST);
             if (q == MXP_OK) q = launch_cast_left(bf, b, b, ws->tinv_l, b, ws->split_l, ws->ldk3, nullptr, st);
             if (q == MXP_OK) q = launch_cast_right(bf, m, b, Urow, lda, ws->split_big, ws->ldk3, nullptr, st);
+            pt.mark(PH_TGEMM);
             if (q == MXP_OK)
                 q = launch_schur(bf, b, m, b, ws->split_l, ws->ldk3, nullptr, ws->split_big, ws->ldk3,
                                  nullptr, Urow, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/2);
@@ -456,13 +463,15 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
     DevStatus h;
     mxp_status rs = read_status(ws, st, &h);
     if (stats) {
-        double ms[4];
-        pt.collect(ms, 4);
+        double ms[6];
+        pt.collect(ms, 6);
         stats->ms_diag_lu = ms[PH_DIAG];
-        stats->ms_trsm = ms[PH_TRSM];
+        stats->ms_trsm = ms[PH_TRSM] + ms[PH_TINV] + ms[PH_TGEMM];
+        stats->ms_trsm_inv = ms[PH_TINV];
+        stats->ms_trsm_gemm = ms[PH_TGEMM];
         stats->ms_cast = ms[PH_CAST];
         stats->ms_schur = ms[PH_SCHUR];
-        stats->ms_total = ms[0] + ms[1] + ms[2] + ms[3];
+        stats->ms_total = ms[0] + ms[1] + ms[2] + ms[3] + ms[4] + ms[5];
         stats->info = h.code == MXP_ZERO_PIVOT ? h.info0 : 0;
         stats->schur_launches = schur_launches;
     }

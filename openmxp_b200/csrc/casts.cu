@@ -46,11 +46,55 @@ __device__ __forceinline__ void store_lowp(void *out, int64_t ldk, int64_t row, 
     }
 }
 
+__device__ __forceinline__ uint32_t pack_h2(float a, float b) {
+    const __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+__device__ __forceinline__ uint32_t pack_bf2(__nv_bfloat16 a, __nv_bfloat16 b) {
+    return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+}
+
+// 8 consecutive k of one row as one 16-byte store per K segment (requires the
+// row start, k0 and b to keep every segment 16-byte aligned; checked by the
+// launcher).
+template <int FORM>
+__device__ __forceinline__ void store8(void *out, int64_t ldk, int64_t row, int k0, int b,
+                                       const float *v, bool is_right) {
+    if (FORM == MXP_FORM_FP16) {
+        uint4 w = make_uint4(pack_h2(v[0], v[1]), pack_h2(v[2], v[3]), pack_h2(v[4], v[5]),
+                             pack_h2(v[6], v[7]));
+        *reinterpret_cast<uint4 *>(reinterpret_cast<__half *>(out) + row * ldk + k0) = w;
+    } else {
+        __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            hi[q] = __float2bfloat16_rn(v[q]);
+            lo[q] = __float2bfloat16_rn(__fsub_rn(v[q], __bfloat162float(hi[q])));
+        }
+        const uint4 H = make_uint4(pack_bf2(hi[0], hi[1]), pack_bf2(hi[2], hi[3]), pack_bf2(hi[4], hi[5]),
+                                   pack_bf2(hi[6], hi[7]));
+        const uint4 Lw = make_uint4(pack_bf2(lo[0], lo[1]), pack_bf2(lo[2], lo[3]), pack_bf2(lo[4], lo[5]),
+                                    pack_bf2(lo[6], lo[7]));
+        __nv_bfloat16 *o = reinterpret_cast<__nv_bfloat16 *>(out) + row * ldk + k0;
+        *reinterpret_cast<uint4 *>(o) = H;
+        *reinterpret_cast<uint4 *>(o + b) = is_right ? Lw : H;
+        *reinterpret_cast<uint4 *>(o + 2 * b) = is_right ? H : Lw;
+    }
+}
+
+template <int FORM>
+__device__ __forceinline__ void store16(void *out, int64_t ldk, int64_t row, int k0, int b,
+                                        const float *v, bool is_right) {
+    store8<FORM>(out, ldk, row, k0, b, v, is_right);
+    store8<FORM>(out, ldk, row, k0 + 8, b, v + 8, is_right);
+}
+
 // L column panel: FP32 m x b column-major -> K-major rows (transpose through
 // shared memory: reads coalesced along rows, writes coalesced along k).
 template <int FORM>
 __global__ void __launch_bounds__(kCastThreads)
-cast_left_kernel(int m, int b, const float *__restrict__ A, int64_t lda, void *out, int64_t ldk) {
+cast_left_kernel(int m, int b, const float *__restrict__ A, int64_t lda, void *out, int64_t ldk,
+                 bool vec) {
     __shared__ float tile[kTile][kTile + 1];
     const int i0 = blockIdx.x * kTile;
     const int k0 = blockIdx.y * kTile;
@@ -67,6 +111,13 @@ cast_left_kernel(int m, int b, const float *__restrict__ A, int64_t lda, void *o
     const int kc = (t % 4) * 16;   // 16 k per thread
     const int64_t row = i0 + ri;
     if (row >= m) return;
+    if (vec && k0 + kc + 16 <= b) {
+        float v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = tile[kc + q][ri];
+        store16<FORM>(out, ldk, row, k0 + kc, b, v, false);
+        return;
+    }
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
         const int k = k0 + kc + q;
@@ -79,13 +130,21 @@ cast_left_kernel(int m, int b, const float *__restrict__ A, int64_t lda, void *o
 // in k.
 template <int FORM>
 __global__ void __launch_bounds__(kCastThreads)
-cast_right_kernel(int m, int b, const float *__restrict__ A, int64_t lda, void *out, int64_t ldk) {
+cast_right_kernel(int m, int b, const float *__restrict__ A, int64_t lda, void *out, int64_t ldk,
+                  bool vec) {
     const int64_t gid = (int64_t)blockIdx.x * kCastThreads + threadIdx.x;
     const int kchunks = (b + 7) / 8;
     const int64_t j = gid / kchunks;
     const int k0 = (int)(gid % kchunks) * 8;
     if (j >= m) return;
     const float *src = A + j * lda;
+    if (vec && k0 + 8 <= b) {
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = src[k0 + q];
+        store8<FORM>(out, ldk, j, k0, b, v, true);
+        return;
+    }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         const int k = k0 + q;
@@ -256,6 +315,11 @@ half_right_trans_ref_kernel(const float *__restrict__ C, int b, int m, int64_t p
 
 }  // namespace
 
+// 16-byte stores need a 16-byte aligned base, row stride and segment offset.
+static bool vec_ok(const void *out, int64_t ldk, int b) {
+    return (reinterpret_cast<uintptr_t>(out) % 16 == 0) && (ldk % 8 == 0) && (b % 8 == 0);
+}
+
 static mxp_status check_cast_args(int form, int m, int b, int64_t lda, int64_t ldk) {
     if (m < 0 || b <= 0) return fail(MXP_INVALID_ARG, "panel cast: bad m/b");
     if (lda < 1) return fail(MXP_INVALID_ARG, "panel cast: bad lda");
@@ -277,11 +341,12 @@ mxp_status launch_cast_left(int form, int m, int b, const float *A, int64_t lda,
         cast_left_fp8_kernel<<<grid, kCastThreads, 0, st>>>(m, b, A, lda, (uint8_t *)out, ldk,
                                                             scales, sc_ld > 0 ? sc_ld : (int)grid.y);
     } else {
+        const bool vec = vec_ok(out, ldk, b);
         dim3 grid((unsigned)cdiv(m, kTile), (unsigned)cdiv(b, kTile));
         if (form == MXP_FORM_FP16)
-            cast_left_kernel<MXP_FORM_FP16><<<grid, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk);
+            cast_left_kernel<MXP_FORM_FP16><<<grid, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk, vec);
         else
-            cast_left_kernel<MXP_FORM_BF16X2><<<grid, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk);
+            cast_left_kernel<MXP_FORM_BF16X2><<<grid, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk, vec);
     }
     MXP_LAUNCHED();
     return MXP_OK;
@@ -298,13 +363,14 @@ mxp_status launch_cast_right(int form, int m, int b, const float *A, int64_t lda
         cast_right_fp8_kernel<<<grid, kCastThreads, 0, st>>>(m, b, A, lda, (uint8_t *)out, ldk,
                                                              scales, sc_ld > 0 ? sc_ld : (int)grid.y);
     } else {
+        const bool vec = vec_ok(out, ldk, b);
         const int64_t threads = (int64_t)m * ((b + 7) / 8);
         const unsigned blocks = (unsigned)cdiv(threads, kCastThreads);
         if (form == MXP_FORM_FP16)
-            cast_right_kernel<MXP_FORM_FP16><<<blocks, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk);
+            cast_right_kernel<MXP_FORM_FP16><<<blocks, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk, vec);
         else
             cast_right_kernel<MXP_FORM_BF16X2><<<blocks, kCastThreads, 0, st>>>(m, b, A, lda, out,
-                                                                                 ldk);
+                                                                                 ldk, vec);
     }
     MXP_LAUNCHED();
     return MXP_OK;

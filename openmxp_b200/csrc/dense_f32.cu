@@ -117,11 +117,17 @@ trsm_llnu_small_kernel(int ncols, int nb, const float *L, int64_t ldl, float *B,
 // ---- C -= A * B, FP32 SIMT GEMM, 128 x 128 tiles, 8 x 8 per thread --------
 constexpr int BM = 128, BN = 128, BK = 16;
 
+// C_z = alpha * A_z * B_z + beta * C_z for batch z = blockIdx.z (pointer strides
+// sA, sB, sC); beta == 0 does not read C.
 __global__ void __launch_bounds__(256)
-sgemm_sub_kernel(int m, int n, int k, const float *__restrict__ A, int64_t lda,
-                 const float *__restrict__ B, int64_t ldb, float *__restrict__ C, int64_t ldc) {
+sgemm_kernel(int m, int n, int k, float alpha, const float *__restrict__ A, int64_t lda,
+             int64_t sA, const float *__restrict__ B, int64_t ldb, int64_t sB, float beta,
+             float *__restrict__ C, int64_t ldc, int64_t sC) {
     __shared__ __align__(16) float As[BK][BM];
     __shared__ __align__(16) float Bs[BK][BN + 4];
+    A += sA * blockIdx.z;
+    B += sB * blockIdx.z;
+    C += sC * blockIdx.z;
     const int t = threadIdx.x;
     const int tx = t % 16, ty = t / 16;
     const int64_t m0 = (int64_t)blockIdx.x * BM, n0 = (int64_t)blockIdx.y * BN;
@@ -192,60 +198,149 @@ sgemm_sub_kernel(int m, int n, int k, const float *__restrict__ A, int64_t lda,
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int64_t gr = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
-            if (gr < m) cc[gr] -= acc[i][j];
+            if (gr < m) cc[gr] = (beta == 0.0f ? 0.0f : beta * cc[gr]) + alpha * acc[i][j];
         }
     }
 }
 
-__global__ void set_identity_kernel(int n, float *X, int64_t ldx) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t j = blockIdx.y;
-    if (i < n) X[j * ldx + i] = (i == j) ? 1.0f : 0.0f;
-}
 
 }  // namespace
 
-// X = U^{-1} for an n x n upper non-unit triangle (the TRSM of the identity,
-// X * U = I, as the reference's -alt 1 path builds its inverse with STRSM on
-// an identity, panel_trf_gdirect.hpp:73-92).  Blocked by 64 with the row
-// range restricted to the non-zero part of X, so the cost is n^3/3.
-mxp_status launch_tri_inv_upper(int n, const float *U, int64_t ldu, float *X, int64_t ldx,
-                                cudaStream_t st) {
-    if (n <= 0) return MXP_OK;
-    set_identity_kernel<<<dim3((unsigned)cdiv(n, 256), (unsigned)n), 256, 0, st>>>(n, X, ldx);
+static mxp_status sgemm_batched(int m, int n, int k, float alpha, const float *A, int64_t lda,
+                                int64_t sA, const float *B, int64_t ldb, int64_t sB, float beta,
+                                float *C, int64_t ldc, int64_t sC, int batch, cudaStream_t st) {
+    if (m <= 0 || n <= 0 || k <= 0 || batch <= 0) return MXP_OK;
+    dim3 grid((unsigned)cdiv(m, BM), (unsigned)cdiv(n, BN), (unsigned)batch);
+    sgemm_kernel<<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
     MXP_LAUNCHED();
-    for (int jb = 0; jb < n; jb += kNB) {
-        const int nbk = n - jb < kNB ? n - jb : kNB;
-        const int rows = jb + nbk;  // X(:, jb:jb+nbk) is zero below row jb+nbk
-        const float *Ujj = U + jb + (int64_t)jb * ldu;
-        float *Xj = X + (int64_t)jb * ldx;
-        trsm_runn_small_kernel<<<(unsigned)cdiv(rows, 128), 128, 0, st>>>(rows, nbk, Ujj, ldu, Xj, ldx);
-        MXP_LAUNCHED();
-        const int rem = n - jb - nbk;
-        if (rem <= 0) continue;
-        mxp_status s = launch_sgemm_sub(rows, rem, nbk, Xj, ldx, Ujj + (int64_t)nbk * ldu, ldu,
-                                        Xj + (int64_t)nbk * ldx, ldx, st);
+    return MXP_OK;
+}
+
+// Triangular inverses by recursive doubling (the reference builds its
+// inverse for the -alt path with STRSM on an identity,
+// panel_trf_gdirect.hpp:73-92; this computes the same X with far fewer,
+// wider launches):
+//   level 0: every 64 x 64 diagonal block is inverted by one CTA;
+//   level S: for adjacent S-blocks [A B; 0 C] (upper) the off-diagonal block
+//   of the inverse is -inv(A) * B * inv(C), two batched SGEMMs per level
+//   through the scratch tmp (>= n*n/4 floats).
+// Upper non-unit: row i of a diagonal block's inverse satisfies x U = e_i.
+__global__ void __launch_bounds__(kNB)
+inv_diag_upper_kernel(int n, const float *__restrict__ U, int64_t ldu, float *__restrict__ X, int64_t ldx) {
+    __shared__ float u[kNB][kNB + 1];  // u[col][row]
+    const int r0 = blockIdx.x * kNB;
+    const int nb = min(kNB, n - r0);
+    for (int idx = threadIdx.x; idx < kNB * kNB; idx += kNB) {
+        const int r = idx % kNB, c = idx / kNB;
+        u[c][r] = (r < nb && c < nb) ? U[(int64_t)(r0 + c) * ldu + r0 + r] : 0.0f;
+    }
+    __syncthreads();
+    const int i = threadIdx.x;
+    if (i >= nb) return;
+    float x[kNB];
+#pragma unroll
+    for (int j = 0; j < kNB; ++j) {
+        float v = (j == i) ? 1.0f : 0.0f;
+#pragma unroll
+        for (int q = 0; q < j; ++q) v -= x[q] * u[j][q];
+        x[j] = (j >= i && j < nb) ? v / u[j][j] : 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < kNB; ++j)
+        if (j < nb) X[(int64_t)(r0 + j) * ldx + r0 + i] = x[j];
+}
+
+// Unit lower: row i of the inverse satisfies x L = e_i, solved from the right.
+__global__ void __launch_bounds__(kNB)
+inv_diag_lower_unit_kernel(int n, const float *__restrict__ L, int64_t ldl, float *__restrict__ X,
+                           int64_t ldx) {
+    __shared__ float l[kNB][kNB + 1];  // l[col][row]
+    const int r0 = blockIdx.x * kNB;
+    const int nb = min(kNB, n - r0);
+    for (int idx = threadIdx.x; idx < kNB * kNB; idx += kNB) {
+        const int r = idx % kNB, c = idx / kNB;
+        l[c][r] = (r < nb && c < nb) ? L[(int64_t)(r0 + c) * ldl + r0 + r] : 0.0f;
+    }
+    __syncthreads();
+    const int i = threadIdx.x;
+    if (i >= nb) return;
+    float x[kNB];
+#pragma unroll
+    for (int jj = 0; jj < kNB; ++jj) {
+        const int j = kNB - 1 - jj;
+        float v = (j == i) ? 1.0f : 0.0f;
+#pragma unroll
+        for (int q = j + 1; q < kNB; ++q) v -= x[q] * l[j][q];
+        x[j] = (j <= i) ? v : 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < kNB; ++j)
+        if (j < nb) X[(int64_t)(r0 + j) * ldx + r0 + i] = x[j];
+}
+
+__global__ void set_zero_kernel(int n, float *X, int64_t ldx) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) X[(int64_t)blockIdx.y * ldx + i] = 0.0f;
+}
+
+mxp_status launch_tri_inv_upper(int n, const float *U, int64_t ldu, float *X, int64_t ldx,
+                                float *tmp, cudaStream_t st) {
+    if (n <= 0) return MXP_OK;
+    set_zero_kernel<<<dim3((unsigned)cdiv(n, 256), (unsigned)n), 256, 0, st>>>(n, X, ldx);
+    MXP_LAUNCHED();
+    inv_diag_upper_kernel<<<(unsigned)cdiv(n, kNB), kNB, 0, st>>>(n, U, ldu, X, ldx);
+    MXP_LAUNCHED();
+    for (int S = kNB; S < n; S *= 2) {
+        const int np = n / (2 * S);
+        const int rem = n - np * 2 * S;
+        const int64_t step = 2 * (int64_t)S * (1 + ldx), stepU = 2 * (int64_t)S * (1 + ldu);
+        const int64_t SS = (int64_t)S * S;
+        // T_p = U12_p * inv(U22_p);  X12_p = -inv(U11_p) * T_p
+        mxp_status s = sgemm_batched(S, S, S, 1.0f, U + (int64_t)S * ldu, ldu, stepU,
+                                     X + S + (int64_t)S * ldx, ldx, step, 0.0f, tmp, S, SS, np, st);
+        if (s == MXP_OK)
+            s = sgemm_batched(S, S, S, -1.0f, X, ldx, step, tmp, S, SS, 0.0f, X + (int64_t)S * ldx, ldx,
+                              step, np, st);
+        if (s == MXP_OK && rem > S) {  // ragged last pair: C block of rem - S
+            const int c = rem - S;
+            const int64_t r0 = (int64_t)np * 2 * S;
+            s = sgemm_batched(S, c, c, 1.0f, U + r0 + (r0 + S) * ldu, ldu, 0, X + (r0 + S) + (r0 + S) * ldx,
+                              ldx, 0, 0.0f, tmp, S, 0, 1, st);
+            if (s == MXP_OK)
+                s = sgemm_batched(S, c, S, -1.0f, X + r0 + r0 * ldx, ldx, 0, tmp, S, 0, 0.0f,
+                                  X + r0 + (r0 + S) * ldx, ldx, 0, 1, st);
+        }
         if (s != MXP_OK) return s;
     }
     return MXP_OK;
 }
 
-// X = L^{-1} for an n x n unit lower triangle (L X = I), blocked by row
-// blocks with the column range restricted to the non-zero part of X.
 mxp_status launch_tri_inv_lower_unit(int n, const float *L, int64_t ldl, float *X, int64_t ldx,
-                                     cudaStream_t st) {
+                                     float *tmp, cudaStream_t st) {
     if (n <= 0) return MXP_OK;
-    set_identity_kernel<<<dim3((unsigned)cdiv(n, 256), (unsigned)n), 256, 0, st>>>(n, X, ldx);
+    set_zero_kernel<<<dim3((unsigned)cdiv(n, 256), (unsigned)n), 256, 0, st>>>(n, X, ldx);
     MXP_LAUNCHED();
-    for (int jb = 0; jb < n; jb += kNB) {
-        const int nbk = n - jb < kNB ? n - jb : kNB;
-        const int cols = jb + nbk;  // X(jb:jb+nbk, :) is zero right of column jb+nbk
-        const float *Ljj = L + jb + (int64_t)jb * ldl;
-        trsm_llnu_small_kernel<<<(unsigned)cdiv(cols, 64), 256, 0, st>>>(cols, nbk, Ljj, ldl, X + jb, ldx);
-        MXP_LAUNCHED();
-        const int rem = n - jb - nbk;
-        if (rem <= 0) continue;
-        mxp_status s = launch_sgemm_sub(rem, cols, nbk, Ljj + nbk, ldl, X + jb, ldx, X + jb + nbk, ldx, st);
+    inv_diag_lower_unit_kernel<<<(unsigned)cdiv(n, kNB), kNB, 0, st>>>(n, L, ldl, X, ldx);
+    MXP_LAUNCHED();
+    for (int S = kNB; S < n; S *= 2) {
+        const int np = n / (2 * S);
+        const int rem = n - np * 2 * S;
+        const int64_t step = 2 * (int64_t)S * (1 + ldx), stepL = 2 * (int64_t)S * (1 + ldl);
+        const int64_t SS = (int64_t)S * S;
+        // [A 0; B C]:  T_p = B_p * inv(A_p);  X21_p = -inv(C_p) * T_p
+        mxp_status s = sgemm_batched(S, S, S, 1.0f, L + S, ldl, stepL, X, ldx, step, 0.0f, tmp, S, SS, np, st);
+        if (s == MXP_OK)
+            s = sgemm_batched(S, S, S, -1.0f, X + S + (int64_t)S * ldx, ldx, step, tmp, S, SS, 0.0f, X + S,
+                              ldx, step, np, st);
+        if (s == MXP_OK && rem > S) {
+            const int c = rem - S;
+            const int64_t r0 = (int64_t)np * 2 * S;
+            s = sgemm_batched(c, S, S, 1.0f, L + (r0 + S) + r0 * ldl, ldl, 0, X + r0 + r0 * ldx, ldx, 0,
+                              0.0f, tmp, c, 0, 1, st);
+            if (s == MXP_OK)
+                s = sgemm_batched(c, S, c, -1.0f, X + (r0 + S) + (r0 + S) * ldx, ldx, 0, tmp, c, 0, 0.0f,
+                                  X + (r0 + S) + r0 * ldx, ldx, 0, 1, st);
+        }
         if (s != MXP_OK) return s;
     }
     return MXP_OK;
@@ -256,7 +351,7 @@ mxp_status launch_sgemm_sub(int m, int n, int k, const float *A, int64_t lda, co
     if (m <= 0 || n <= 0 || k <= 0) return MXP_OK;
     dim3 grid((unsigned)cdiv(m, BM), (unsigned)cdiv(n, BN));
     if (grid.y > 65535) return fail(MXP_UNSUPPORTED, "sgemm_sub: n too large");
-    sgemm_sub_kernel<<<grid, 256, 0, st>>>(m, n, k, A, lda, B, ldb, C, ldc);
+    sgemm_kernel<<<grid, 256, 0, st>>>(m, n, k, -1.0f, A, lda, 0, B, ldb, 0, 1.0f, C, ldc, 0);
     MXP_LAUNCHED();
     return MXP_OK;
 }

@@ -129,10 +129,11 @@ mxp_status launch_trsm_runn(int m, int n, const float *U, int64_t ldu, float *B,
                             cudaStream_t st);
 mxp_status launch_trsm_llnu(int m, int n, const float *L, int64_t ldl, float *B, int64_t ldb,
                             cudaStream_t st);
+// tmp: scratch of at least n*n/4 + 64*n floats
 mxp_status launch_tri_inv_upper(int n, const float *U, int64_t ldu, float *X, int64_t ldx,
-                                cudaStream_t st);
+                                float *tmp, cudaStream_t st);
 mxp_status launch_tri_inv_lower_unit(int n, const float *L, int64_t ldl, float *X, int64_t ldx,
-                                     cudaStream_t st);
+                                     float *tmp, cudaStream_t st);
 mxp_status launch_sgemm_sub(int m, int n, int k, const float *A, int64_t lda, const float *B,
                             int64_t ldb, float *C, int64_t ldc, cudaStream_t st);
 

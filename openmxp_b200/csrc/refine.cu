@@ -135,7 +135,20 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
     const int64_t grow = row0 + r;
     const bool row_ok = r < nrows;
     const int ncb = LOWER ? rb : nrb - 1 - rb;
+    // The factor values do not depend on other blocks: prefetch the next
+    // column block's 16 values while this one waits for its solved x.
+    float lv[16], lnext[16];
+    auto load_l = [&](int q, float *dst) {
+        const int cb = LOWER ? q : nrb - 1 - q;
+        const int64_t c0 = (int64_t)cb * kRB + cph * 16;
+        const int clen = (int)imin64(16, n - c0);
+        const float *col = LU + c0 * lda + grow;
+#pragma unroll
+        for (int cc = 0; cc < 16; ++cc) dst[cc] = (row_ok && cc < clen) ? col[cc * lda] : 0.0f;
+    };
+    if (ncb > 0) load_l(0, lv);
     for (int q = 0; q < ncb && !timed_out; ++q) {
+        if (q + 1 < ncb) load_l(q + 1, lnext);
         const int cb = LOWER ? q : nrb - 1 - q;
         const bool need = LOWER ? (cb > known) : (cb < known);
         if (need) {
@@ -157,11 +170,13 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
         if (timed_out) break;
         const int64_t c0 = (int64_t)cb * kRB + cph * 16;
         const int clen = (int)imin64(16, n - c0);
-        if (row_ok) {
-            const float *col = LU + c0 * lda + grow;
-#pragma unroll 16
-            for (int cc = 0; cc < clen; ++cc) acc = __fma_rn((double)col[cc * lda], __ldcg(x + c0 + cc), acc);
-        }
+        double xv[16];
+#pragma unroll
+        for (int cc = 0; cc < 16; ++cc) xv[cc] = (cc < clen) ? __ldcg(x + c0 + cc) : 0.0;
+#pragma unroll
+        for (int cc = 0; cc < 16; ++cc) acc = __fma_rn((double)lv[cc], xv[cc], acc);
+#pragma unroll
+        for (int cc = 0; cc < 16; ++cc) lv[cc] = lnext[cc];
     }
     if (timed_out) report(dst, MXP_TIMEOUT, 10 + (LOWER ? 0 : 1), rb);
     part[cph][r] = acc;

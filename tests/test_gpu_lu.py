@@ -26,6 +26,8 @@ def test_panel_lu_factors(mxp, orc, torch_cuda, form, n, b, seed, rule, trsm_ten
     # off-diagonal factor entries are tiny next to the diagonal; check them alone too
     low = np.tril(np.ones((n, n), bool), -1)
     assert rel_fro(got[low], A[low]) <= 1e-3
+    up = np.triu(np.ones((n, n), bool), 1)
+    assert rel_fro(got[up], A[up]) <= 1e-3
     nb = n // b
     if not merge or (form == 2 and b % 128):
         assert st["schur_launches"] == nb - 1
