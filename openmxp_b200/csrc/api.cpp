@@ -82,6 +82,7 @@ struct mxp_workspace {
     int64_t kp = 0;          // K extent of one panel (b, or 3b for BF16X2)
     int sc_ld = 0;           // FP8 scale-table row stride (tiles): two panels side by side
     int merge = 1;           // merged look-ahead: two panels per trailing pass
+    int pair = 0;            // Schur / panel products on the 2-SM (cta_group::2) kernel
     size_t esize = 2;        // panel element size
     void *lpanel[2] = {nullptr, nullptr};
     void *rpanel[2] = {nullptr, nullptr};
@@ -228,6 +229,9 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
         case MXP_OPT_MERGE_PANELS:
             ws->merge = value ? 1 : 0;
             return MXP_OK;
+        case MXP_OPT_SCHUR_PAIR:
+            ws->pair = value ? 1 : 0;
+            return MXP_OK;
         case MXP_OPT_GMRES_RESTART:
             if (value < 1 || value > 30) return fail(MXP_INVALID_ARG, "set_option: GMRES restart must be 1..30");
             ws->gm_m = value;
@@ -314,7 +318,7 @@ extern "C" mxp_status mxp_schur_update(int form, int m, int n, int k, const void
                                        mxp_workspace *ws, void *stream) {
     if (!ws) return fail(MXP_INVALID_ARG, "schur: workspace is NULL");
     return launch_schur(form, m, n, k, d_L, ldl, d_lscales, d_R, ldr, d_rscales, d_C, ldc,
-                        ws->status, as_stream(stream));
+                        ws->status, as_stream(stream), 0, 0, 0, 0, ws->pair);
 }
 
 // ---------------------------------------------------------------------------
@@ -377,7 +381,7 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
         return launch_schur(form, (int)mrows, (int)ncols, b * kfac, Lb + lrow * ldk * es, ldk,
                             fp8 ? Ls + (lrow / 128) * scl : nullptr, Rb + rrow * ldk * es, ldk,
                             fp8 ? Rs + (rrow / 128) * scl : nullptr, C, lda, ws->status, st, store,
-                            scl, scl);
+                            scl, scl, 0, ws->pair);
     };
     // Factor the diagonal block of step kk, solve its two panels, and cast them
     // into panel slot `slot` (0 or 1) of the buffers at buffer row `row0`.
@@ -405,14 +409,14 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
             pt.mark(PH_TGEMM);
             if (q == MXP_OK)
                 q = launch_schur(bf, m, b, b, ws->split_big, ws->ldk3, nullptr, ws->split_u, ws->ldk3,
-                                 nullptr, Lcol, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/1);
+                                 nullptr, Lcol, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/1, ws->pair);
             pt.mark(PH_CAST);
             if (q == MXP_OK) q = launch_cast_left(bf, b, b, ws->tinv_l, b, ws->split_l, ws->ldk3, nullptr, st);
             if (q == MXP_OK) q = launch_cast_right(bf, m, b, Urow, lda, ws->split_big, ws->ldk3, nullptr, st);
             pt.mark(PH_TGEMM);
             if (q == MXP_OK)
                 q = launch_schur(bf, b, m, b, ws->split_l, ws->ldk3, nullptr, ws->split_big, ws->ldk3,
-                                 nullptr, Urow, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/2);
+                                 nullptr, Urow, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/2, ws->pair);
         } else {
             q = launch_trsm_runn(m, b, Akk, lda, Lcol, lda, st);
             if (q == MXP_OK) q = launch_trsm_llnu(b, m, Akk, lda, Urow, lda, st);

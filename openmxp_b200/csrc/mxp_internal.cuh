@@ -151,7 +151,7 @@ mxp_status launch_half_right_trans_ref(const float *C, int b, int m, int64_t pld
 mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ldl,
                         const uint8_t *lsc, const void *R, int64_t ldr, const uint8_t *rsc,
                         float *C, int64_t ldc, DevStatus *dst, cudaStream_t st, int store = 0,
-                        int lsc_ld = 0, int rsc_ld = 0, int tri_mode = 0);
+                        int lsc_ld = 0, int rsc_ld = 0, int tri_mode = 0, int pair = 0);
 
 mxp_status launch_otf_gemv(int n, uint64_t seed, const double *d, double alpha, const double *x,
                            double beta, double *y, double *partials, int max_splits,

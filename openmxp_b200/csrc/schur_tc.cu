@@ -9,7 +9,7 @@
 // Design (one CTA per SM, persistent over output tiles):
 //   * tile 128 (rows of L) x 256 (rows of R), K step 64 (2-byte types),
 //     4-stage shared-memory ring filled by TMA (cp.async.bulk.tensor, 128-byte
-//     swizzle, no multicast), synchronised with mbarriers;
+//     swizzle, single-destination loads), synchronised with mbarriers;
 //   * warp 0: TMA producer; warp 1: allocates 512 TMEM columns and issues
 //     tcgen05.mma (kind::f16, M=128, N=256, K=16) from one lane, committing
 //     each stage back to the producer and each finished accumulator to the
@@ -30,10 +30,13 @@
 #include <mutex>
 
 #include "mxp_internal.cuh"
+#include "tc_ptx.cuh"
 
 namespace mxp {
 
 namespace {
+
+using namespace tc;
 
 constexpr int kBM = 128;
 constexpr int kBN = 256;
@@ -45,114 +48,7 @@ constexpr int kThreads = 64 + 32 * kEpiWarps;  // 2 control warps + epilogue
 constexpr int kTmemCols = 512;
 constexpr int kSmemBytes = 1024 /*align slack*/ + kStages * (kStageBytesA + kStageBytesB) + 256;
 
-// ---- PTX wrappers ----------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait: false when the deadline passed or another role aborted.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const unsigned long long t0 = globaltimer_ns();
-    for (uint32_t it = 1;; ++it) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 63u) == 0u) {
-            if (*abort_flag) return false;
-            if (globaltimer_ns() - t0 > kWaitTimeoutNs) return false;
-        }
-    }
-}
-
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
-                                            uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-        : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() {
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-__device__ __forceinline__ void tc_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     bar)
-                 : "memory");
-}
-
-__device__ __forceinline__ void tc_mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
-                                           uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-
-// 32 lanes x 32 consecutive 32-bit columns -> 32 registers per thread.
-__device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&r)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-// Shared-memory matrix descriptor: K-major operand tile, 128-byte swizzle,
-// 8-row core groups 1024 bytes apart (SBO), descriptor version 1 (sm_100).
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
-    uint64_t d = 0;
-    d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);     // start address  [0,14)
-    d |= (uint64_t)1 << 16;                        // LBO (unused with swizzle) [16,30)
-    d |= (uint64_t)(1024 >> 4) << 32;              // SBO [32,46)
-    d |= (uint64_t)1 << 46;                        // version [46,48)
-    d |= (uint64_t)2 << 61;                        // SWIZZLE_128B [61,64)
-    return d;
-}
-
-// Instruction descriptor, kind::f16: D = F32, A/B = F16 (0) or BF16 (1),
-// both K-major, M = 128, N = 256.
-__host__ __device__ constexpr uint32_t idesc_f16(uint32_t ab_fmt) {
-    return (1u << 4) | (ab_fmt << 7) | (ab_fmt << 10) | ((uint32_t)(kBN >> 3) << 17) |
-           ((uint32_t)(kBM >> 4) << 24);
-}
+__host__ __device__ constexpr uint32_t idesc_f16(uint32_t ab_fmt) { return idesc_f16_mn(ab_fmt, kBM, kBN); }
 
 struct TileMap {
     int tiles_m, tiles_n, group_m;
@@ -635,6 +531,8 @@ schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
 
 // ---- host side ---------------------------------------------------------------
 
+}  // namespace
+
 PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;
@@ -668,12 +566,17 @@ mxp_status make_kmajor_map(CUtensorMap *map, CUtensorMapDataType dt, int esize, 
     return MXP_OK;
 }
 
-}  // namespace
+mxp_status launch_schur2(int form, int m, int n, int k, const void *L, int64_t ldl, const uint8_t *lsc,
+                         const void *R, int64_t ldr, const uint8_t *rsc, float *C, int64_t ldc,
+                         DevStatus *dst, cudaStream_t st, int store, int lsc_ld, int rsc_ld, int tri_mode);
 
 mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ldl,
                         const uint8_t *lsc, const void *R, int64_t ldr, const uint8_t *rsc,
                         float *C, int64_t ldc, DevStatus *dst, cudaStream_t st, int store,
-                        int lsc_ld, int rsc_ld, int tri_mode) {
+                        int lsc_ld, int rsc_ld, int tri_mode, int pair) {
+    if (pair)
+        return launch_schur2(form, m, n, k, L, ldl, lsc, R, ldr, rsc, C, ldc, dst, st, store, lsc_ld,
+                             rsc_ld, tri_mode);
     if (m < 0 || n < 0 || k < 0) return fail(MXP_INVALID_ARG, "schur: negative size");
     if (m == 0 || n == 0 || k == 0) return MXP_OK;
     if (ldc < m) return fail(MXP_INVALID_ARG, "schur: ldc < m");

@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 FORMS = [0, 1, 2]  # FP16, BF16X2, FP8 (block-scaled)
 
 
-def _run(mxp, torch, form, m, n, K, seed=0):
+def _run(mxp, torch, form, m, n, K, seed=0, pair=True):
     rng = np.random.default_rng(seed + 31 * m + n + K + form)
     L = (rng.standard_normal((m, K)) * 1e-2).astype(np.float32)
     U = (rng.standard_normal((K, n)) * 0.5).astype(np.float32)
@@ -28,7 +28,7 @@ def _run(mxp, torch, form, m, n, K, seed=0):
     Rp = torch.zeros(n * ldk + 64, dtype=dt, device="cuda")
     ls = torch.zeros(((m + 127) // 128) * ((K + 127) // 128) + 16, dtype=torch.uint8, device="cuda")
     rs = torch.zeros(((n + 127) // 128) * ((K + 127) // 128) + 16, dtype=torch.uint8, device="cuda")
-    ws = mxp.Workspace(max(m, n, K) + K, K, form)
+    ws = mxp.Workspace(max(m, n, K) + K, K, form, schur_pair=pair)
     mxp.panel_cast_left(form, m, K, dL, m, Lp, ldk, ls if form == 2 else None)
     mxp.panel_cast_right(form, n, K, dU, K, Rp, ldk, rs if form == 2 else None)
     mxp.schur_update(form, m, n, K, Lp, ldk, Rp, ldk, dC, ldc, ws, ls if form == 2 else None,
@@ -37,18 +37,20 @@ def _run(mxp, torch, form, m, n, K, seed=0):
     return L, U, Cm, to_np_colmajor(dC, m, n, ldc)
 
 
+@pytest.mark.parametrize("pair", [True, False])
 @pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("m,n,K", [(128, 256, 64), (300, 500, 128), (1, 1, 64), (129, 257, 192),
                                    (1024, 1024, 256), (257, 300, 2560), (2048, 1536, 1024)])
-def test_schur_vs_oracle(mxp, orc, torch_cuda, form, m, n, K):
-    L, U, Cm, got = _run(mxp, torch_cuda, form, m, n, K)
+def test_schur_vs_oracle(mxp, orc, torch_cuda, form, m, n, K, pair):
+    L, U, Cm, got = _run(mxp, torch_cuda, form, m, n, K, pair=pair)
     want = orc.schur_update(form, Cm, L, U)
     bound = np.abs(L.astype(np.float64)) @ np.abs(U.astype(np.float64))
     err = np.abs(got.astype(np.float64) - want.astype(np.float64))
     assert np.all(err <= 1e-5 * bound + 1e-6 * np.abs(want) + 1e-30), float(np.max(err - 1e-5 * bound))
 
 
-def test_schur_exact_small_integers(mxp, orc, torch_cuda):
+@pytest.mark.parametrize("pair", [True, False])
+def test_schur_exact_small_integers(mxp, orc, torch_cuda, pair):
     """Integer-valued operands make every product and partial sum exact in
     FP32, so the tensor-core result must equal the oracle bit for bit: a
     direct check of the descriptor / swizzle / TMEM-lane mapping."""
@@ -63,7 +65,7 @@ def test_schur_exact_small_integers(mxp, orc, torch_cuda):
     dC = from_np_colmajor(torch, Cm)
     Lp = torch.zeros(m * K, dtype=torch.int16, device="cuda")
     Rp = torch.zeros(n * K, dtype=torch.int16, device="cuda")
-    ws = mxp.Workspace(1024, K, 0)
+    ws = mxp.Workspace(1024, K, 0, schur_pair=pair)
     mxp.panel_cast_left(0, m, K, dL, m, Lp, K)
     mxp.panel_cast_right(0, n, K, dU, K, Rp, K)
     mxp.schur_update(0, m, n, K, Lp, K, Rp, K, dC, m, ws)
@@ -82,7 +84,8 @@ def _tiles(rng, rows, cols, scales):
     return a
 
 
-def test_schur_fp8_exact_tile_scales(mxp, orc, torch_cuda):
+@pytest.mark.parametrize("pair", [True, False])
+def test_schur_fp8_exact_tile_scales(mxp, orc, torch_cuda, pair):
     """FP8 with different power-of-two scales per 128x128 tile: every value is
     exact in E4M3 after scaling, every product and sum exact in FP32, so the
     block-scaled MMA must reproduce C - L U^T bit for bit.  Pins the scale-
@@ -101,7 +104,7 @@ def test_schur_fp8_exact_tile_scales(mxp, orc, torch_cuda):
     Rp = torch.zeros(n * K, dtype=torch.uint8, device="cuda")
     ls = torch.zeros(3 * 3 + 16, dtype=torch.uint8, device="cuda")
     rs = torch.zeros(4 * 3 + 16, dtype=torch.uint8, device="cuda")
-    ws = mxp.Workspace(1024, 128, 2)
+    ws = mxp.Workspace(1024, 128, 2, schur_pair=pair)
     mxp.panel_cast_left(2, m, K, dL, m, Lp, K, ls)
     mxp.panel_cast_right(2, n, K, dU, K, Rp, K, rs)
     mxp.schur_update(2, m, n, K, Lp, K, Rp, K, dC, m, ws, ls, rs)
