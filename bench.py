@@ -7,8 +7,12 @@ residual < 16.  Credited FLOPs are the reference's (2/3 N^3 + 3/2 N^2,
 main.cpp:663); the time is LU + refinement with generation excluded, as in
 main.cpp:617-657.  Default workload: N=122880, B=2560, seed 7.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp16|bf16x2|fp8]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp8|fp16|bf16x2]
+                    [--compare fp16|...|none] [--no-forward-error]
     python bench.py --impl reference      # CPU implementation of the path
+The headline value is the FP8 form; the plain FP16 form is solved beside it on
+the same system ("plain", "ratio_vs_plain"), and both solutions are compared
+with an FP64 reference solve ("forward_error").
 Under torchrun each rank solves its own system (replicas: the path does not
 shard); value = all ranks' credited FLOPs / max-over-ranks time.
 """
@@ -26,7 +30,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "solve TFLOP/s ((2/3N^3+3/2N^2)/t) at residual<16"
+METRIC = "solve TFLOP/s ((2/3N^3+3/2N^2)/t) at residual<16: FP8 form vs FP16 plain"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 
 
@@ -217,8 +221,11 @@ def cpu_baseline_sample_text(cores):
 
 def workload_config(args):
     return {"workload": (f"HPL-MxP solve N={args.n} B={args.b} seed={args.seed} "
-                         f"{args.form}-Schur + FP64 {args.ir} IR to scaled residual<16"),
+                         f"{args.form}-Schur + FP64 {args.ir} IR to scaled residual<16"
+                         + (f", beside the {args.compare} plain form" if args.compare not in
+                            ("none", args.form) else "")),
             "n": args.n, "b": args.b, "seed": args.seed, "form": args.form,
+            "compare": args.compare,
             "diag_rule": "rowsum" if args.diag_rule == 0 else "0.55*rowsum+1",
             "ir": args.ir, "trsm": args.trsm,
             "parallelism": "replicas (one independent system per GPU)",
@@ -228,21 +235,15 @@ def workload_config(args):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
-def run_gpu(args):
+def _solve_arm(args, form_name, p, dev, dist, local, e2e_on):
+    """Warm up, then time args.steps solves of form `form_name` on problem p."""
     import torch
 
     import openmxp_b200 as mxp
 
-    ws_n, rank, local = dist_env()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    dist = init_dist("nccl") if ws_n > 1 else None
-    form = mxp.FORMS[args.form]
-    kmul = 3 if form == mxp.FORM_BF16X2 else 1
+    ws_n = dist_env()[0]
+    form = mxp.FORMS[form_name]
     n, b = args.n, args.b
-    seed = args.seed + (rank if args.distinct_seeds else 0)
-
-    p = mxp.panel_matgen(n, seed, args.diag_rule)
     ws = mxp.Workspace(n, b, form, device=local, trsm_tensor=(args.trsm == "tensor"))
     method = mxp.IR_GMRES if args.ir == "gmres" else mxp.IR_CLASSIC
     x = torch.empty(n, dtype=torch.float64, device=dev)
@@ -275,27 +276,13 @@ def run_gpu(args):
         irs.append(ist)
     launches = mxp.kernel_launches()
     clk = clocks.stop()
+    x_keep = x.clone()
 
-    local_total_ms = sum(step_ms)
-    total_ms = max_over_ranks(local_total_ms, dist, dev)
+    total_ms = max_over_ranks(sum(step_ms), dist, dev)
     value = hpl_flops(n) * args.steps * ws_n / (total_ms / 1e3) / 1e12
 
-    # dominant kernel: the tcgen05 Schur update, timed with events on its stream
-    schur_ms = sum(l["ms_schur"] for l in lus) / len(lus)
-    sflops = schur_flops(n, b, kmul)
-    peaks, peak_kind = load_peaks()
-    peak = peaks.get("bf16_tflops_sustained", PEAKS_FALLBACK["bf16_tflops_sustained"])
-    achieved = sflops / (schur_ms / 1e3) / 1e12 if schur_ms > 0 else None
-    roofline = {"bound": "tensor", "kernel": "schur_tc_f16_kernel",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if achieved else None,
-                "peak_source": f"{peak_kind} bf16 dense, sustained (MEASURED_PEAKS.json)",
-                "traffic": None,
-                "algorithmic_per_launch": "2*m_k^2*K flops, m_k = N-(k+1)B, K = B (x3 for bf16x2)"}
-
-    # end-to-end through the C ABI with host buffers
     e2e = None
-    if not args.no_e2e:
+    if e2e_on:
         h_rhs = torch.empty(n, dtype=torch.float64).pin_memory()
         h_x = torch.empty(n, dtype=torch.float64).pin_memory()
         e2e_s = []
@@ -313,32 +300,126 @@ def run_gpu(args):
         e2e = {"value": hpl_flops(n) * len(e2e_s) * ws_n / tot / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
                "api": "mxp_solve_host (C ABI), pinned host rhs in / x out"}
+    ws.close()
+    last_ir = irs[-1]
+    return {
+        "form": form_name, "value": value, "ms_per_step": total_ms / args.steps, "e2e": e2e,
+        "clocks": clk, "gpu_launches": launches,
+        "ir": {"iterations": last_ir["iterations"], "inner": last_ir["inner_iterations"],
+               "hpl_harness": last_ir["hpl_harness"], "residual": last_ir["residual"],
+               "converged": last_ir["converged"]},
+        "phases_ms": {k: sum(l[k] for l in lus) / len(lus)
+                      for k in ("ms_total", "ms_diag_lu", "ms_trsm", "ms_trsm_inv", "ms_trsm_gemm",
+                                "ms_cast", "ms_schur")},
+        "ir_ms": sum(i["ms_total"] for i in irs) / len(irs),
+        "x": x_keep,
+    }
 
-    line = None
+
+# DRAM bytes (read + write) per Schur launch over the algorithmic bytes (C read +
+# write, L and R panels once), from one ncu capture of each kernel at m = n = 16384
+# (profiles/schur_tc_*.md).  The traffic of a launch of the solve is this ratio
+# times its algorithmic bytes: the C read-modify-write dominates both.
+SCHUR_TRAFFIC_RATIO = {"schur_tc_f16_kernel": 2.853 / 2.315, "schur_tc_fp8_kernel": 2.857 / 2.315}
+
+
+def _schur_launch_bytes(n, b, es, kmul):
+    """Average algorithmic bytes of one trailing Schur launch of the merged schedule."""
+    tot, cnt = 0.0, 0
+    for k in range(0, n // b, 2):
+        m = n - (k + 2) * b
+        if m <= 0:
+            break
+        K = 2 * b * kmul
+        tot += 8.0 * m * m + 2.0 * m * K * es
+        cnt += 1
+    return tot / max(cnt, 1)
+
+
+def _roofline(args, arm):
+    """Dominant kernel: the tcgen05 Schur update, event-timed on the solve stream."""
+    import openmxp_b200 as mxp
+    form = mxp.FORMS[arm["form"]]
+    kmul = 3 if form == mxp.FORM_BF16X2 else 1
+    es = 1 if form == mxp.FORM_FP8 else 2
+    schur_ms = arm["phases_ms"]["ms_schur"]
+    sflops = schur_flops(args.n, args.b, kmul)
+    peaks, peak_kind = load_peaks()
+    bf16 = peaks.get("bf16_tflops_sustained", PEAKS_FALLBACK["bf16_tflops_sustained"])
+    if form == mxp.FORM_FP8:
+        # no FP8 figure is measured for this pool: FP8 dense issues at twice the
+        # BF16 rate per SM, so the denominator is 2 x the measured BF16 peak
+        peak, src = 2.0 * bf16, f"2 x {peak_kind} bf16 dense sustained (MEASURED_PEAKS.json)"
+        kern = "schur_tc_fp8_kernel"
+    else:
+        peak, src = bf16, f"{peak_kind} bf16 dense sustained (MEASURED_PEAKS.json)"
+        kern = "schur_tc_f16_kernel"
+    achieved = sflops / (schur_ms / 1e3) / 1e12 if schur_ms > 0 else None
+    alg = _schur_launch_bytes(args.n, args.b, es, kmul)
+    return {"bound": "tensor", "kernel": kern, "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
+            "peak_source": src,
+            "traffic": SCHUR_TRAFFIC_RATIO[kern] * alg if kern in SCHUR_TRAFFIC_RATIO else None,
+            "traffic_note": ("bytes per average trailing launch: ncu DRAM/algorithmic ratio at "
+                             "m=16384 times the launch's algorithmic bytes"),
+            "algorithmic_per_launch": "2*m_k^2*K flops, m_k = N-(k+1)B, K = B (x3 for bf16x2)"}
+
+
+def run_gpu(args):
+    import torch
+
+    import openmxp_b200 as mxp
+
+    ws_n, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = init_dist("nccl") if ws_n > 1 else None
+    n = args.n
+    seed = args.seed + (rank if args.distinct_seeds else 0)
+
+    p = mxp.panel_matgen(n, seed, args.diag_rule)
+    arm = _solve_arm(args, args.form, p, dev, dist, local, not args.no_e2e)
+    plain = None
+    if args.compare not in ("none", args.form):
+        plain = _solve_arm(args, args.compare, p, dev, dist, local, False)
+    rhs = p.rhs.clone()
+    del p
+    torch.cuda.empty_cache()
+
+    fwd = None
+    if not args.no_forward_error:
+        from openmxp_b200 import forward_error as fe
+        x_ref = fe.reference_solution(n, seed, args.diag_rule, rhs)
+        fwd = {arm["form"]: fe.forward_error(arm["x"], x_ref)}
+        if plain is not None:
+            fwd[plain["form"]] = fe.forward_error(plain["x"], x_ref)
+        del x_ref
+        torch.cuda.empty_cache()
+
     if rank == 0:
         cpu = None
         if ws_n == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(1)
-        last_ir = irs[-1]
         line = {
-            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": ws_n,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "metric": METRIC, "value": arm["value"], "unit": "TFLOP/s", "n_gpus": ws_n,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": arm["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"fp16": "f16", "bf16x2": "bf16", "fp8": "e4m3"}[args.form],
             "data": "synthetic (HPL-MxP LCG generator; generation excluded from t)",
             "config": workload_config(args),
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "gpu_launches": launches,
-            "ir": {"iterations": last_ir["iterations"], "inner": last_ir["inner_iterations"],
-                   "hpl_harness": last_ir["hpl_harness"],
-                   "residual": last_ir["residual"], "converged": last_ir["converged"]},
-            "phases_ms": {k: sum(l[k] for l in lus) / len(lus)
-                          for k in ("ms_total", "ms_diag_lu", "ms_trsm", "ms_trsm_inv", "ms_trsm_gemm",
-                                    "ms_cast", "ms_schur")},
-            "ir_ms": sum(i["ms_total"] for i in irs) / len(irs),
+            "roofline": _roofline(args, arm), "cpu_baseline": cpu, "e2e": arm["e2e"],
+            "clocks": arm["clocks"], "gpu_launches": arm["gpu_launches"],
+            "ir": arm["ir"], "phases_ms": arm["phases_ms"], "ir_ms": arm["ir_ms"],
+            "forward_error": fwd,
+            "forward_error_reference": ("FP64 no-pivot blocked LU of the FP64 system (mxp_matgen_f64) "
+                                        "with cuSOLVER/cuBLAS FP64 calls; ||x-x64||inf/||x64||inf"),
         }
+        if plain is not None:
+            line["plain"] = {k: plain[k] for k in ("form", "value", "ms_per_step", "ir", "phases_ms",
+                                                   "ir_ms", "clocks", "gpu_launches")}
+            line["plain"]["roofline"] = _roofline(args, plain)
+            line["ratio_vs_plain"] = arm["value"] / plain["value"]
         print(json.dumps(line), flush=True)
-    ws.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -387,11 +468,49 @@ def run_micro(args):
         def launch():
             mxp.otf_gemv(m, 7, d, -1.0, x, 1.0, y, ws)
         flops = 2.0 * m * m
+    elif args.micro == "cublas":
+        # vendor yardstick at the Schur shape: C(m x m) = L(m x b) . R(m x b)^T through
+        # cuBLAS (torch.mm, FP16 in / FP32 out; torch._scaled_mm for FP8 E4M3 with
+        # tensor-wise scales).  Not part of the solve path.
+        ws = None
+        if es == 1:
+            A8 = (torch.randn(m, b, device="cuda", generator=g) * 8).to(torch.float8_e4m3fn)
+            B8 = (torch.randn(m, b, device="cuda", generator=g) * 8).to(torch.float8_e4m3fn)
+            one = torch.ones((), device="cuda")
+            out_dt = torch.float32
+            try:
+                torch._scaled_mm(A8[:256], B8[:256].t(), scale_a=one, scale_b=one, out_dtype=out_dt)
+            except Exception:  # FP32 output not offered: BF16 output (half the C bytes)
+                out_dt = torch.bfloat16
+            out["out_dtype"] = str(out_dt)
+
+            def launch():
+                torch._scaled_mm(A8, B8.t(), scale_a=one, scale_b=one, out_dtype=out_dt)
+        else:
+            A16 = torch.randn(m, b, device="cuda", generator=g).half()
+            B16 = torch.randn(m, b, device="cuda", generator=g).half()
+            try:
+                torch.mm(A16[:256], B16[:256].t(), out_dtype=torch.float32)
+                out["out_dtype"] = "torch.float32"
+
+                def launch():
+                    torch.mm(A16, B16.t(), out_dtype=torch.float32)
+            except Exception:
+                out["out_dtype"] = "torch.float16"
+
+                def launch():
+                    torch.mm(A16, B16.t())
+        flops = 2.0 * m * m * b
     else:
         raise SystemExit(f"unknown micro benchmark {args.micro}")
     for _ in range(args.warmup):
         launch()
     torch.cuda.synchronize()
+    if args.micro_seconds > 0:  # sustained: repeat until the power cap has settled
+        t_end = time.perf_counter() + args.micro_seconds
+        while time.perf_counter() < t_end:
+            launch()
+            torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -414,7 +533,11 @@ def parse(argv=None):
     ap.add_argument("--n", type=int, default=122880)
     ap.add_argument("--b", type=int, default=2560)
     ap.add_argument("--seed", type=int, default=7)
-    ap.add_argument("--form", choices=["fp16", "bf16x2", "fp8"], default="fp16")
+    ap.add_argument("--form", choices=["fp16", "bf16x2", "fp8"], default="fp8")
+    ap.add_argument("--compare", choices=["fp16", "bf16x2", "fp8", "none"], default="fp16",
+                    help="form measured beside --form on the same system (the plain FP16 form)")
+    ap.add_argument("--no-forward-error", action="store_true",
+                    help="skip the FP64 reference solve (8 N^2 bytes of device memory)")
     ap.add_argument("--diag-rule", type=int, default=0)
     ap.add_argument("--maxit", type=int, default=50)
     ap.add_argument("--ir", choices=["classic", "gmres"], default="classic")
@@ -422,8 +545,10 @@ def parse(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--micro", choices=["schur", "otf_gemv"], default=None,
+    ap.add_argument("--micro", choices=["schur", "otf_gemv", "cublas"], default=None,
                     help="time one kernel alone at m=--n, k=--b (for profiler captures)")
+    ap.add_argument("--micro-seconds", type=float, default=0.0,
+                    help="micro: run the launch this long before timing (sustained clocks)")
     ap.add_argument("--distinct-seeds", action="store_true",
                     help="rank r solves seed+r instead of the same system")
     return ap.parse_args(argv)

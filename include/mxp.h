@@ -118,6 +118,13 @@ size_t mxp_workspace_bytes(int n, int b, int form);
 mxp_status mxp_matgen(int n, uint64_t seed, int diag_rule, float *d_A, int64_t lda, double *d_d,
                       double *d_rowsum, double *d_rhs, void *stream);
 
+/* The FP64 system that refinement solves: off-diagonals regenerated in FP64
+ * (the values otf_gemv uses, otf_gemv.cpp:5-133) and the diagonal d of
+ * mxp_matgen (FP64, not rounded to FP32).  n x n column-major, lda >= n.
+ * Used to build FP64 forward-error references. */
+mxp_status mxp_matgen_f64(int n, uint64_t seed, int diag_rule, double *d_A, int64_t lda,
+                          void *stream);
+
 /* ---- granular LU pieces ----------------------------------------------- */
 
 /* GPUSOLVER_SGETRF(h, b, b, A, lda, work, NULL, info) (panel_trf.hpp:

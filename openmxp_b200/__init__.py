@@ -66,6 +66,7 @@ _SIGS = {
     "mxp_workspace_bytes": (C.c_size_t, [_i32, _i32, _i32]),
     "mxp_workspace_set_option": (_i32, [_vp, _i32, _i32]),
     "mxp_matgen": (_i32, [_i32, _u64, _i32, _vp, _i64, _vp, _vp, _vp, _vp]),
+    "mxp_matgen_f64": (_i32, [_i32, _u64, _i32, _vp, _i64, _vp]),
     "mxp_getrf_nopiv": (_i32, [_i32, _vp, _i64, _vp, _vp]),
     "mxp_trsm_right_upper": (_i32, [_i32, _i32, _vp, _i64, _vp, _i64, _vp]),
     "mxp_trsm_left_lower_unit": (_i32, [_i32, _i32, _vp, _i64, _vp, _i64, _vp]),
@@ -196,6 +197,18 @@ def panel_matgen(n: int, seed: int = 42, diag_rule: int = DIAG_ROWSUM, device=No
     check(lib().mxp_matgen(n, seed, diag_rule, _ptr(A), lda, _ptr(d), _ptr(rs), _ptr(rhs),
                            _stream(stream)))
     return Problem(n, seed, diag_rule, A, lda, d, rs, rhs)
+
+
+def matgen_f64(n: int, seed: int = 42, diag_rule: int = DIAG_ROWSUM, A=None, lda: int | None = None,
+               stream=None):
+    """The FP64 system refinement solves (FP64 off-diagonals, diagonal d), column-major."""
+    import torch
+    lda = n if lda is None else lda
+    if A is None:
+        A = torch.empty(n * lda, dtype=torch.float64,
+                        device=torch.device("cuda", torch.cuda.current_device()))
+    check(lib().mxp_matgen_f64(n, seed, diag_rule, _ptr(A), lda, _stream(stream)))
+    return A
 
 
 def regenerate(p: Problem, stream=None) -> None:

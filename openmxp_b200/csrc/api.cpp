@@ -273,6 +273,11 @@ extern "C" mxp_status mxp_matgen(int n, uint64_t seed, int diag_rule, float *d_A
     return launch_matgen(n, seed, diag_rule, d_A, lda, d_d, d_rowsum, d_rhs, as_stream(stream));
 }
 
+extern "C" mxp_status mxp_matgen_f64(int n, uint64_t seed, int diag_rule, double *d_A, int64_t lda,
+                                     void *stream) {
+    return launch_matgen_f64(n, seed, diag_rule, d_A, lda, as_stream(stream));
+}
+
 extern "C" mxp_status mxp_getrf_nopiv(int n, float *d_A, int64_t lda, mxp_workspace *ws,
                                       void *stream) {
     if (!ws) return fail(MXP_INVALID_ARG, "getrf: workspace is NULL");

@@ -67,8 +67,8 @@ fill_kernel(int n, int64_t nrows, int64_t c0, int64_t ncols, uint64_t s00, Aff j
 constexpr int kDiagThreads = 512;  // MATGEM_THREADS of matgen.hpp:7, pinned by the reduction order
 
 __global__ void __launch_bounds__(kDiagThreads)
-diag_kernel(int n, uint64_t s00, Aff jn, Aff j512, int diag_rule, float *A, int64_t lda,
-            double *d, double *rowsum) {
+diag_kernel(int n, uint64_t s00, Aff jn, Aff j512, int diag_rule, float *A, double *A64,
+            int64_t lda, double *d, double *rowsum) {
     __shared__ double sh[kDiagThreads];
     const int64_t row = blockIdx.x;
     const int t = threadIdx.x;
@@ -95,6 +95,7 @@ diag_kernel(int n, uint64_t s00, Aff jn, Aff j512, int diag_rule, float *A, int6
         if (rowsum) rowsum[row] = s;
         if (d) d[row] = dv;
         if (A) A[row * lda + row] = __double2float_rn(dv);
+        if (A64) A64[row * lda + row] = dv;
     }
 }
 
@@ -127,9 +128,35 @@ mxp_status launch_matgen(int n, uint64_t seed, int diag_rule, float *A, int64_t 
     }
     if (A || d || rowsum) {
         const Aff j512 = aff_pow(jn, kDiagThreads);
-        diag_kernel<<<n, kDiagThreads, 0, st>>>(n, s00, jn, j512, diag_rule, A, lda, d, rowsum);
+        diag_kernel<<<n, kDiagThreads, 0, st>>>(n, s00, jn, j512, diag_rule, A, nullptr, lda, d,
+                                                 rowsum);
         MXP_LAUNCHED();
     }
+    return MXP_OK;
+}
+
+mxp_status launch_matgen_f64(int n, uint64_t seed, int diag_rule, double *A, int64_t lda,
+                             cudaStream_t st) {
+    if (n <= 0 || !A) return fail(MXP_INVALID_ARG, "mxp_matgen_f64: bad arguments");
+    if (lda < n) return fail(MXP_INVALID_ARG, "mxp_matgen_f64: lda < n");
+    if (diag_rule != MXP_DIAG_ROWSUM && diag_rule != MXP_DIAG_055_PLUS1)
+        return fail(MXP_INVALID_ARG, "mxp_matgen_f64: unknown diag_rule");
+    const uint64_t s00 = lcg_stat00(seed);
+    const Aff jn = aff_pow(lcg_inc1(), (uint64_t)n);
+    const int64_t row_bands = cdiv(n, kFillRowBand);
+    const int64_t col_bands = cdiv(n, kFillColBand);
+    for (int64_t cb = 0; cb < col_bands; cb += 65535) {
+        const int64_t nb = col_bands - cb < 65535 ? col_bands - cb : 65535;
+        dim3 grid((unsigned)row_bands, (unsigned)nb);
+        const int64_t c0 = cb * kFillColBand;
+        fill_kernel<double><<<grid, kFillThreads, 0, st>>>(n, n, c0, n - c0, s00, jn, A + c0 * lda,
+                                                            lda);
+        MXP_LAUNCHED();
+    }
+    const Aff j512 = aff_pow(jn, kDiagThreads);
+    diag_kernel<<<n, kDiagThreads, 0, st>>>(n, s00, jn, j512, diag_rule, nullptr, A, lda, nullptr,
+                                             nullptr);
+    MXP_LAUNCHED();
     return MXP_OK;
 }
 

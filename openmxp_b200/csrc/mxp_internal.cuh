@@ -120,6 +120,8 @@ __host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { retur
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // Launchers implemented in the individual translation units ---------------
+mxp_status launch_matgen_f64(int n, uint64_t seed, int diag_rule, double *A, int64_t lda,
+                             cudaStream_t st);
 mxp_status launch_matgen(int n, uint64_t seed, int diag_rule, float *A, int64_t lda, double *d,
                          double *rowsum, double *rhs, cudaStream_t st);
 
