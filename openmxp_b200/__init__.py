@@ -130,11 +130,13 @@ OPT_GMRES_RESTART = 2
 OPT_GMRES_TOL_EXP = 3
 OPT_MERGE_PANELS = 4
 OPT_SCHUR_PAIR = 5
+OPT_DIAG_COOP = 6
 
 
 class Workspace:
     def __init__(self, n: int, b: int, form: int | str = FORM_FP16, device: int = 0,
-                 trsm_tensor: bool = True, merge_panels: bool = True, schur_pair: bool = False):
+                 trsm_tensor: bool = True, merge_panels: bool = True, schur_pair: bool = False,
+                 diag_coop: bool = True):
         if isinstance(form, str):
             form = FORMS[form]
         self.n, self.b, self.form, self.device = n, b, form, device
@@ -144,6 +146,7 @@ class Workspace:
         self.set_option(OPT_TRSM_TENSOR, int(trsm_tensor))
         self.set_option(OPT_MERGE_PANELS, int(merge_panels))
         self.set_option(OPT_SCHUR_PAIR, int(schur_pair))
+        self.set_option(OPT_DIAG_COOP, int(diag_coop))
 
     def set_option(self, key: int, value: int) -> None:
         check(lib().mxp_workspace_set_option(self.handle, key, value))

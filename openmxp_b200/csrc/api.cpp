@@ -98,6 +98,10 @@ struct mxp_workspace {
     int trsm_tc = 1;
     int64_t ldk3 = 0;
     float *tinv_u = nullptr, *tinv_l = nullptr, *tinv_tmp = nullptr;
+    // cooperative diagonal-block factorisation (LU + inverses in one launch)
+    int coop = 1;
+    float *coop_tmp = nullptr;          // 2 x diag_factor_tmp_floats(b)
+    unsigned int *coop_sync = nullptr;  // grid-barrier counter + abort word
     void *split_big = nullptr, *split_u = nullptr, *split_l = nullptr;
     // GMRES-IR: basis V ((m+1) x n), Hessenberg H ((m+1) x m), rotations, scalars
     int gm_m = 30;
@@ -118,7 +122,7 @@ static size_t trsm_bytes(int n, int b) {
     const int64_t ldk3 = panel_ldk(b, MXP_FORM_BF16X2);
     const int64_t rows = n > b ? n - b : 1;
     return 2 * (size_t)b * b * 4 + ((size_t)b * b / 4 + 64 * (size_t)b) * 4 +
-           (size_t)(rows + 2 * (int64_t)b) * ldk3 * 2 + 4096;
+           (size_t)(rows + 2 * (int64_t)b) * ldk3 * 2 + 4096 + 2 * diag_factor_tmp_floats(b) * 4 + 256;
 }
 
 static size_t ws_layout(int n, int b, int form, size_t *panel_bytes, size_t *scale_bytes,
@@ -191,6 +195,8 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
         ok = ok && (ws->tinv_u = (float *)alloc((size_t)b * b * 4));
         ok = ok && (ws->tinv_l = (float *)alloc((size_t)b * b * 4));
         ok = ok && (ws->tinv_tmp = (float *)alloc(((size_t)b * b / 4 + 64 * (size_t)b) * 4));
+        ok = ok && (ws->coop_tmp = (float *)alloc(2 * diag_factor_tmp_floats(b) * 4));
+        ok = ok && (ws->coop_sync = (unsigned int *)alloc(256));
         ok = ok && (ws->split_big = alloc((size_t)rows * ws->ldk3 * 2 + 1024));
         ok = ok && (ws->split_u = alloc((size_t)b * ws->ldk3 * 2 + 1024));
         ok = ok && (ws->split_l = alloc((size_t)b * ws->ldk3 * 2 + 1024));
@@ -231,6 +237,9 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
             return MXP_OK;
         case MXP_OPT_SCHUR_PAIR:
             ws->pair = value ? 1 : 0;
+            return MXP_OK;
+        case MXP_OPT_DIAG_COOP:
+            ws->coop = value ? 1 : 0;
             return MXP_OK;
         case MXP_OPT_GMRES_RESTART:
             if (value < 1 || value > 30) return fail(MXP_INVALID_ARG, "set_option: GMRES restart must be 1..30");
@@ -282,7 +291,9 @@ extern "C" mxp_status mxp_getrf_nopiv(int n, float *d_A, int64_t lda, mxp_worksp
                                       void *stream) {
     if (!ws) return fail(MXP_INVALID_ARG, "getrf: workspace is NULL");
     cudaStream_t st = as_stream(stream);
-    mxp_status s = launch_getrf_blocked(n, d_A, lda, ws->status, 0, st);
+    mxp_status s = ws->coop ? launch_diag_factor(n, d_A, lda, nullptr, nullptr, 0, nullptr, nullptr,
+                                                 ws->coop_sync, ws->status, 0, st)
+                            : launch_getrf_blocked(n, d_A, lda, ws->status, 0, st);
     if (s != MXP_OK) return s;
     return read_status(ws, st);
 }
@@ -393,8 +404,15 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
     auto factor_panel = [&](int64_t kk, int slot, int64_t row0) -> mxp_status {
         float *Akk = d_A + kk + kk * lda;
         pt.mark(PH_DIAG);
-        mxp_status q = launch_getrf_blocked(b, Akk, lda, ws->status, (int)kk, st);
         const int m = n - (int)kk - b;
+        // one cooperative launch: LU of the diagonal block and, for the
+        // tensor-core TRSM, the inverses of both triangles
+        const bool coop_inv = ws->coop && ws->trsm_tc && m > 0;
+        float *tmpU = ws->coop_tmp, *tmpL = ws->coop_tmp + diag_factor_tmp_floats(b);
+        mxp_status q = ws->coop ? launch_diag_factor(b, Akk, lda, coop_inv ? ws->tinv_u : nullptr,
+                                                     coop_inv ? ws->tinv_l : nullptr, b, tmpU, tmpL,
+                                                     ws->coop_sync, ws->status, (int)kk, st)
+                                : launch_getrf_blocked(b, Akk, lda, ws->status, (int)kk, st);
         if (q != MXP_OK || m <= 0) return q;
         float *Lcol = Akk + b;
         float *Urow = Akk + (int64_t)b * lda;
@@ -405,9 +423,11 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
             // TRSM-by-inverse idea as the reference's -alt path (panel_trf_gdirect.hpp:73-142)
             // at near-FP32 accuracy instead of FP16.
             const int bf = MXP_FORM_BF16X2;
-            pt.mark(PH_TINV);
-            q = launch_tri_inv_upper(b, Akk, lda, ws->tinv_u, b, ws->tinv_tmp, st);
-            if (q == MXP_OK) q = launch_tri_inv_lower_unit(b, Akk, lda, ws->tinv_l, b, ws->tinv_tmp, st);
+            if (!coop_inv) {
+                pt.mark(PH_TINV);
+                q = launch_tri_inv_upper(b, Akk, lda, ws->tinv_u, b, ws->tinv_tmp, st);
+                if (q == MXP_OK) q = launch_tri_inv_lower_unit(b, Akk, lda, ws->tinv_l, b, ws->tinv_tmp, st);
+            }
             pt.mark(PH_CAST);
             if (q == MXP_OK) q = launch_cast_left(bf, m, b, Lcol, lda, ws->split_big, ws->ldk3, nullptr, st);
             if (q == MXP_OK) q = launch_cast_right(bf, b, b, ws->tinv_u, b, ws->split_u, ws->ldk3, nullptr, st);

@@ -120,6 +120,14 @@ __host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { retur
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // Launchers implemented in the individual translation units ---------------
+// Cooperative diagonal-block factorisation (diag_coop.cu): in-place no-pivot LU
+// of the n x n block A and, when XU/XL are given, inv(U) -> XU and inv(L) -> XL
+// (ld ldx).  tmpU/tmpL: diag_factor_tmp_floats(n) floats each; sync_words: 2
+// words of device memory (zeroed on the stream before the launch).
+size_t diag_factor_tmp_floats(int n);
+mxp_status launch_diag_factor(int n, float *A, int64_t lda, float *XU, float *XL, int64_t ldx,
+                              float *tmpU, float *tmpL, unsigned int *sync_words, DevStatus *dst,
+                              int pivot_base, cudaStream_t st);
 mxp_status launch_matgen_f64(int n, uint64_t seed, int diag_rule, double *A, int64_t lda,
                              cudaStream_t st);
 mxp_status launch_matgen(int n, uint64_t seed, int diag_rule, float *A, int64_t lda, double *d,

@@ -8,12 +8,14 @@ from tests.gpu_util import from_np_colmajor, to_np_colmajor, rel_fro
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("n,pad", [(64, 0), (200, 7), (512, 0), (1000, 24)])
-def test_getrf_nopiv(mxp, orc, torch_cuda, n, pad):
+@pytest.mark.parametrize("coop", [True, False])
+@pytest.mark.parametrize("n,pad", [(64, 0), (200, 7), (512, 0), (1000, 24), (2560, 0)])
+def test_getrf_nopiv(mxp, orc, torch_cuda, n, pad, coop):
+    """coop: the single cooperative launch (grid barriers) vs one launch per 64 columns."""
     torch = torch_cuda
     A, _, _, _ = orc.matgen(n, 5)
     dA = from_np_colmajor(torch, A, ld=n + pad)
-    ws = mxp.Workspace(n, n, 0)
+    ws = mxp.Workspace(n, n, 0, diag_coop=coop)
     mxp.getrf_nopiv(dA, n, n + pad, ws)
     got = to_np_colmajor(dA, n, n, n + pad)
     ref = A.copy(order="F")
@@ -21,14 +23,15 @@ def test_getrf_nopiv(mxp, orc, torch_cuda, n, pad):
     assert rel_fro(got, ref) < 1e-6
 
 
-def test_getrf_zero_pivot_reported(mxp, orc, torch_cuda):
+@pytest.mark.parametrize("coop", [True, False])
+def test_getrf_zero_pivot_reported(mxp, orc, torch_cuda, coop):
     torch = torch_cuda
     n = 128
     A, _, _, _ = orc.matgen(n, 5)
     A[70, 70] = 0.0
     A[70, :] = 0.0           # row 70 all zero -> pivot 70 is exactly zero
     dA = from_np_colmajor(torch, A)
-    ws = mxp.Workspace(n, n, 0)
+    ws = mxp.Workspace(n, n, 0, diag_coop=coop)
     with pytest.raises(mxp.MxpError) as e:
         mxp.getrf_nopiv(dA, n, n, ws)
     assert e.value.status == mxp.ZERO_PIVOT

@@ -9,14 +9,15 @@ from tests.gpu_util import to_np_colmajor, rel_fro
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("trsm_tensor,merge", [(True, True), (True, False), (False, True)])
+@pytest.mark.parametrize("trsm_tensor,merge,coop", [(True, True, True), (True, False, True),
+                                                   (False, True, True), (True, True, False)])
 @pytest.mark.parametrize("form", [0, 1, 2])
 @pytest.mark.parametrize("n,b,seed,rule", [(512, 64, 42, 0), (1024, 128, 7, 0), (2048, 256, 11, 1),
                                            (1536, 512, 42, 0), (1280, 256, 3, 0)])
-def test_panel_lu_factors(mxp, orc, torch_cuda, form, n, b, seed, rule, trsm_tensor, merge):
+def test_panel_lu_factors(mxp, orc, torch_cuda, form, n, b, seed, rule, trsm_tensor, merge, coop):
     torch = torch_cuda
     p = mxp.panel_matgen(n, seed, rule)
-    ws = mxp.Workspace(n, b, form, trsm_tensor=trsm_tensor, merge_panels=merge)
+    ws = mxp.Workspace(n, b, form, trsm_tensor=trsm_tensor, merge_panels=merge, diag_coop=coop)
     st = mxp.panel_lu(p, b, ws)
     got = to_np_colmajor(p.A, n, n, n)
     A, _, _, _ = orc.matgen(n, seed, rule)
