@@ -468,6 +468,37 @@ def run_micro(args):
         def launch():
             mxp.otf_gemv(m, 7, d, -1.0, x, 1.0, y, ws)
         flops = 2.0 * m * m
+    elif args.micro == "diag":
+        # diagonal-block factorisation alone (n = --b): LU, and LU + both triangular
+        # inverses, as one cooperative launch and as the per-step launch chain
+        n = b
+        p = mxp.panel_matgen(n, 3)
+        A0 = p.A.clone()
+        XU = torch.empty(n * n, device="cuda")
+        XL = torch.empty(n * n, device="cuda")
+        res = {}
+        for coop in (True, False):
+            ws = mxp.Workspace(n, n, 0, diag_coop=coop)
+            for inv in (False, True):
+                tot = 0.0
+                for it in range(args.warmup + args.steps):
+                    p.A.copy_(A0)
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    if inv:
+                        mxp.getrf_nopiv_inv(p.A, n, n, XU, XL, n, ws)
+                    else:
+                        mxp.getrf_nopiv(p.A, n, n, ws)
+                    e1.record()
+                    torch.cuda.synchronize()
+                    if it >= args.warmup:
+                        tot += e0.elapsed_time(e1)
+                res[f"{'coop' if coop else 'chain'}_{'lu_inv' if inv else 'lu'}_ms"] = tot / args.steps
+            ws.close()
+        out.update(res)
+        print(json.dumps(out), flush=True)
+        return 0
     elif args.micro == "cublas":
         # vendor yardstick at the Schur shape: C(m x m) = L(m x b) . R(m x b)^T through
         # cuBLAS (torch.mm, FP16 in / FP32 out; torch._scaled_mm for FP8 E4M3 with
@@ -545,7 +576,7 @@ def parse(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--micro", choices=["schur", "otf_gemv", "cublas"], default=None,
+    ap.add_argument("--micro", choices=["schur", "otf_gemv", "cublas", "diag"], default=None,
                     help="time one kernel alone at m=--n, k=--b (for profiler captures)")
     ap.add_argument("--micro-seconds", type=float, default=0.0,
                     help="micro: run the launch this long before timing (sustained clocks)")

@@ -135,6 +135,14 @@ mxp_status mxp_matgen_f64(int n, uint64_t seed, int diag_rule, double *d_A, int6
  * or non-finite pivot is reported through the workspace status. */
 mxp_status mxp_getrf_nopiv(int n, float *d_A, int64_t lda, mxp_workspace *ws, void *stream);
 
+/* GETRF followed by the inverses of both triangles, the operands of the
+ * tensor-core TRSM-by-inverse (the reference's -alt path builds the same
+ * inverses with STRSM on an identity, panel_trf_gdirect.hpp:73-92):
+ * A (n x n) is factored in place, inv(U) -> d_XU and inv(L) (unit lower)
+ * -> d_XL, both n x n with leading dimension ldx.  n <= the workspace's b. */
+mxp_status mxp_getrf_nopiv_inv(int n, float *d_A, int64_t lda, float *d_XU, float *d_XL, int64_t ldx,
+                               mxp_workspace *ws, void *stream);
+
 /* update_left_panels_wGPU (panel_trf.hpp:188-207):
  * STRSM(Right, Upper, NoTrans, NonUnit): B(m x n) <- B * U^{-1}. */
 mxp_status mxp_trsm_right_upper(int m, int n, const float *d_U, int64_t ldu, float *d_B,

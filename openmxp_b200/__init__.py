@@ -68,6 +68,7 @@ _SIGS = {
     "mxp_matgen": (_i32, [_i32, _u64, _i32, _vp, _i64, _vp, _vp, _vp, _vp]),
     "mxp_matgen_f64": (_i32, [_i32, _u64, _i32, _vp, _i64, _vp]),
     "mxp_getrf_nopiv": (_i32, [_i32, _vp, _i64, _vp, _vp]),
+    "mxp_getrf_nopiv_inv": (_i32, [_i32, _vp, _i64, _vp, _vp, _i64, _vp, _vp]),
     "mxp_trsm_right_upper": (_i32, [_i32, _i32, _vp, _i64, _vp, _i64, _vp]),
     "mxp_trsm_left_lower_unit": (_i32, [_i32, _i32, _vp, _i64, _vp, _i64, _vp]),
     "mxp_half_conversion_left": (_i32, [_vp, _i32, _i32, _i64, _vp, _i64, _vp]),
@@ -231,6 +232,11 @@ def panel_lu(p: Problem, b: int, ws: Workspace, stream=None) -> dict:
 
 def getrf_nopiv(A, n: int, lda: int, ws: Workspace, stream=None) -> None:
     check(lib().mxp_getrf_nopiv(n, _ptr(A), lda, ws.handle, _stream(stream)))
+
+
+def getrf_nopiv_inv(A, n: int, lda: int, XU, XL, ldx: int, ws: Workspace, stream=None) -> None:
+    """In-place no-pivot LU of A plus inv(U) -> XU and inv(L) -> XL."""
+    check(lib().mxp_getrf_nopiv_inv(n, _ptr(A), lda, _ptr(XU), _ptr(XL), ldx, ws.handle, _stream(stream)))
 
 
 def trsm_right_upper(m, n, U, ldu, B, ldb, stream=None):

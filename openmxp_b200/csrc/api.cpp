@@ -298,6 +298,25 @@ extern "C" mxp_status mxp_getrf_nopiv(int n, float *d_A, int64_t lda, mxp_worksp
     return read_status(ws, st);
 }
 
+extern "C" mxp_status mxp_getrf_nopiv_inv(int n, float *d_A, int64_t lda, float *d_XU, float *d_XL,
+                                          int64_t ldx, mxp_workspace *ws, void *stream) {
+    if (!ws || !d_A || !d_XU || !d_XL) return fail(MXP_INVALID_ARG, "getrf_inv: NULL argument");
+    if (n <= 0 || n > ws->b) return fail(MXP_INVALID_ARG, "getrf_inv: n must be in 1..b of the workspace");
+    if (lda < n || ldx < n) return fail(MXP_INVALID_ARG, "getrf_inv: bad leading dimension");
+    cudaStream_t st = as_stream(stream);
+    mxp_status s;
+    if (ws->coop) {
+        s = launch_diag_factor(n, d_A, lda, d_XU, d_XL, ldx, ws->coop_tmp,
+                               ws->coop_tmp + diag_factor_tmp_floats(ws->b), ws->coop_sync, ws->status, 0, st);
+    } else {
+        s = launch_getrf_blocked(n, d_A, lda, ws->status, 0, st);
+        if (s == MXP_OK) s = launch_tri_inv_upper(n, d_A, lda, d_XU, ldx, ws->tinv_tmp, st);
+        if (s == MXP_OK) s = launch_tri_inv_lower_unit(n, d_A, lda, d_XL, ldx, ws->tinv_tmp, st);
+    }
+    if (s != MXP_OK) return s;
+    return read_status(ws, st);
+}
+
 extern "C" mxp_status mxp_trsm_right_upper(int m, int n, const float *d_U, int64_t ldu, float *d_B,
                                            int64_t ldb, void *stream) {
     return launch_trsm_runn(m, n, d_U, ldu, d_B, ldb, as_stream(stream));

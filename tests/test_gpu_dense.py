@@ -24,6 +24,31 @@ def test_getrf_nopiv(mxp, orc, torch_cuda, n, pad, coop):
 
 
 @pytest.mark.parametrize("coop", [True, False])
+@pytest.mark.parametrize("n", [64, 200, 1000, 2560])
+def test_getrf_nopiv_inv(mxp, orc, torch_cuda, n, coop):
+    """LU plus both triangular inverses: X_U U = I and X_L L = I to FP32 accuracy."""
+    torch = torch_cuda
+    A, _, _, _ = orc.matgen(n, 3)
+    dA = from_np_colmajor(torch, A)
+    XU = torch.full((n * n,), float("nan"), dtype=torch.float32, device="cuda")
+    XL = torch.full((n * n,), float("nan"), dtype=torch.float32, device="cuda")
+    ws = mxp.Workspace(max(n, 128), n, 0, diag_coop=coop)
+    mxp.getrf_nopiv_inv(dA, n, n, XU, XL, n, ws)
+    LU = to_np_colmajor(dA, n, n, n).astype(np.float64)
+    U = np.triu(LU)
+    L = np.tril(LU, -1) + np.eye(n)
+    xu = to_np_colmajor(XU, n, n, n).astype(np.float64)
+    xl = to_np_colmajor(XL, n, n, n).astype(np.float64)
+    assert np.array_equal(np.tril(xu, -1), np.zeros((n, n)))
+    assert np.array_equal(np.triu(xl, 1), np.zeros((n, n)))
+    assert np.abs(xu @ U - np.eye(n)).max() < 1e-5
+    assert np.abs(xl @ L - np.eye(n)).max() < 1e-5
+    ref = A.copy(order="F")
+    assert orc.lib().orc_getrf_nopiv(n, n, ref.ctypes.data, n) == 0
+    assert rel_fro(LU, ref) < 1e-6
+
+
+@pytest.mark.parametrize("coop", [True, False])
 def test_getrf_zero_pivot_reported(mxp, orc, torch_cuda, coop):
     torch = torch_cuda
     n = 128
