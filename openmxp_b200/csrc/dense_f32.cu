@@ -190,6 +190,18 @@ sgemm_kernel(int m, int n, int k, float alpha, const float *__restrict__ A, int6
                 for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
         }
     }
+    // C is read in full before any store (loads interleaved with stores through
+    // one pointer would be serialised by the compiler)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int64_t gc = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int64_t gr = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
+            acc[i][j] *= alpha;
+            if (beta != 0.0f && gr < m && gc < n) acc[i][j] += beta * C[gc * ldc + gr];
+        }
+    }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int64_t gc = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
@@ -198,7 +210,7 @@ sgemm_kernel(int m, int n, int k, float alpha, const float *__restrict__ A, int6
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int64_t gr = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
-            if (gr < m) cc[gr] = (beta == 0.0f ? 0.0f : beta * cc[gr]) + alpha * acc[i][j];
+            if (gr < m) cc[gr] = acc[i][j];
         }
     }
 }

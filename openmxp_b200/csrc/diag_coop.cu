@@ -13,12 +13,12 @@
 //
 //   LU, for each 64-column step j (D_j = diagonal 64 x 64 block):
 //     strips : L strip rows (thread per row, X = B U_jj^{-1}) and U strip
-//              columns (warp per column, X = L_jj^{-1} B) against D_j held in
-//              shared memory, items spread over all CTAs;
+//              columns (thread per column, X = L_jj^{-1} B) against D_j held
+//              in shared memory, items of 256 rows / columns over all CTAs;
 //     update : trailing rank-64 update in 128 x 128 SIMT tiles.  CTA 0 takes
 //              the tile holding D_{j+1} alone and factors D_{j+1} right after
-//              it (look-ahead), so the 64-step serial factor overlaps the
-//              rest of the update.
+//              it (look-ahead, four threads per row), so the 64-step serial
+//              factor overlaps the rest of the update.
 //   inverses: 64 x 64 diagonal blocks of inv(U) and inv(L) one per item,
 //             then recursive doubling: for adjacent S-blocks the off-diagonal
 //             block of the inverse is -inv(A) B inv(C), two GEMM phases per
@@ -162,6 +162,25 @@ __device__ void gemm_tile(Smem &sm, int m, int n, int kb, int ke, float alpha,
                 for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
         }
     }
+    // C is read in full before any store: interleaved loads and stores through a
+    // pointer the compiler cannot disambiguate would serialise 64 L2 round trips
+    if (accumulate) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int gc = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int gr = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
+                acc[i][j] *= alpha;
+                if (gr < m && gc < n) acc[i][j] += __ldcg(C + (int64_t)gc * ldc + gr);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+#pragma unroll
+            for (int i = 0; i < 8; ++i) acc[i][j] *= alpha;
+    }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int gc = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
@@ -170,44 +189,54 @@ __device__ void gemm_tile(Smem &sm, int m, int n, int kb, int ke, float alpha,
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int gr = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
-            if (gr < m) cc[gr] = (accumulate ? __ldcg(cc + gr) : 0.0f) + alpha * acc[i][j];
+            if (gr < m) cc[gr] = acc[i][j];
         }
     }
     __syncthreads();  // shared tiles are reused by the caller's next item
 }
 
-// ---- 64 x 64 no-pivot LU of D (nb <= 64), rows in registers of threads 0..63 -----
+// ---- 64 x 64 no-pivot LU of D (nb <= 64): four threads per row, 16 columns each ----
 // sgetrf_nopiv_naive order (sgetrf_nopiv.cpp:27-61): scale by the reciprocal
-// pivot, then the rank-1 update.  All CTA threads pass the barriers.
+// pivot, then the rank-1 update.  Thread (row i, quarter q) holds a(i, 16q..16q+15)
+// in registers; the four threads of a row are adjacent lanes of one warp, so the
+// multiplier is shared by a shuffle.  All CTA threads pass the barriers.
 __device__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, DevStatus *dst, int pivot_base) {
-    const int i = threadIdx.x;
-    float a[kNB];
+    const int i = threadIdx.x >> 2, q = threadIdx.x & 3;
+    const int lane_base = (threadIdx.x & 31) & ~3;
+    float a[16];
 #pragma unroll
-    for (int j = 0; j < kNB; ++j) a[j] = (i < nb && j < nb) ? __ldcg(D + (int64_t)j * lda + i) : 0.0f;
+    for (int c = 0; c < 16; ++c) {
+        const int col = q * 16 + c;
+        a[c] = (i < nb && col < nb) ? __ldcg(D + (int64_t)col * lda + i) : 0.0f;
+    }
 #pragma unroll
     for (int k = 0; k < kNB; ++k) {
         if (k < nb) {  // uniform across the CTA
+            const int qk = k >> 4, ck = k & 15;
             if (i == k) {
 #pragma unroll
-                for (int j = 0; j < kNB; ++j)
-                    if (j >= k) sm.t.prow[k & 1][j] = a[j];
+                for (int c = 0; c < 16; ++c)
+                    if (q * 16 + c >= k) sm.t.prow[k & 1][q * 16 + c] = a[c];
             }
             __syncthreads();
             const float piv = sm.t.prow[k & 1][k];
-            if (i == k && (!(piv != 0.0f) || !isfinite(piv))) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
+            if (i == k && q == qk && (!(piv != 0.0f) || !isfinite(piv)))
+                report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
+            const float rcp = 1.0f / piv;
+            float l = (q == qk) ? a[ck] * rcp : 0.0f;
+            l = __shfl_sync(0xffffffffu, l, lane_base + qk);
             if (i > k && i < nb) {
-                const float l = a[k] * (1.0f / piv);
-                a[k] = l;
+                if (q == qk) a[ck] = l;
 #pragma unroll
-                for (int j = 0; j < kNB; ++j)
-                    if (j > k) a[j] -= l * sm.t.prow[k & 1][j];
+                for (int c = 0; c < 16; ++c)
+                    if (q * 16 + c > k) a[c] -= l * sm.t.prow[k & 1][q * 16 + c];
             }
         }
     }
     if (i < nb) {
 #pragma unroll
-        for (int j = 0; j < kNB; ++j)
-            if (j < nb) D[(int64_t)j * lda + i] = a[j];
+        for (int c = 0; c < 16; ++c)
+            if (q * 16 + c < nb) D[(int64_t)(q * 16 + c) * lda + i] = a[c];
     }
     __syncthreads();
 }
@@ -244,23 +273,27 @@ __device__ void trsm_rows(Smem &sm, int m, int nb, float *B, int64_t ldb, int r0
         if (c < nb) B[(int64_t)c * ldb + i] = x[c];
 }
 
-// U strip columns [c0, c0 + 64) of B (nb x ncols): X = L^{-1} B, L = unit lower part of sm.t.
+// U strip columns [c0, c0 + 256) of B (nb x ncols): X = L^{-1} B, L = unit lower
+// part of sm.t; one thread per column, the column's nb values in registers.
 __device__ void trsm_cols(Smem &sm, int ncols, int nb, float *B, int64_t ldb, int c0) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int cc = warp; cc < 64; cc += kCT / 32) {
-        const int j = c0 + cc;
-        if (j >= ncols) break;
-        float *bj = B + (int64_t)j * ldb;
-        float x0 = (lane < nb) ? __ldcg(bj + lane) : 0.0f;
-        float x1 = (lane + 32 < nb) ? __ldcg(bj + lane + 32) : 0.0f;
-        for (int k = 0; k < nb; ++k) {
-            const float xk = __shfl_sync(0xffffffffu, k < 32 ? x0 : x1, k & 31);
-            if (lane > k) x0 -= sm.t.t[k][lane] * xk;
-            if (lane + 32 > k && lane + 32 < nb) x1 -= sm.t.t[k][lane + 32] * xk;
+    const int j = c0 + threadIdx.x;
+    if (j >= ncols) return;
+    float *bj = B + (int64_t)j * ldb;
+    float x[kNB];
+#pragma unroll
+    for (int k = 0; k < kNB; ++k) x[k] = (k < nb) ? __ldcg(bj + k) : 0.0f;
+#pragma unroll
+    for (int r = 1; r < kNB; ++r) {
+        if (r < nb) {
+            float v = x[r];
+#pragma unroll
+            for (int k = 0; k < r; ++k) v -= sm.t.t[k][r] * x[k];
+            x[r] = v;
         }
-        if (lane < nb) bj[lane] = x0;
-        if (lane + 32 < nb) bj[lane + 32] = x1;
     }
+#pragma unroll
+    for (int k = 0; k < kNB; ++k)
+        if (k < nb) bj[k] = x[k];
 }
 
 // Inverse of the 64 x 64 diagonal block `blk` of an upper non-unit (upper = true)
@@ -359,12 +392,12 @@ diag_factor_kernel(int n, float *A, int64_t lda, float *XU, float *XL, int64_t l
         float *Lstrip = Djj + nbk;
         float *Ustrip = Djj + (int64_t)nbk * lda;
         // strips
-        const int lit = (rem + kCT - 1) / kCT, uit = (rem + 63) / 64;
+        const int lit = (rem + kCT - 1) / kCT, uit = (rem + kCT - 1) / kCT;
         if (cta < lit + uit) {
             load_tri(sm, nbk, Djj, lda);
             for (int it = cta; it < lit + uit; it += G) {
                 if (it < lit) trsm_rows(sm, rem, nbk, Lstrip, lda, it * kCT);
-                else trsm_cols(sm, rem, nbk, Ustrip, lda, (it - lit) * 64);
+                else trsm_cols(sm, rem, nbk, Ustrip, lda, (it - lit) * kCT);
             }
         }
         if (!grid_sync(ctl, epoch, 21)) return;

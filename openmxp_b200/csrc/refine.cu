@@ -105,65 +105,131 @@ __device__ __forceinline__ void st_release(int *p, int v) {
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// flags[0..nrb) : block done; flags[nrb] : ticket
+// Block forward (LOWER: unit L) or backward (upper: U) substitution, one
+// 64-row block per CTA, CTAs taking row blocks in solve order from a ticket.
+// flags[0..nrb): block done; flags[nrb]: ticket.
+//
+// The blocks form a chain (block b needs x of every earlier block), so the
+// time per link is what bounds the solve.  Everything that does not depend
+// on the predecessor is done before waiting for it:
+//   * Minv = inverse of the diagonal block (FP64, from the FP32 factor) and
+//     P = Minv * A_adj, A_adj the off-diagonal block next in the chain;
+//   * the products of all other off-diagonal blocks with their (already
+//     solved) x, streamed with one column block of look-ahead;
+//   * w = Minv (r_b - those products).
+// When the predecessor publishes its x, the block finishes with one 64 x 64
+// FP64 matrix-vector product, x_b = w - P x_adj, and publishes its own x.
+// This is the block substitution of the reference's trsvL_h / trsvU_h
+// (panel_trsv.hpp:308-597: FP64 solve of each upcast diagonal block, FP32 x
+// FP64 products for the rest) with the diagonal solve applied as a product
+// with its inverse.
+constexpr size_t kTrsvSmem = 2 * sizeof(double) * kRB * (kRB + 1) + sizeof(float) * kRB * (kRB + 1) +
+                             sizeof(double) * kRB + sizeof(double) * 4 * kRB + 16;
+
 template <bool LOWER>
 __global__ void __launch_bounds__(kTrsvThreads)
 trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *flags,
             DevStatus *dst) {
-    __shared__ float tri[kRB][kRB + 1];  // tri[col][row] of the diagonal block
-    __shared__ double part[kTrsvThreads / kRB][kRB];
-    __shared__ double zs[kRB];
-    __shared__ int s_ticket;
+    extern __shared__ __align__(16) unsigned char trsv_smem[];
+    double(*minv)[kRB + 1] = reinterpret_cast<double(*)[kRB + 1]>(trsv_smem);
+    double(*pm)[kRB + 1] = minv + kRB;
+    float(*blk)[kRB + 1] = reinterpret_cast<float(*)[kRB + 1]>(pm + kRB);   // blk[col][row]
+    double *zs = reinterpret_cast<double *>(blk + kRB);
+    double(*part)[kRB] = reinterpret_cast<double(*)[kRB]>(zs + kRB);
+    int *s_ticket = reinterpret_cast<int *>(part + 4);
+
     const int nrb = (n + kRB - 1) / kRB;
     const int tid = threadIdx.x;
-    if (tid == 0) s_ticket = atomicAdd(&flags[nrb], 1);
+    if (tid == 0) *s_ticket = atomicAdd(&flags[nrb], 1);
     __syncthreads();
-    const int rb = LOWER ? s_ticket : nrb - 1 - s_ticket;
+    const int rb = LOWER ? *s_ticket : nrb - 1 - *s_ticket;
     const int64_t row0 = (int64_t)rb * kRB;
     const int nrows = (int)imin64(kRB, n - row0);
-    const int r = tid % kRB, cph = tid / kRB;  // 4 column phases of 16
+    const int ncb = LOWER ? rb : nrb - 1 - rb;  // off-diagonal column blocks
+    const bool has_adj = ncb > 0;
+    const int adj = LOWER ? rb - 1 : rb + 1;    // chain predecessor
 
-    // diagonal block into shared memory
+    // ---- Minv: inverse of the diagonal block (padded with the identity) ----
     for (int idx = tid; idx < kRB * kRB; idx += kTrsvThreads) {
         const int rr = idx % kRB, cc = idx / kRB;
-        tri[cc][rr] = (rr < nrows && cc < nrows) ? LU[(row0 + cc) * lda + row0 + rr] : 0.0f;
+        float v = (rr < nrows && cc < nrows) ? LU[(row0 + cc) * lda + row0 + rr] : 0.0f;
+        if (rr == cc && (rr >= nrows || LOWER)) v = 1.0f;
+        blk[cc][rr] = v;
+    }
+    __syncthreads();
+    if (tid < kRB) {  // column j of the inverse: T y = e_j
+        const int j = tid;
+        if (LOWER) {
+            for (int i = 0; i < kRB; ++i) {
+                double v = (i == j) ? 1.0 : 0.0;
+                if (i > j)
+                    for (int k = j; k < i; ++k) v = __fma_rn(-(double)blk[k][i], minv[k][j], v);
+                minv[i][j] = (i >= j) ? v : 0.0;
+            }
+        } else {
+            for (int i = kRB - 1; i >= 0; --i) {
+                double v = (i == j) ? 1.0 : 0.0;
+                if (i < j)
+                    for (int k = i + 1; k <= j; ++k) v = __fma_rn(-(double)blk[k][i], minv[k][j], v);
+                minv[i][j] = (i <= j) ? v / (double)blk[i][i] : 0.0;
+            }
+        }
+    }
+    __syncthreads();
+    // ---- P = Minv * A_adj ----
+    const int pi = tid >> 2, ph = tid & 3;  // row of a 64-vector, quarter of its columns
+    if (has_adj) {
+        const int64_t c0 = (int64_t)adj * kRB;
+        const int ncols = (int)imin64(kRB, n - c0);
+        for (int idx = tid; idx < kRB * kRB; idx += kTrsvThreads) {
+            const int rr = idx % kRB, cc = idx / kRB;
+            blk[cc][rr] = (rr < nrows && cc < ncols) ? LU[(c0 + cc) * lda + row0 + rr] : 0.0f;
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int c = ph * 16; c < ph * 16 + 16; ++c) {
+            double v = 0.0;
+#pragma unroll 8
+            for (int k = 0; k < kRB; ++k) v = __fma_rn(minv[pi][k], (double)blk[c][k], v);
+            pm[pi][c] = v;
+        }
     }
 
+    // ---- products with every other off-diagonal block ----
     double acc = 0.0;
     int known = LOWER ? -1 : nrb;  // furthest block known complete
     bool timed_out = false;
+    const int r = tid % kRB, cph = tid / kRB;  // 4 column phases of 16
     const int64_t grow = row0 + r;
     const bool row_ok = r < nrows;
-    const int ncb = LOWER ? rb : nrb - 1 - rb;
-    // The factor values do not depend on other blocks: prefetch the next
-    // column block's 16 values while this one waits for its solved x.
+    const int nstream = has_adj ? ncb - 1 : 0;
     float lv[16], lnext[16];
-    auto load_l = [&](int q, float *dst) {
+    auto load_l = [&](int q, float *d) {
         const int cb = LOWER ? q : nrb - 1 - q;
         const int64_t c0 = (int64_t)cb * kRB + cph * 16;
         const int clen = (int)imin64(16, n - c0);
         const float *col = LU + c0 * lda + grow;
 #pragma unroll
-        for (int cc = 0; cc < 16; ++cc) dst[cc] = (row_ok && cc < clen) ? col[cc * lda] : 0.0f;
+        for (int cc = 0; cc < 16; ++cc) d[cc] = (row_ok && cc < clen) ? col[cc * lda] : 0.0f;
     };
-    if (ncb > 0) load_l(0, lv);
-    for (int q = 0; q < ncb && !timed_out; ++q) {
-        if (q + 1 < ncb) load_l(q + 1, lnext);
+    auto wait_flag = [&](int b) -> bool {
+        const unsigned long long t0 = globaltimer_ns();
+        uint32_t it = 0;
+        while (!ld_acquire(&flags[b])) {
+            if ((++it & 255u) == 0u && globaltimer_ns() - t0 > kWaitTimeoutNs) return false;
+        }
+        return true;
+    };
+    if (nstream > 0) load_l(0, lv);
+    for (int q = 0; q < nstream && !timed_out; ++q) {
+        if (q + 1 < nstream) load_l(q + 1, lnext);
         const int cb = LOWER ? q : nrb - 1 - q;
         const bool need = LOWER ? (cb > known) : (cb < known);
         if (need) {
-            const int latest = LOWER ? rb - 1 : rb + 1;
-            if (ld_acquire(&flags[latest])) {
-                known = latest;
+            if (ld_acquire(&flags[adj - (LOWER ? 1 : -1)])) {
+                known = adj - (LOWER ? 1 : -1);  // blocks complete in chain order
             } else {
-                const unsigned long long t0 = globaltimer_ns();
-                uint32_t it = 0;
-                while (!ld_acquire(&flags[cb])) {
-                    if ((++it & 255u) == 0u && globaltimer_ns() - t0 > kWaitTimeoutNs) {
-                        timed_out = true;
-                        break;
-                    }
-                }
+                timed_out = !wait_flag(cb);
                 known = cb;
             }
         }
@@ -178,42 +244,39 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
 #pragma unroll
         for (int cc = 0; cc < 16; ++cc) lv[cc] = lnext[cc];
     }
-    if (timed_out) report(dst, MXP_TIMEOUT, 10 + (LOWER ? 0 : 1), rb);
     part[cph][r] = acc;
     __syncthreads();
     if (tid < kRB) {
-        double s = part[0][tid] + part[1][tid] + part[2][tid] + part[3][tid];
+        const double s = part[0][tid] + part[1][tid] + part[2][tid] + part[3][tid];
         zs[tid] = (tid < nrows) ? __ldcg(x + row0 + tid) - s : 0.0;
     }
     __syncthreads();
-    if (tid < 32) {
-        // 64 x 64 triangle in FP64 by one warp; lane holds rows lane, lane+32
-        double z0 = zs[tid], z1 = zs[tid + 32];
-        if (LOWER) {
-            for (int k = 0; k < nrows; ++k) {
-                const double zk = __shfl_sync(0xffffffffu, k < 32 ? z0 : z1, k & 31);
-                if (tid > k) z0 -= (double)tri[k][tid] * zk;
-                if (tid + 32 > k) z1 -= (double)tri[k][tid + 32] * zk;
-            }
-        } else {
-            for (int k = nrows - 1; k >= 0; --k) {
-                double dk = (double)tri[k][k];
-                if (k < 32) {
-                    if (tid == k) z0 = z0 / dk;
-                } else {
-                    if (tid + 32 == k) z1 = z1 / dk;
-                }
-                const double zk = __shfl_sync(0xffffffffu, k < 32 ? z0 : z1, k & 31);
-                if (tid < k) z0 -= (double)tri[k][tid] * zk;
-                if (tid + 32 < k) z1 -= (double)tri[k][tid + 32] * zk;
-            }
-        }
-        if (tid < nrows) __stcg(x + row0 + tid, z0);
-        if (tid + 32 < nrows) __stcg(x + row0 + tid + 32, z1);
-        __threadfence();
-        __syncwarp();
-        if (tid == 0) st_release(&flags[rb], 1);
+    // ---- w = Minv z (row pi, four lanes per row) ----
+    double w = 0.0;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) w = __fma_rn(minv[pi][ph * 16 + c], zs[ph * 16 + c], w);
+    w += __shfl_xor_sync(0xffffffffu, w, 1);
+    w += __shfl_xor_sync(0xffffffffu, w, 2);
+    // ---- the chain link: x_b = w - P x_adj ----
+    if (has_adj && !timed_out) {
+        timed_out = !wait_flag(adj);
+        const int64_t c0 = (int64_t)adj * kRB + ph * 16;
+        const int clen = (int)imin64(16, n - c0);
+        double xa[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) xa[c] = (c < clen) ? __ldcg(x + c0 + c) : 0.0;
+        double p = 0.0;
+#pragma unroll
+        for (int c = 0; c < 16; ++c) p = __fma_rn(pm[pi][ph * 16 + c], xa[c], p);
+        p += __shfl_xor_sync(0xffffffffu, p, 1);
+        p += __shfl_xor_sync(0xffffffffu, p, 2);
+        w -= p;
     }
+    if (timed_out) report(dst, MXP_TIMEOUT, 10 + (LOWER ? 0 : 1), rb);
+    if (ph == 0 && pi < nrows) __stcg(x + row0 + pi, w);
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) st_release(&flags[rb], 1);  // published even after a timeout: successors never stall
 }
 
 // ---------------------------------------------------------------------------
@@ -305,9 +368,11 @@ mxp_status launch_lu_solve(int n, const float *LU, int64_t lda, double *x, int *
     if (lda < n) return fail(MXP_INVALID_ARG, "lu_solve: lda < n");
     const int nrb = (int)cdiv(n, kRB);
     MXP_CUDA(cudaMemsetAsync(flags, 0, lu_solve_flag_ints(n) * sizeof(int), st));
-    trsv_kernel<true><<<nrb, kTrsvThreads, 0, st>>>(n, LU, lda, x, flags, dst);
+    MXP_CUDA(cudaFuncSetAttribute(trsv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
+    MXP_CUDA(cudaFuncSetAttribute(trsv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
+    trsv_kernel<true><<<nrb, kTrsvThreads, kTrsvSmem, st>>>(n, LU, lda, x, flags, dst);
     MXP_LAUNCHED();
-    trsv_kernel<false><<<nrb, kTrsvThreads, 0, st>>>(n, LU, lda, x, flags + nrb + 1, dst);
+    trsv_kernel<false><<<nrb, kTrsvThreads, kTrsvSmem, st>>>(n, LU, lda, x, flags + nrb + 1, dst);
     MXP_LAUNCHED();
     return MXP_OK;
 }
