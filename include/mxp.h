@@ -267,6 +267,56 @@ mxp_status mxp_infnorm(int n, const double *d_x, double *h_out, mxp_workspace *w
 int64_t mxp_kernel_launches(void);
 void mxp_reset_kernel_launches(void);
 
+/* ---- batched form ----------------------------------------------------------
+ * Many independent systems of uneven orders (each n a multiple of 128, at most
+ * 8192), every one generated, factored and refined exactly as the single-system
+ * path does (diagonal rule: row sum), all in ONE persistent kernel launch that
+ * is captured once in a CUDA graph and replayed.  The reference has no batched
+ * entry point: it solves one system per job (main.cpp:617-657); this is that
+ * solve repeated over a batch.  Storage is packed: system i's column-major
+ * matrix starts at float offset a_off[i] of A (lda = n[i]) and its vectors at
+ * double offset v_off[i] of d, rhs and x (mxp_batch_layout gives both). */
+typedef struct mxp_batch mxp_batch;
+
+typedef struct {
+    int iterations;      /* refinement corrections applied */
+    int converged;       /* 1 when the scaled residual went below 16 */
+    int info;            /* first zero pivot (1-based) or 0 */
+    int pad;
+    double hpl_harness;  /* final scaled residual */
+    double residual;     /* final ||b - A x||_inf */
+} mxp_batch_result;
+
+typedef struct {
+    double ms_total;     /* device time of the launch */
+    int b, tile_n, stages;
+    int autotuned;
+    int grid;
+} mxp_batch_stats;
+
+/* Orders of a batch drawn from the generator stream of size_seed: value i,
+ * v in [-0.5, 0.5], gives n = 128 * (2 + floor((v + 0.5) * 31)). */
+mxp_status mxp_batch_sizes(int count, uint64_t size_seed, int *h_n);
+mxp_status mxp_batch_create(int count, const int *h_n, const uint64_t *h_seed, int device, mxp_batch **out);
+mxp_status mxp_batch_destroy(mxp_batch *bt);
+mxp_status mxp_batch_layout(const mxp_batch *bt, int64_t *matrix_floats, int64_t *vector_doubles,
+                            int64_t *h_a_off, int64_t *h_v_off);
+/* panel_matgen_dev + panel_colvgen for every system (matgen.hpp:84-117, 419-436) */
+mxp_status mxp_batch_matgen(mxp_batch *bt, float *d_A, double *d_d, double *d_rhs, void *stream);
+/* block size b in {64, 128, 256}, Schur tile width tile_n in {128, 256}, smem
+ * pipeline depth stages in 2..4 (default 128 / 256 / 4) */
+mxp_status mxp_batch_set_config(mxp_batch *bt, int b, int tile_n, int stages);
+/* times every admissible configuration on `sample` systems (0: an eighth of
+ * the batch, spread over the sizes; those matrices are regenerated and
+ * overwritten) and keeps the fastest */
+mxp_status mxp_batch_autotune(mxp_batch *bt, float *d_A, double *d_d, double *d_rhs, double *d_x, int sample,
+                              void *stream, mxp_batch_stats *stats);
+/* LU + classic refinement of every system; A is overwritten by the factors,
+ * x receives the solutions.  Blocking (reads the status word). */
+mxp_status mxp_batch_solve(mxp_batch *bt, float *d_A, const double *d_d, const double *d_rhs, double *d_x,
+                           int maxit, void *stream, mxp_batch_stats *stats);
+mxp_status mxp_batch_results(const mxp_batch *bt, mxp_batch_result *h_results);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,19 @@ class IrStats(C.Structure):
         return d
 
 
+class BatchResult(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("info", C.c_int), ("pad", C.c_int),
+                ("hpl_harness", C.c_double), ("residual", C.c_double)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("ms_total", C.c_double), ("b", C.c_int), ("tile_n", C.c_int), ("stages", C.c_int),
+                ("autotuned", C.c_int), ("grid", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 _vp, _i32, _i64, _u64, _dbl = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double
 
@@ -87,6 +100,15 @@ _SIGS = {
     "mxp_solve_host": (_i32, [_i32, _i32, _u64, _vp, _i64, _vp, _vp, _vp, _vp, _i32, _i32, _vp,
                               _vp, C.POINTER(LuStats), C.POINTER(IrStats)]),
     "mxp_infnorm": (_i32, [_i32, _vp, C.POINTER(_dbl), _vp, _vp]),
+    "mxp_batch_sizes": (_i32, [_i32, _u64, C.POINTER(C.c_int)]),
+    "mxp_batch_create": (_i32, [_i32, C.POINTER(C.c_int), C.POINTER(C.c_uint64), _i32, C.POINTER(_vp)]),
+    "mxp_batch_destroy": (_i32, [_vp]),
+    "mxp_batch_layout": (_i32, [_vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
+    "mxp_batch_matgen": (_i32, [_vp, _vp, _vp, _vp, _vp]),
+    "mxp_batch_set_config": (_i32, [_vp, _i32, _i32, _i32]),
+    "mxp_batch_autotune": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _vp, C.POINTER(BatchStats)]),
+    "mxp_batch_solve": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _vp, C.POINTER(BatchStats)]),
+    "mxp_batch_results": (_i32, [_vp, C.POINTER(BatchResult)]),
     "mxp_kernel_launches": (_i64, []),
     "mxp_reset_kernel_launches": (None, []),
 }
@@ -340,3 +362,80 @@ def reset_kernel_launches() -> None:
 def hpl_flops(n: int) -> float:
     """Credited FLOPs of main.cpp:663: 2/3 n^3 + 3/2 n^2."""
     return 2.0 / 3.0 * n ** 3 + 1.5 * n ** 2
+
+
+# ---------------------------------------------------------------------------
+# batched form: many systems of uneven orders in one persistent launch
+# ---------------------------------------------------------------------------
+def batch_sizes(count: int, size_seed: int = 3) -> list:
+    """Orders 128 * (2 + floor((v + 0.5) * 31)) from the generator stream of size_seed."""
+    out = (C.c_int * count)()
+    check(lib().mxp_batch_sizes(count, size_seed, out))
+    return list(out)
+
+
+class Batch:
+    """count systems (orders n_list, generator seeds seeds) packed in one set of
+    device buffers: A (FP32 matrices), d, rhs, x (FP64 vectors)."""
+
+    def __init__(self, n_list, seeds, device: int = 0):
+        import torch
+        self.count = len(n_list)
+        self.n = list(n_list)
+        self.seeds = list(seeds)
+        h = _vp()
+        ns = (C.c_int * self.count)(*self.n)
+        ss = (C.c_uint64 * self.count)(*self.seeds)
+        check(lib().mxp_batch_create(self.count, ns, ss, device, C.byref(h)))
+        self.handle = h
+        mf, vd = C.c_int64(), C.c_int64()
+        ao, vo = (C.c_int64 * self.count)(), (C.c_int64 * self.count)()
+        check(lib().mxp_batch_layout(h, C.byref(mf), C.byref(vd), ao, vo))
+        self.a_off, self.v_off = list(ao), list(vo)
+        dev = torch.device("cuda", device)
+        self.A = torch.empty(mf.value, dtype=torch.float32, device=dev)
+        self.d = torch.empty(vd.value, dtype=torch.float64, device=dev)
+        self.rhs = torch.empty(vd.value, dtype=torch.float64, device=dev)
+        self.x = torch.empty(vd.value, dtype=torch.float64, device=dev)
+
+    def matrix(self, i: int):
+        """System i's matrix as an (n x n) torch view with [r, c] = a_rc."""
+        n = self.n[i]
+        return self.A[self.a_off[i]:self.a_off[i] + n * n].view(n, n).t()
+
+    def vec(self, t, i: int):
+        return t[self.v_off[i]:self.v_off[i] + self.n[i]]
+
+    def matgen(self, stream=None) -> None:
+        check(lib().mxp_batch_matgen(self.handle, _ptr(self.A), _ptr(self.d), _ptr(self.rhs), _stream(stream)))
+
+    def set_config(self, b: int, tile_n: int = 256, stages: int = 4) -> None:
+        check(lib().mxp_batch_set_config(self.handle, b, tile_n, stages))
+
+    def autotune(self, sample: int = 0, stream=None) -> dict:
+        st = BatchStats()
+        check(lib().mxp_batch_autotune(self.handle, _ptr(self.A), _ptr(self.d), _ptr(self.rhs), _ptr(self.x),
+                                       sample, _stream(stream), C.byref(st)))
+        return st.as_dict()
+
+    def solve(self, maxit: int = 50, stream=None) -> dict:
+        st = BatchStats()
+        check(lib().mxp_batch_solve(self.handle, _ptr(self.A), _ptr(self.d), _ptr(self.rhs), _ptr(self.x),
+                                    maxit, _stream(stream), C.byref(st)))
+        return st.as_dict()
+
+    def results(self) -> list:
+        out = (BatchResult * self.count)()
+        check(lib().mxp_batch_results(self.handle, out))
+        return [{k: getattr(r, k) for k, _ in BatchResult._fields_ if k != "pad"} for r in out]
+
+    def close(self) -> None:
+        if self.handle:
+            lib().mxp_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

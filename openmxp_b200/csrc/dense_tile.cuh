@@ -1,0 +1,322 @@
+// SIMT FP32 building blocks shared by the cooperative diagonal-block
+// factorisation (diag_coop.cu) and the batched solver (batched.cu): a
+// 128 x 128 GEMM tile, the 64 x 64 no-pivot LU and the two 64-wide strip
+// solves.  Every function is called by all kCT threads of the CTA (they
+// contain __syncthreads) and reads its inputs through L2 (ld.global.cg), so it
+// may follow writes made by other CTAs behind a grid barrier.
+#pragma once
+
+#include "mxp_internal.cuh"
+
+namespace mxp {
+namespace dt {
+namespace {  // internal linkage: each translation unit keeps its own copy
+
+constexpr int kCT = 256;  // threads per CTA
+constexpr int kNB = 64;   // inner block of the LU
+constexpr int GBM = 128, GBN = 128, GBK = 16;
+
+struct SmemGemm {
+    float As[GBK][GBM];
+    float Bs[GBK][GBN + 4];
+};
+struct SmemTri {
+    float t[kNB][kNB + 1];   // t[col][row] of a 64 x 64 block
+    float ub[kNB][kNB + 1];  // staging of 64 U-strip columns, ub[col][row]
+    float dinv[kNB];
+    float prow[2][kNB];
+};
+union __align__(16) Smem {
+    SmemGemm g;
+    SmemTri t;
+};
+
+
+// ---- 128 x 128 SIMT GEMM tile ------------------------------------------------
+// C[m0:m0+128, n0:n0+128] (clipped to m x n) = alpha * sum_{k in [kb, ke)} A(:,k) B(k,:)
+// (+ C when accumulate).  8 x 8 outputs per thread.
+// skip > 0 leaves the tile's top-left skip x skip corner untouched (another CTA
+// owns it).
+__device__ void gemm_tile(Smem &sm, int m, int n, int kb, int ke, float alpha,
+                          const float *__restrict__ A, int64_t lda, const float *__restrict__ B,
+                          int64_t ldb, bool accumulate, float *C, int64_t ldc, int m0, int n0,
+                          int skip = 0) {
+    const int t = threadIdx.x;
+    const int tx = t % 16, ty = t / 16;
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+
+    float ra[8], rb[8];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = t + kCT * q;
+            const int kk = idx / GBM, r = idx % GBM;
+            const int gr = m0 + r, gk = k0 + kk;
+            ra[q] = (gr < m && gk < ke) ? __ldcg(A + (int64_t)gk * lda + gr) : 0.0f;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = t + kCT * q;
+            const int cc = idx / GBK, kk = idx % GBK;
+            const int gc = n0 + cc, gk = k0 + kk;
+            rb[q] = (gc < n && gk < ke) ? __ldcg(B + (int64_t)gc * ldb + gk) : 0.0f;
+        }
+    };
+    if (kb < ke) load(kb);
+    for (int k0 = kb; k0 < ke; k0 += GBK) {
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = t + kCT * q;
+            sm.g.As[idx / GBM][idx % GBM] = ra[q];
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = t + kCT * q;
+            sm.g.Bs[idx % GBK][idx / GBK] = rb[q];
+        }
+        __syncthreads();
+        if (k0 + GBK < ke) load(k0 + GBK);
+#pragma unroll
+        for (int kk = 0; kk < GBK; ++kk) {
+            const float4 a0 = *reinterpret_cast<const float4 *>(&sm.g.As[kk][tx * 4]);
+            const float4 a1 = *reinterpret_cast<const float4 *>(&sm.g.As[kk][64 + tx * 4]);
+            const float4 b0 = *reinterpret_cast<const float4 *>(&sm.g.Bs[kk][ty * 4]);
+            const float4 b1 = *reinterpret_cast<const float4 *>(&sm.g.Bs[kk][64 + ty * 4]);
+            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        }
+    }
+    // C is read in full before any store: interleaved loads and stores through a
+    // pointer the compiler cannot disambiguate would serialise 64 L2 round trips
+    if (accumulate) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int gc = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int gr = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
+                acc[i][j] *= alpha;
+                if (gr < m && gc < n) acc[i][j] += __ldcg(C + (int64_t)gc * ldc + gr);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+#pragma unroll
+            for (int i = 0; i < 8; ++i) acc[i][j] *= alpha;
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int gc = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
+        if (gc >= n) continue;
+        float *cc = C + (int64_t)gc * ldc;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int gr = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
+            if (gr < m && !(gr - m0 < skip && gc - n0 < skip)) cc[gr] = acc[i][j];
+        }
+    }
+    __syncthreads();  // shared tiles are reused by the caller's next item
+}
+
+// C[0:m, 0:n] += alpha * A(:, 0:k) B(0:k, :) for m, n <= 64 (one 64 x 64 tile,
+// 4 x 4 outputs per thread): the look-ahead update of the next diagonal block.
+__device__ void gemm_tile64(Smem &sm, int m, int n, int k, float alpha, const float *__restrict__ A, int64_t lda,
+                            const float *__restrict__ B, int64_t ldb, float *C, int64_t ldc) {
+    const int t = threadIdx.x;
+    const int tx = t % 16, ty = t / 16;
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+    for (int k0 = 0; k0 < k; k0 += GBK) {
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int idx = t + kCT * q;           // 0..1023
+            const int kk = idx / 64, r = idx % 64;
+            const int gk = k0 + kk;
+            sm.g.As[kk][r] = (r < m && gk < k) ? __ldcg(A + (int64_t)gk * lda + r) : 0.0f;
+            const int c = idx / GBK, kb = idx % GBK;
+            const int gkb = k0 + kb;
+            sm.g.Bs[kb][c] = (c < n && gkb < k) ? __ldcg(B + (int64_t)c * ldb + gkb) : 0.0f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < GBK; ++kk) {
+            const float4 a = *reinterpret_cast<const float4 *>(&sm.g.As[kk][tx * 4]);
+            const float4 b = *reinterpret_cast<const float4 *>(&sm.g.Bs[kk][ty * 4]);
+            const float av[4] = {a.x, a.y, a.z, a.w};
+            const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int gc = ty * 4 + j;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int gr = tx * 4 + i;
+            acc[i][j] *= alpha;
+            if (gr < m && gc < n) acc[i][j] += __ldcg(C + (int64_t)gc * ldc + gr);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int gc = ty * 4 + j;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int gr = tx * 4 + i;
+            if (gr < m && gc < n) C[(int64_t)gc * ldc + gr] = acc[i][j];
+        }
+    }
+    __syncthreads();
+}
+
+// ---- 64 x 64 no-pivot LU of D (nb <= 64), one row per thread of warps 0-1 ----
+// sgetrf_nopiv_naive order (sgetrf_nopiv.cpp:27-61): scale by the reciprocal
+// pivot, then the rank-1 update.  The two working warps meet at a 64-thread
+// named barrier once per pivot; the rest of the CTA waits at the final
+// __syncthreads.
+__device__ __forceinline__ void bar_sync_rows() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
+
+__device__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, DevStatus *dst, int pivot_base) {
+    const int i = threadIdx.x;
+    if (i < kNB) {
+        float a[kNB];
+#pragma unroll
+        for (int j = 0; j < kNB; ++j) a[j] = (i < nb && j < nb) ? __ldcg(D + (int64_t)j * lda + i) : 0.0f;
+#pragma unroll
+        for (int k = 0; k < kNB; ++k) {
+            if (k < nb) {  // uniform
+                if (i == k) {
+#pragma unroll
+                    for (int j = 0; j < kNB; ++j)
+                        if (j >= k) sm.t.prow[k & 1][j] = a[j];
+                }
+                bar_sync_rows();
+                const float piv = sm.t.prow[k & 1][k];
+                if (i == k && (!(piv != 0.0f) || !isfinite(piv))) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
+                if (i > k && i < nb) {
+                    const float l = a[k] * (1.0f / piv);
+                    a[k] = l;
+#pragma unroll
+                    for (int j = 0; j < kNB; ++j)
+                        if (j > k) a[j] -= l * sm.t.prow[k & 1][j];
+                }
+            }
+        }
+        if (i < nb) {
+#pragma unroll
+            for (int j = 0; j < kNB; ++j)
+                if (j < nb) D[(int64_t)j * lda + i] = a[j];
+        }
+    }
+    __syncthreads();
+}
+
+// D (nb x nb, factored) into shared memory, t[col][row], plus reciprocal diagonal.
+__device__ void load_tri(Smem &sm, int nb, const float *D, int64_t lda) {
+    for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
+        const int r = idx % kNB, c = idx / kNB;
+        sm.t.t[c][r] = (r < nb && c < nb) ? __ldcg(D + (int64_t)c * lda + r) : 0.0f;
+    }
+    __syncthreads();
+    if (threadIdx.x < nb) sm.t.dinv[threadIdx.x] = 1.0f / sm.t.t[threadIdx.x][threadIdx.x];
+    __syncthreads();
+}
+
+// L strip rows [r0, r0 + 256) of B (m x nb): X = B U^{-1}, U = upper part of sm.t.
+__device__ void trsm_rows(Smem &sm, int m, int nb, float *B, int64_t ldb, int r0) {
+    const int i = r0 + threadIdx.x;
+    if (i >= m) return;
+    float x[kNB];
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) x[c] = (c < nb) ? __ldcg(B + (int64_t)c * ldb + i) : 0.0f;
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) {
+        if (c < nb) {
+            float v = x[c];
+#pragma unroll
+            for (int k = 0; k < c; ++k) v -= sm.t.t[c][k] * x[k];
+            x[c] = v * sm.t.dinv[c];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kNB; ++c)
+        if (c < nb) B[(int64_t)c * ldb + i] = x[c];
+}
+
+// U strip columns [c0, c0 + 256) of B (nb x ncols): X = L^{-1} B, L = unit lower
+// part of sm.t; one thread per column, the column's nb values in registers.
+__device__ void trsm_cols(Smem &sm, int ncols, int nb, float *B, int64_t ldb, int c0) {
+    const int j = c0 + threadIdx.x;
+    if (j >= ncols) return;
+    float *bj = B + (int64_t)j * ldb;
+    float x[kNB];
+#pragma unroll
+    for (int k = 0; k < kNB; ++k) x[k] = (k < nb) ? __ldcg(bj + k) : 0.0f;
+#pragma unroll
+    for (int r = 1; r < kNB; ++r) {
+        if (r < nb) {
+            float v = x[r];
+#pragma unroll
+            for (int k = 0; k < r; ++k) v -= sm.t.t[k][r] * x[k];
+            x[r] = v;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kNB; ++k)
+        if (k < nb) bj[k] = x[k];
+}
+
+// U strip columns [c0, c0 + 64) of B (nb x ncols): X = L^{-1} B, L = unit lower
+// part of sm.t.  The 64 x 64 block moves through shared memory with coalesced
+// loads and stores; threads 0..63 solve one column each.
+__device__ void trsm_cols64(Smem &sm, int ncols, int nb, float *B, int64_t ldb, int c0) {
+    for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
+        const int k = idx % kNB, j = idx / kNB;
+        sm.t.ub[j][k] = (k < nb && c0 + j < ncols) ? __ldcg(B + (int64_t)(c0 + j) * ldb + k) : 0.0f;
+    }
+    __syncthreads();
+    if (threadIdx.x < kNB) {
+        const int j = threadIdx.x;
+        float x[kNB];
+#pragma unroll
+        for (int k = 0; k < kNB; ++k) x[k] = sm.t.ub[j][k];
+#pragma unroll
+        for (int r = 1; r < kNB; ++r) {
+            if (r < nb) {
+                float v = x[r];
+#pragma unroll
+                for (int k = 0; k < r; ++k) v -= sm.t.t[k][r] * x[k];
+                x[r] = v;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kNB; ++k) sm.t.ub[j][k] = x[k];
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
+        const int k = idx % kNB, j = idx / kNB;
+        if (k < nb && c0 + j < ncols) B[(int64_t)(c0 + j) * ldb + k] = sm.t.ub[j][k];
+    }
+    __syncthreads();
+}
+
+}  // namespace
+}  // namespace dt
+}  // namespace mxp

@@ -12,13 +12,14 @@
 // grid barriers:
 //
 //   LU, for each 64-column step j (D_j = diagonal 64 x 64 block):
-//     strips : L strip rows (thread per row, X = B U_jj^{-1}) and U strip
-//              columns (thread per column, X = L_jj^{-1} B) against D_j held
-//              in shared memory, items of 256 rows / columns over all CTAs;
-//     update : trailing rank-64 update in 128 x 128 SIMT tiles.  CTA 0 takes
-//              the tile holding D_{j+1} alone and factors D_{j+1} right after
-//              it (look-ahead, four threads per row), so the 64-step serial
-//              factor overlaps the rest of the update.
+//     strips : L strip rows (thread per row, X = B U_jj^{-1}, 256 rows per
+//              item) and U strip columns (thread per column, X = L_jj^{-1} B,
+//              64 columns per item staged through shared memory) against D_j
+//              held in shared memory, items spread over all CTAs;
+//     update : trailing rank-64 update in 128 x 128 SIMT tiles.  CTA 0
+//              updates only D_{j+1} (64 x 64) and factors it right away
+//              (look-ahead), so the 64-step serial factor overlaps the rest of
+//              the update; the CTA owning tile 0 skips that corner.
 //   inverses: 64 x 64 diagonal blocks of inv(U) and inv(L) one per item,
 //             then recursive doubling: for adjacent S-blocks the off-diagonal
 //             block of the inverse is -inv(A) B inv(C), two GEMM phases per
@@ -30,29 +31,14 @@
 // kWaitTimeoutNs, after which the CTA records MXP_TIMEOUT, raises the shared
 // abort word so the others leave at their next barrier, and returns.
 // All reads of data written by other CTAs go through L2 (ld.global.cg).
+#include "dense_tile.cuh"
 #include "mxp_internal.cuh"
 
 namespace mxp {
 
 namespace {
 
-constexpr int kCT = 256;  // threads per CTA
-constexpr int kNB = 64;   // inner block of the LU
-constexpr int GBM = 128, GBN = 128, GBK = 16;
-
-struct SmemGemm {
-    float As[GBK][GBM];
-    float Bs[GBK][GBN + 4];
-};
-struct SmemTri {
-    float t[kNB][kNB + 1];  // t[col][row] of a 64 x 64 block
-    float dinv[kNB];
-    float prow[2][kNB];
-};
-union __align__(16) Smem {
-    SmemGemm g;
-    SmemTri t;
-};
+using namespace dt;
 
 struct Ctl {
     unsigned int *count;  // grid-barrier arrivals (zero at launch)
@@ -100,200 +86,6 @@ __device__ bool grid_sync(const Ctl &c, unsigned int &epoch, int where) {
     }
     __syncthreads();
     return ok_sh != 0;
-}
-
-// ---- 128 x 128 SIMT GEMM tile ------------------------------------------------
-// C[m0:m0+128, n0:n0+128] (clipped to m x n) = alpha * sum_{k in [kb, ke)} A(:,k) B(k,:)
-// (+ C when accumulate).  8 x 8 outputs per thread.
-__device__ void gemm_tile(Smem &sm, int m, int n, int kb, int ke, float alpha,
-                          const float *__restrict__ A, int64_t lda, const float *__restrict__ B,
-                          int64_t ldb, bool accumulate, float *C, int64_t ldc, int m0, int n0) {
-    const int t = threadIdx.x;
-    const int tx = t % 16, ty = t / 16;
-    float acc[8][8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
-
-    float ra[8], rb[8];
-    auto load = [&](int k0) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int idx = t + kCT * q;
-            const int kk = idx / GBM, r = idx % GBM;
-            const int gr = m0 + r, gk = k0 + kk;
-            ra[q] = (gr < m && gk < ke) ? __ldcg(A + (int64_t)gk * lda + gr) : 0.0f;
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int idx = t + kCT * q;
-            const int cc = idx / GBK, kk = idx % GBK;
-            const int gc = n0 + cc, gk = k0 + kk;
-            rb[q] = (gc < n && gk < ke) ? __ldcg(B + (int64_t)gc * ldb + gk) : 0.0f;
-        }
-    };
-    if (kb < ke) load(kb);
-    for (int k0 = kb; k0 < ke; k0 += GBK) {
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int idx = t + kCT * q;
-            sm.g.As[idx / GBM][idx % GBM] = ra[q];
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int idx = t + kCT * q;
-            sm.g.Bs[idx % GBK][idx / GBK] = rb[q];
-        }
-        __syncthreads();
-        if (k0 + GBK < ke) load(k0 + GBK);
-#pragma unroll
-        for (int kk = 0; kk < GBK; ++kk) {
-            const float4 a0 = *reinterpret_cast<const float4 *>(&sm.g.As[kk][tx * 4]);
-            const float4 a1 = *reinterpret_cast<const float4 *>(&sm.g.As[kk][64 + tx * 4]);
-            const float4 b0 = *reinterpret_cast<const float4 *>(&sm.g.Bs[kk][ty * 4]);
-            const float4 b1 = *reinterpret_cast<const float4 *>(&sm.g.Bs[kk][64 + ty * 4]);
-            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
-        }
-    }
-    // C is read in full before any store: interleaved loads and stores through a
-    // pointer the compiler cannot disambiguate would serialise 64 L2 round trips
-    if (accumulate) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int gc = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int gr = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
-                acc[i][j] *= alpha;
-                if (gr < m && gc < n) acc[i][j] += __ldcg(C + (int64_t)gc * ldc + gr);
-            }
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-#pragma unroll
-            for (int i = 0; i < 8; ++i) acc[i][j] *= alpha;
-    }
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const int gc = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
-        if (gc >= n) continue;
-        float *cc = C + (int64_t)gc * ldc;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int gr = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
-            if (gr < m) cc[gr] = acc[i][j];
-        }
-    }
-    __syncthreads();  // shared tiles are reused by the caller's next item
-}
-
-// ---- 64 x 64 no-pivot LU of D (nb <= 64): four threads per row, 16 columns each ----
-// sgetrf_nopiv_naive order (sgetrf_nopiv.cpp:27-61): scale by the reciprocal
-// pivot, then the rank-1 update.  Thread (row i, quarter q) holds a(i, 16q..16q+15)
-// in registers; the four threads of a row are adjacent lanes of one warp, so the
-// multiplier is shared by a shuffle.  All CTA threads pass the barriers.
-__device__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, DevStatus *dst, int pivot_base) {
-    const int i = threadIdx.x >> 2, q = threadIdx.x & 3;
-    const int lane_base = (threadIdx.x & 31) & ~3;
-    float a[16];
-#pragma unroll
-    for (int c = 0; c < 16; ++c) {
-        const int col = q * 16 + c;
-        a[c] = (i < nb && col < nb) ? __ldcg(D + (int64_t)col * lda + i) : 0.0f;
-    }
-#pragma unroll
-    for (int k = 0; k < kNB; ++k) {
-        if (k < nb) {  // uniform across the CTA
-            const int qk = k >> 4, ck = k & 15;
-            if (i == k) {
-#pragma unroll
-                for (int c = 0; c < 16; ++c)
-                    if (q * 16 + c >= k) sm.t.prow[k & 1][q * 16 + c] = a[c];
-            }
-            __syncthreads();
-            const float piv = sm.t.prow[k & 1][k];
-            if (i == k && q == qk && (!(piv != 0.0f) || !isfinite(piv)))
-                report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
-            const float rcp = 1.0f / piv;
-            float l = (q == qk) ? a[ck] * rcp : 0.0f;
-            l = __shfl_sync(0xffffffffu, l, lane_base + qk);
-            if (i > k && i < nb) {
-                if (q == qk) a[ck] = l;
-#pragma unroll
-                for (int c = 0; c < 16; ++c)
-                    if (q * 16 + c > k) a[c] -= l * sm.t.prow[k & 1][q * 16 + c];
-            }
-        }
-    }
-    if (i < nb) {
-#pragma unroll
-        for (int c = 0; c < 16; ++c)
-            if (q * 16 + c < nb) D[(int64_t)(q * 16 + c) * lda + i] = a[c];
-    }
-    __syncthreads();
-}
-
-// D (nb x nb, factored) into shared memory, t[col][row], plus reciprocal diagonal.
-__device__ void load_tri(Smem &sm, int nb, const float *D, int64_t lda) {
-    for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
-        const int r = idx % kNB, c = idx / kNB;
-        sm.t.t[c][r] = (r < nb && c < nb) ? __ldcg(D + (int64_t)c * lda + r) : 0.0f;
-    }
-    __syncthreads();
-    if (threadIdx.x < nb) sm.t.dinv[threadIdx.x] = 1.0f / sm.t.t[threadIdx.x][threadIdx.x];
-    __syncthreads();
-}
-
-// L strip rows [r0, r0 + 256) of B (m x nb): X = B U^{-1}, U = upper part of sm.t.
-__device__ void trsm_rows(Smem &sm, int m, int nb, float *B, int64_t ldb, int r0) {
-    const int i = r0 + threadIdx.x;
-    if (i >= m) return;
-    float x[kNB];
-#pragma unroll
-    for (int c = 0; c < kNB; ++c) x[c] = (c < nb) ? __ldcg(B + (int64_t)c * ldb + i) : 0.0f;
-#pragma unroll
-    for (int c = 0; c < kNB; ++c) {
-        if (c < nb) {
-            float v = x[c];
-#pragma unroll
-            for (int k = 0; k < c; ++k) v -= sm.t.t[c][k] * x[k];
-            x[c] = v * sm.t.dinv[c];
-        }
-    }
-#pragma unroll
-    for (int c = 0; c < kNB; ++c)
-        if (c < nb) B[(int64_t)c * ldb + i] = x[c];
-}
-
-// U strip columns [c0, c0 + 256) of B (nb x ncols): X = L^{-1} B, L = unit lower
-// part of sm.t; one thread per column, the column's nb values in registers.
-__device__ void trsm_cols(Smem &sm, int ncols, int nb, float *B, int64_t ldb, int c0) {
-    const int j = c0 + threadIdx.x;
-    if (j >= ncols) return;
-    float *bj = B + (int64_t)j * ldb;
-    float x[kNB];
-#pragma unroll
-    for (int k = 0; k < kNB; ++k) x[k] = (k < nb) ? __ldcg(bj + k) : 0.0f;
-#pragma unroll
-    for (int r = 1; r < kNB; ++r) {
-        if (r < nb) {
-            float v = x[r];
-#pragma unroll
-            for (int k = 0; k < r; ++k) v -= sm.t.t[k][r] * x[k];
-            x[r] = v;
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < kNB; ++k)
-        if (k < nb) bj[k] = x[k];
 }
 
 // Inverse of the 64 x 64 diagonal block `blk` of an upper non-unit (upper = true)
@@ -392,28 +184,31 @@ diag_factor_kernel(int n, float *A, int64_t lda, float *XU, float *XL, int64_t l
         float *Lstrip = Djj + nbk;
         float *Ustrip = Djj + (int64_t)nbk * lda;
         // strips
-        const int lit = (rem + kCT - 1) / kCT, uit = (rem + kCT - 1) / kCT;
+        const int lit = (rem + kCT - 1) / kCT, uit = (rem + kNB - 1) / kNB;
         if (cta < lit + uit) {
             load_tri(sm, nbk, Djj, lda);
             for (int it = cta; it < lit + uit; it += G) {
                 if (it < lit) trsm_rows(sm, rem, nbk, Lstrip, lda, it * kCT);
-                else trsm_cols(sm, rem, nbk, Ustrip, lda, (it - lit) * kCT);
+                else trsm_cols64(sm, rem, nbk, Ustrip, lda, (it - lit) * kNB);
             }
         }
         if (!grid_sync(ctl, epoch, 21)) return;
-        // trailing rank-nbk update; CTA 0 also factors the next diagonal block
+        // trailing rank-nbk update.  CTA 0 updates only the next diagonal block
+        // (64 x 64) and factors it at once (look-ahead); the CTA owning tile 0
+        // leaves that corner alone.
         float *C = Ustrip + nbk;
         const int tm = (rem + GBM - 1) / GBM;
         const int ntiles = tm * tm;
-        if (G == 1 || cta == 0) {
-            for (int t = 0; t < (G == 1 ? ntiles : 1); ++t)
+        const int dn = min(kNB, rem);
+        if (cta == 0) {
+            gemm_tile64(sm, dn, dn, nbk, -1.0f, Lstrip, lda, Ustrip, lda, C, lda);
+            getrf64(sm, dn, C, lda, ctl.dst, pivot_base + jb + nbk);
+        }
+        if (G == 1 || cta > 0) {
+            const int first = G == 1 ? 0 : cta - 1, stride = G == 1 ? 1 : G - 1;
+            for (int t = first; t < ntiles; t += stride)
                 gemm_tile(sm, rem, rem, 0, nbk, -1.0f, Lstrip, lda, Ustrip, lda, true, C, lda,
-                          (t % tm) * GBM, (t / tm) * GBN);
-            getrf64(sm, min(kNB, rem), C, lda, ctl.dst, pivot_base + jb + nbk);
-        } else {
-            for (int t = cta; t < ntiles; t += G - 1)
-                gemm_tile(sm, rem, rem, 0, nbk, -1.0f, Lstrip, lda, Ustrip, lda, true, C, lda,
-                          (t % tm) * GBM, (t / tm) * GBN);
+                          (t % tm) * GBM, (t / tm) * GBN, t == 0 ? kNB : 0);
         }
         if (!grid_sync(ctl, epoch, 22)) return;
     }
