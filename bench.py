@@ -555,6 +555,84 @@ def run_micro(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# batched form: 2048 systems of uneven orders in one persistent launch
+# ---------------------------------------------------------------------------
+def batch_flops(sizes) -> float:
+    return sum(hpl_flops(n) for n in sizes)
+
+
+def run_batched(args):
+    """Systems/s and credited TFLOP/s of the batched solve (one graph-replayed
+    persistent launch per step), beside a per-system loop of the plain
+    single-system path (mxp_solve, FP16 Schur) over the same systems."""
+    import torch
+
+    import openmxp_b200 as mxp
+    torch.cuda.set_device(0)
+    sizes = mxp.batch_sizes(args.batch_count, args.batch_size_seed)
+    seeds = [1000 + i for i in range(len(sizes))]
+    bt = mxp.Batch(sizes, seeds)
+    bt.matgen()
+    tune = bt.autotune() if not args.batch_config else None
+    if args.batch_config:
+        b, tn, stg = (int(v) for v in args.batch_config.split(","))
+        bt.set_config(b, tn, stg)
+    flops = batch_flops(sizes)
+    for _ in range(args.warmup):
+        bt.matgen()
+        bt.solve()
+    ms = []
+    clocks = ClockSampler(0)
+    clocks.start()
+    mxp.reset_kernel_launches()
+    for _ in range(args.steps):
+        bt.matgen()
+        torch.cuda.synchronize()
+        ms.append(bt.solve()["ms_total"])
+    launches = mxp.kernel_launches()
+    clk = clocks.stop()
+    res = bt.results()
+    t = sum(ms) / len(ms) / 1e3
+    out = {"metric": "batched solve: systems/s and credited TFLOP/s", "value": len(sizes) / t,
+           "unit": "systems/s", "tflops": flops / t / 1e12, "ms_per_step": 1e3 * t,
+           "steps": args.steps, "warmup": args.warmup, "systems": len(sizes),
+           "orders": {"min": min(sizes), "max": max(sizes), "sum_n3": float(sum(n ** 3 for n in sizes))},
+           "config": tune if tune else {"b": b, "tile_n": tn, "stages": stg},
+           "converged": sum(r["converged"] for r in res), "max_iterations": max(r["iterations"] for r in res),
+           "max_hpl_harness": max(r["hpl_harness"] for r in res), "gpu_launches": launches, "clocks": clk}
+    # per-system loop of the plain single-system path on a sample of the systems
+    if args.batch_loop_sample > 0:
+        stride = max(1, len(sizes) // args.batch_loop_sample)
+        idx = list(range(0, len(sizes), stride))[: args.batch_loop_sample]
+        loop_s, loop_flops = 0.0, 0.0
+        nmax = max(sizes[i] for i in idx)
+        for i in idx:
+            n = sizes[i]
+            p = mxp.panel_matgen(n, seeds[i])
+            ws = mxp.Workspace(n, min(256, n), mxp.FORM_FP16)
+            mxp.solve(p, min(256, n), ws)  # warm
+            mxp.regenerate(p)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            mxp.solve(p, min(256, n), ws)
+            e1.record()
+            torch.cuda.synchronize()
+            loop_s += e0.elapsed_time(e1) / 1e3
+            loop_flops += hpl_flops(n)
+            ws.close()
+            del p
+        out["per_system_loop"] = {"systems_timed": len(idx), "systems_per_s": len(idx) / loop_s,
+                                  "tflops": loop_flops / loop_s / 1e12,
+                                  "what": "mxp_solve (FP16 Schur, B=min(256,n), classic IR) one system at a time"}
+        out["speedup_vs_loop"] = out["value"] / out["per_system_loop"]["systems_per_s"]
+    bt.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def parse(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -580,6 +658,13 @@ def parse(argv=None):
                     help="time one kernel alone at m=--n, k=--b (for profiler captures)")
     ap.add_argument("--micro-seconds", type=float, default=0.0,
                     help="micro: run the launch this long before timing (sustained clocks)")
+    ap.add_argument("--batched", action="store_true",
+                    help="the batched form: --batch-count systems of orders 128*{2..32}")
+    ap.add_argument("--batch-count", type=int, default=2048)
+    ap.add_argument("--batch-size-seed", type=int, default=3)
+    ap.add_argument("--batch-config", default="", help="b,tile_n,stages (default: autotune)")
+    ap.add_argument("--batch-loop-sample", type=int, default=128,
+                    help="systems timed through the per-system loop for comparison")
     ap.add_argument("--distinct-seeds", action="store_true",
                     help="rank r solves seed+r instead of the same system")
     return ap.parse_args(argv)
@@ -593,6 +678,8 @@ def main(argv=None):
         return run_reference(args)
     if args.micro:
         return run_micro(args)
+    if args.batched:
+        return run_batched(args)
     return run_gpu(args)
 
 
