@@ -621,7 +621,8 @@ struct mxp_batch {
     int64_t staging_stride = 0, rstage_off = 0;
     BatchConfig cfg;
     int autotuned = 0;
-    // captured launch
+    // captured launch (captured on a private stream, replayed on the caller's)
+    cudaStream_t cap = nullptr;
     cudaGraphExec_t exec = nullptr;
     const void *g_A = nullptr, *g_d = nullptr, *g_rhs = nullptr, *g_x = nullptr;
     int g_maxit = -1, g_b = -1, g_tn = -1, g_st = -1, g_count = -1;
@@ -767,7 +768,8 @@ extern "C" mxp_status mxp_batch_create(int count, const int *h_n, const uint64_t
               cudaMalloc(&bt->d_sys_status, sizeof(DevStatus) * count) == cudaSuccess &&
               cudaMalloc(&bt->d_status, sizeof(DevStatus)) == cudaSuccess &&
               cudaMalloc(&bt->d_ticket, 256) == cudaSuccess &&
-              cudaMalloc(&bt->d_staging, (size_t)bt->staging_stride * bt->grid) == cudaSuccess;
+              cudaMalloc(&bt->d_staging, (size_t)bt->staging_stride * bt->grid) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&bt->cap, cudaStreamNonBlocking) == cudaSuccess;
     if (ok)
         ok = cudaMemcpy(bt->d_sys, hs.data(), sizeof(BatchSys) * count, cudaMemcpyHostToDevice) == cudaSuccess &&
              cudaMemcpy(bt->d_order, bt->order.data(), sizeof(int) * count, cudaMemcpyHostToDevice) == cudaSuccess &&
@@ -792,6 +794,7 @@ extern "C" mxp_status mxp_batch_destroy(mxp_batch *bt) {
     cudaFree(bt->d_status);
     cudaFree(bt->d_ticket);
     cudaFree(bt->d_staging);
+    if (bt->cap) cudaStreamDestroy(bt->cap);
     delete bt;
     return MXP_OK;
 }
@@ -845,9 +848,9 @@ extern "C" mxp_status mxp_batch_solve(mxp_batch *bt, float *d_A, const double *d
         mxp_status sa = set_smem_attr(bt, c);
         if (sa != MXP_OK) return sa;
         cudaGraph_t g = nullptr;
-        MXP_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        mxp_status s = launch_batch(bt, c, bt->count, bt->d_order, d_A, d_d, d_rhs, d_x, maxit, st);
-        cudaError_t e = cudaStreamEndCapture(st, &g);
+        MXP_CUDA(cudaStreamBeginCapture(bt->cap, cudaStreamCaptureModeThreadLocal));
+        mxp_status s = launch_batch(bt, c, bt->count, bt->d_order, d_A, d_d, d_rhs, d_x, maxit, bt->cap);
+        cudaError_t e = cudaStreamEndCapture(bt->cap, &g);
         if (s != MXP_OK) {
             if (g) cudaGraphDestroy(g);
             return s;
