@@ -304,7 +304,7 @@ mxp_status mxp_batch_layout(const mxp_batch *bt, int64_t *matrix_floats, int64_t
 /* panel_matgen_dev + panel_colvgen for every system (matgen.hpp:84-117, 419-436) */
 mxp_status mxp_batch_matgen(mxp_batch *bt, float *d_A, double *d_d, double *d_rhs, void *stream);
 /* block size b in {64, 128, 256}, Schur tile width tile_n in {128, 256}, smem
- * pipeline depth stages in 2..4 (default 128 / 256 / 4) */
+ * pipeline depth stages in 2..4 within 227 KB of shared memory (default 128 / 256 / 3) */
 mxp_status mxp_batch_set_config(mxp_batch *bt, int b, int tile_n, int stages);
 /* times every admissible configuration on `sample` systems (0: an eighth of
  * the batch, spread over the sizes; those matrices are regenerated and

@@ -126,10 +126,47 @@ __device__ __forceinline__ void stage_zero_row(uint8_t *base, int nblk, int row,
     }
 }
 
+// U-strip columns [c0, c0 + 256) of B (nb x ncols): X = L^{-1} B with L the unit
+// lower part of sm.t.  The 64 x 256 block goes through shared memory (stage:
+// 256 x 65 floats) with coalesced loads and stores; thread j solves column j.
+constexpr size_t kColStageOff = 36864;  // after the Smem union
+constexpr size_t kColStageBytes = sizeof(float) * kCT * (kNB + 1);
+
+__device__ void trsm_cols_staged(Smem &sm, float *stage, int ncols, int nb, float *B, int64_t ldb, int c0) {
+    for (int idx = threadIdx.x; idx < kNB * kCT; idx += kCT) {
+        const int k = idx % kNB, j = idx / kNB;
+        stage[j * (kNB + 1) + k] = (k < nb && c0 + j < ncols) ? __ldcg(B + (int64_t)(c0 + j) * ldb + k) : 0.0f;
+    }
+    __syncthreads();
+    {
+        const int j = threadIdx.x;
+        float x[kNB];
+#pragma unroll
+        for (int k = 0; k < kNB; ++k) x[k] = stage[j * (kNB + 1) + k];
+#pragma unroll
+        for (int r = 1; r < kNB; ++r) {
+            if (r < nb) {
+                float v = x[r];
+#pragma unroll
+                for (int k = 0; k < r; ++k) v -= sm.t.t[k][r] * x[k];
+                x[r] = v;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kNB; ++k) stage[j * (kNB + 1) + k] = x[k];
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kNB * kCT; idx += kCT) {
+        const int k = idx % kNB, j = idx / kNB;
+        if (k < nb && c0 + j < ncols) B[(int64_t)(c0 + j) * ldb + k] = stage[j * (kNB + 1) + k];
+    }
+    __syncthreads();
+}
+
 // ---- panel factorisation of one block step (SIMT FP32, whole CTA) -----------
 // D = A(k0, k0) (bk x bk), L strip = A(k0+bk.., k0..) (m x bk), U strip =
 // A(k0.., k0+bk..) (bk x m); lda = n.
-__device__ void factor_step(Smem &sm, float *A, int n, int k0, int bk, DevStatus *dst) {
+__device__ void factor_step(Smem &sm, float *stage, float *A, int n, int k0, int bk, DevStatus *dst) {
     const int64_t lda = n;
     float *D = A + k0 + (int64_t)k0 * lda;
     const int m = n - k0 - bk;
@@ -141,7 +178,7 @@ __device__ void factor_step(Smem &sm, float *A, int n, int k0, int bk, DevStatus
         if (rem <= 0) break;
         load_tri(sm, kNB, Dj, lda);
         for (int r0 = 0; r0 < rem; r0 += kCT) trsm_rows(sm, rem, kNB, Dj + kNB, lda, r0);
-        for (int c0 = 0; c0 < rem; c0 += kCT) trsm_cols(sm, rem, kNB, Dj + (int64_t)kNB * lda, lda, c0);
+        for (int c0 = 0; c0 < rem; c0 += kCT) trsm_cols_staged(sm, stage, rem, kNB, Dj + (int64_t)kNB * lda, lda, c0);
         __syncthreads();
         const int tm = (rem + GBM - 1) / GBM;
         for (int t = 0; t < tm * tm; ++t)
@@ -168,7 +205,7 @@ __device__ void factor_step(Smem &sm, float *A, int n, int k0, int bk, DevStatus
     // U strip: L X = B, one 64-row block at a time
     for (int c = 0; c < bk; c += kNB) {
         load_tri(sm, kNB, D + c + (int64_t)c * lda, lda);
-        for (int c0 = 0; c0 < m; c0 += kCT) trsm_cols(sm, m, kNB, Us + c, lda, c0);
+        for (int c0 = 0; c0 < m; c0 += kCT) trsm_cols_staged(sm, stage, m, kNB, Us + c, lda, c0);
         __syncthreads();
         const int rest = bk - c - kNB;
         if (rest > 0) {
@@ -188,6 +225,7 @@ __device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void *src, uin
 }
 
 struct Ring {
+    float *cbuf;            // epilogue staging of C: 128 columns x 128 rows
     uint8_t *sA;            // stages x 16 KB
     uint8_t *sB;            // stages x TN x 128 B
     uint64_t *full, *empty; // per stage
@@ -284,28 +322,41 @@ __device__ bool schur_step(const Ring &rg, RoleState &rs, volatile int *abort_fl
             }
             __syncwarp();
             tc_fence_after();
-            const int row = rt * kRowTile + quarter * 32 + lane;
+            const int r = quarter * 32 + lane;  // row within the tile
+            const int row = rt * kRowTile + r;
             const uint32_t tbase = rg.tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(rs.acc * TN);
 #pragma unroll 1
-            for (int g = 0; g < TN / 64; ++g) {
-                uint32_t r0[32], r1[32];
-                tmem_ld_32x32b_x32(tbase + g * 64, r0);
-                tmem_ld_32x32b_x32(tbase + g * 64 + 32, r1);
-                if (g == TN / 64 - 1) {  // accumulator drained: the next tile may use it
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(smem_u32(&rg.tempty[rs.acc]));
-                }
-                const int col0 = ct * TN + g * 64;
+            for (int h = 0; h < TN / 128; ++h) {
+                // C for 128 columns of this row -> shared memory with async copies (the
+                // bytes in flight are not bounded by registers), then subtract the
+                // accumulator column by column and store
+                const int colh = ct * TN + h * 128;
                 if (row < m) {
-                    float *cp = C + (int64_t)col0 * ldc + row;
-                    float cv[64];
+                    const float *cp = C + (int64_t)colh * ldc + row;
+#pragma unroll 8
+                    for (int j = 0; j < 128; ++j)
+                        if (colh + j < m)
+                            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(rg.cbuf + j * 128 + r)),
+                                         "l"(cp + (int64_t)j * ldc)
+                                         : "memory");
+                }
+                asm volatile("cp.async.commit_group;" ::: "memory");
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
+#pragma unroll 1
+                for (int c = 0; c < 4; ++c) {
+                    uint32_t v[32];
+                    tmem_ld_32x32b_x32(tbase + h * 128 + c * 32, v);
+                    if (h == TN / 128 - 1 && c == 3) {  // accumulator drained: the next tile may use it
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(smem_u32(&rg.tempty[rs.acc]));
+                    }
+                    if (row < m) {
+                        float *cp = C + (int64_t)(colh + c * 32) * ldc + row;
 #pragma unroll
-                    for (int j = 0; j < 64; ++j) cv[j] = (col0 + j < m) ? __ldcs(cp + (int64_t)j * ldc) : 0.0f;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        if (col0 + j < m) __stcs(cp + (int64_t)j * ldc, cv[j] - __uint_as_float(r0[j]));
-                        if (col0 + 32 + j < m) __stcs(cp + (int64_t)(32 + j) * ldc, cv[32 + j] - __uint_as_float(r1[j]));
+                        for (int j = 0; j < 32; ++j)
+                            if (colh + c * 32 + j < m)
+                                __stcs(cp + (int64_t)j * ldc, rg.cbuf[(c * 32 + j) * 128 + r] - __uint_as_float(v[j]));
                     }
                 }
             }
@@ -371,19 +422,26 @@ __device__ void otf_residual(int n, uint64_t seed, const double *__restrict__ d,
 // 64-row blocks, the diagonal block solved in FP64 by one warp, the block's
 // column panel applied to the remaining rows by all threads (the block
 // substitution of panel_trsv.hpp:601-747).
-__device__ void lu_solve_shared(int n, const float *__restrict__ LU, double *r) {
+__device__ void lu_solve_shared(int n, const float *__restrict__ LU, double *r, float (*tri)[kNB + 1]) {
     const int64_t lda = n;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nb = n / kNB;
+    auto load_diag = [&](int c0) {  // tri[col][row] of the 64 x 64 diagonal block, coalesced
+        for (int idx = threadIdx.x; idx < kNB * kNB; idx += kBatchThreads) {
+            const int rr = idx % kNB, cc = idx / kNB;
+            tri[cc][rr] = LU[(int64_t)(c0 + cc) * lda + c0 + rr];
+        }
+        __syncthreads();
+    };
     for (int blk = 0; blk < nb; ++blk) {  // forward, unit lower
         const int c0 = blk * kNB;
+        load_diag(c0);
         if (warp == 0) {
             double z0 = r[c0 + lane], z1 = r[c0 + 32 + lane];
             for (int k = 0; k < kNB; ++k) {
                 const double zk = __shfl_sync(0xffffffffu, k < 32 ? z0 : z1, k & 31);
-                const float *col = LU + (int64_t)(c0 + k) * lda + c0;
-                if (lane > k) z0 -= (double)__ldg(col + lane) * zk;
-                if (lane + 32 > k) z1 -= (double)__ldg(col + lane + 32) * zk;
+                if (lane > k) z0 -= (double)tri[k][lane] * zk;
+                if (lane + 32 > k) z1 -= (double)tri[k][lane + 32] * zk;
             }
             r[c0 + lane] = z0;
             r[c0 + 32 + lane] = z1;
@@ -391,7 +449,7 @@ __device__ void lu_solve_shared(int n, const float *__restrict__ LU, double *r) 
         __syncthreads();
         for (int i = c0 + kNB + threadIdx.x; i < n; i += kBatchThreads) {
             double acc = 0.0;
-#pragma unroll 8
+#pragma unroll 16
             for (int k = 0; k < kNB; ++k) acc = __fma_rn((double)__ldg(LU + (int64_t)(c0 + k) * lda + i), r[c0 + k], acc);
             r[i] -= acc;
         }
@@ -399,19 +457,19 @@ __device__ void lu_solve_shared(int n, const float *__restrict__ LU, double *r) 
     }
     for (int blk = nb - 1; blk >= 0; --blk) {  // backward, upper non-unit
         const int c0 = blk * kNB;
+        load_diag(c0);
         if (warp == 0) {
             double z0 = r[c0 + lane], z1 = r[c0 + 32 + lane];
             for (int k = kNB - 1; k >= 0; --k) {
-                const float *col = LU + (int64_t)(c0 + k) * lda + c0;
-                const double dk = (double)__ldg(col + k);
+                const double rdk = 1.0 / (double)tri[k][k];
                 if (k < 32) {
-                    if (lane == k) z0 = z0 / dk;
+                    if (lane == k) z0 = z0 * rdk;
                 } else if (lane + 32 == k) {
-                    z1 = z1 / dk;
+                    z1 = z1 * rdk;
                 }
                 const double zk = __shfl_sync(0xffffffffu, k < 32 ? z0 : z1, k & 31);
-                if (lane < k) z0 -= (double)__ldg(col + lane) * zk;
-                if (lane + 32 < k) z1 -= (double)__ldg(col + lane + 32) * zk;
+                if (lane < k) z0 -= (double)tri[k][lane] * zk;
+                if (lane + 32 < k) z1 -= (double)tri[k][lane + 32] * zk;
             }
             r[c0 + lane] = z0;
             r[c0 + 32 + lane] = z1;
@@ -419,7 +477,7 @@ __device__ void lu_solve_shared(int n, const float *__restrict__ LU, double *r) 
         __syncthreads();
         for (int i = threadIdx.x; i < c0; i += kBatchThreads) {
             double acc = 0.0;
-#pragma unroll 8
+#pragma unroll 16
             for (int k = 0; k < kNB; ++k) acc = __fma_rn((double)__ldg(LU + (int64_t)(c0 + k) * lda + i), r[c0 + k], acc);
             r[i] -= acc;
         }
@@ -430,7 +488,7 @@ __device__ void lu_solve_shared(int n, const float *__restrict__ LU, double *r) 
 // Classic refinement of iterative_refinement.hpp:141-171 for one system whose
 // factors are in A; returns the number of corrections applied.
 __device__ void refine_system(int n, uint64_t seed, const float *A, const double *d, const double *b, double *x,
-                              int maxit, double *xs, double *rs, double *red, BatchOut *out) {
+                              int maxit, double *xs, double *rs, double *red, float (*tri)[kNB + 1], BatchOut *out) {
     double mb = 0.0, md = 0.0;
     for (int i = threadIdx.x; i < n; i += kBatchThreads) {
         mb = fmax(mb, fabs(b[i]));
@@ -454,7 +512,7 @@ __device__ void refine_system(int n, uint64_t seed, const float *A, const double
         const double normx = block_max(mx, red);
         hpl = normr / (norma * normx + normb) * 1.0 / ((double)n * eps);
         if (!(hpl < 16.0) && isfinite(hpl)) {
-            lu_solve_shared(n, A, rs);
+            lu_solve_shared(n, A, rs, tri);
             for (int i = threadIdx.x; i < n; i += kBatchThreads) xs[i] += rs[i];
             __syncthreads();
             continue;
@@ -517,6 +575,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batched_kernel(BatchKernelAr
     Ring rg;
     rg.sA = smem;
     rg.sB = smem + (size_t)a.stages * kBlockBytes;
+    rg.cbuf = reinterpret_cast<float *>(rg.sB + (size_t)a.stages * TN * 128);
     rg.full = bar_full;
     rg.empty = bar_empty;
     rg.tfull = bar_tfull;
@@ -525,6 +584,8 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batched_kernel(BatchKernelAr
     rg.stages = a.stages;
     RoleState rs;
     Smem &sm = *reinterpret_cast<Smem *>(smem);  // SIMT phases reuse the ring's memory
+    float *colstage = reinterpret_cast<float *>(smem + kColStageOff);
+    static_assert(sizeof(Smem) <= kColStageOff, "column stage overlaps the SIMT scratch");
     uint8_t *Lst = a.staging + (int64_t)blockIdx.x * a.staging_stride;
     uint8_t *Rst = Lst + a.rstage_off;
 
@@ -542,7 +603,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batched_kernel(BatchKernelAr
         // ---------------- LU ----------------
         for (int k0 = 0; k0 < n && !abort_flag; k0 += a.b) {
             const int bk = min(a.b, n - k0);
-            factor_step(sm, A, n, k0, bk, sst);
+            factor_step(sm, colstage, A, n, k0, bk, sst);
             const int m = n - k0 - bk;
             if (m <= 0) break;
             const int mp = (m + kRowTile - 1) / kRowTile * kRowTile;
@@ -573,7 +634,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batched_kernel(BatchKernelAr
         double *xs = reinterpret_cast<double *>(smem);
         double *rsv = xs + n;
         refine_system(n, S.seed, A, a.d + S.v_off, a.rhs + S.v_off, a.x + S.v_off, a.maxit, xs, rsv, red,
-                      a.out + si);
+                      reinterpret_cast<float(*)[kNB + 1]>(rsv + n), a.out + si);
         if (threadIdx.x == 0) a.out[si].info = sst->code == MXP_ZERO_PIVOT ? sst->info0 : 0;
     }
 
@@ -597,7 +658,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batched_kernel(BatchKernelAr
 // host side
 // ---------------------------------------------------------------------------------
 struct BatchConfig {
-    int b = 128, tile_n = 256, stages = 4;
+    int b = 128, tile_n = 256, stages = 3;
 };
 
 }  // namespace mxp
@@ -635,10 +696,12 @@ constexpr int kBatchMaxN = 8192;
 
 size_t ring_bytes(int tile_n, int stages) { return (size_t)stages * (kBlockBytes + (size_t)tile_n * 128); }
 
+constexpr size_t kCbufBytes = 128 * 128 * 4;  // epilogue staging of C
+
 size_t smem_bytes(const mxp_batch *bt, const BatchConfig &c) {
-    size_t s = ring_bytes(c.tile_n, c.stages);
-    s = std::max(s, (size_t)16 * bt->nmax);   // refinement vectors x, r (FP64)
-    s = std::max(s, sizeof(Smem));
+    size_t s = ring_bytes(c.tile_n, c.stages) + kCbufBytes;
+    s = std::max(s, (size_t)16 * bt->nmax + sizeof(float) * kNB * (kNB + 1));  // x, r (FP64) + a 64 x 64 block
+    s = std::max(s, kColStageOff + kColStageBytes);
     return s + 1024;                          // 1024-byte alignment of the ring
 }
 

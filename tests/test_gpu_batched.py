@@ -27,7 +27,7 @@ def _check_system(orc, bt, i, b, factors=True):
     assert np.max(np.abs(x - x64)) / np.max(np.abs(x64)) < 1e-10
 
 
-@pytest.mark.parametrize("b,tile_n,stages", [(64, 256, 4), (128, 256, 4), (128, 128, 2), (256, 256, 3),
+@pytest.mark.parametrize("b,tile_n,stages", [(64, 256, 3), (128, 256, 3), (128, 128, 2), (256, 256, 2),
                                              (256, 128, 4)])
 def test_batched_factors_and_solutions(mxp, orc, torch_cuda, b, tile_n, stages):
     sizes = [n for n in (256, 512, 768, 1024, 1280, 512, 2048) if n % b == 0]
@@ -47,7 +47,7 @@ def test_batched_ragged_blocks_and_small_orders(mxp, orc, torch_cuda):
     """Orders that are not multiples of the block size (a short last block)."""
     sizes = [128, 384, 640, 896, 1152]
     bt = mxp.Batch(sizes, [77 + i for i in range(len(sizes))])
-    bt.set_config(256, 256, 4)
+    bt.set_config(256, 256, 3)
     bt.matgen()
     bt.solve()
     for i, r in enumerate(bt.results()):
