@@ -76,6 +76,7 @@ typedef struct {
     int gemv_calls, trsv_calls;
     int inner_iterations; /* GMRES Arnoldi steps over all corrections (0 for classic) */
     double history[64];  /* scaled residual of every evaluation */
+    double history_residual[64];  /* ||b - A x||_inf of every evaluation */
 } mxp_ir_stats;
 
 typedef struct mxp_workspace mxp_workspace;

@@ -46,10 +46,11 @@ class IrStats(C.Structure):
                 ("hpl_harness", C.c_double), ("norma", C.c_double), ("normb", C.c_double),
                 ("normx", C.c_double), ("ms_total", C.c_double), ("ms_gemv", C.c_double),
                 ("ms_trsv", C.c_double), ("gemv_calls", C.c_int), ("trsv_calls", C.c_int),
-                ("inner_iterations", C.c_int), ("history", C.c_double * 64)]
+                ("inner_iterations", C.c_int), ("history", C.c_double * 64),
+                ("history_residual", C.c_double * 64)]
 
     def as_dict(self):
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "history"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("history")}
         d["history"] = [self.history[i] for i in range(min(64, self.iterations + 1))]
         return d
 

@@ -64,9 +64,29 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
+    build_cli()
     if verbose:
         print("built", LIB)
     return LIB
+
+
+CLI_SRC = os.path.join(PKG, "cli", "mxp_main.cpp")
+CLI = os.path.join(PKG, "mxp")
+
+
+def build_cli() -> str:
+    """The `mxp` command-line driver (C++ over the C ABI), linked to libmxp.so."""
+    deps = [CLI_SRC, LIB, os.path.join(ROOT, "include", "mxp.h")]
+    if os.path.exists(CLI) and all(os.path.getmtime(CLI) >= os.path.getmtime(d) for d in deps):
+        return CLI
+    cmd = [nvcc(), "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), CLI_SRC, "-o", CLI + ".tmp",
+           "-L", PKG, "-lmxp", "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN", "-lcudart_static", "-ldl",
+           "-lpthread", "-lrt"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"CLI build failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
 
 
 if __name__ == "__main__":

@@ -709,7 +709,10 @@ extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float
         normx = h[0];
         normr = h[1];
         hpl = normr / (norma * normx + normb) * 1.0 / ((double)n * eps);
-        if (stats && it < 64) stats->history[it] = hpl;
+        if (stats && it < 64) {
+            stats->history[it] = hpl;
+            stats->history_residual[it] = normr;
+        }
         if (!std::isfinite(hpl)) {
             s = fail(MXP_NONFINITE, "IR: non-finite residual");
             break;
