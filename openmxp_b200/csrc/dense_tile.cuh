@@ -20,11 +20,13 @@ struct SmemGemm {
     float As[GBK][GBM];
     float Bs[GBK][GBN + 4];
 };
-struct SmemTri {
-    float t[kNB][kNB + 1];   // t[col][row] of a 64 x 64 block
+struct __align__(16) SmemTri {
+    float t[kNB][kNB + 4];   // t[col][row] of a 64 x 64 block (16-byte rows)
+    float tt[kNB][kNB + 4];  // tt[row][col]: the same block row-major
     float ub[kNB][kNB + 1];  // staging of 64 U-strip columns, ub[col][row]
+    float prow[2][kNB];      // pivot row of the 64 x 64 LU, zero left of the pivot
     float dinv[kNB];
-    float prow[2][kNB];
+    float pivv[2];
 };
 union __align__(16) Smem {
     SmemGemm g;
@@ -202,20 +204,34 @@ __device__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, DevStatus *dst,
 #pragma unroll
         for (int k = 0; k < kNB; ++k) {
             if (k < nb) {  // uniform
-                if (i == k) {
+                float *pr = sm.t.prow[k & 1];
+                if (i == k) {  // publish the pivot row, zero at and left of the pivot
 #pragma unroll
-                    for (int j = 0; j < kNB; ++j)
-                        if (j >= k) sm.t.prow[k & 1][j] = a[j];
+                    for (int j4 = k / 4; j4 < kNB / 4; ++j4) {
+                        float4 v;
+                        v.x = (4 * j4 + 0 > k) ? a[4 * j4 + 0] : 0.0f;
+                        v.y = (4 * j4 + 1 > k) ? a[4 * j4 + 1] : 0.0f;
+                        v.z = (4 * j4 + 2 > k) ? a[4 * j4 + 2] : 0.0f;
+                        v.w = (4 * j4 + 3 > k) ? a[4 * j4 + 3] : 0.0f;
+                        *reinterpret_cast<float4 *>(pr + 4 * j4) = v;
+                    }
+                    sm.t.pivv[k & 1] = a[k];
                 }
                 bar_sync_rows();
-                const float piv = sm.t.prow[k & 1][k];
+                const float piv = sm.t.pivv[k & 1];
                 if (i == k && (!(piv != 0.0f) || !isfinite(piv))) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
-                if (i > k && i < nb) {
-                    const float l = a[k] * (1.0f / piv);
-                    a[k] = l;
+                const bool act = i > k && i < nb;
+                const float l = act ? a[k] * __frcp_rn(piv) : 0.0f;
+                if (act) a[k] = l;
+                // a(i, j) -= l * u(k, j) for j > k; the zeros of the published row
+                // leave columns <= k untouched (and rows <= k have l = 0)
 #pragma unroll
-                    for (int j = 0; j < kNB; ++j)
-                        if (j > k) a[j] -= l * sm.t.prow[k & 1][j];
+                for (int j4 = k / 4; j4 < kNB / 4; ++j4) {
+                    const float4 p = *reinterpret_cast<const float4 *>(pr + 4 * j4);
+                    if (4 * j4 + 0 > k) a[4 * j4 + 0] = fmaf(-l, p.x, a[4 * j4 + 0]);
+                    if (4 * j4 + 1 > k) a[4 * j4 + 1] = fmaf(-l, p.y, a[4 * j4 + 1]);
+                    if (4 * j4 + 2 > k) a[4 * j4 + 2] = fmaf(-l, p.z, a[4 * j4 + 2]);
+                    if (4 * j4 + 3 > k) a[4 * j4 + 3] = fmaf(-l, p.w, a[4 * j4 + 3]);
                 }
             }
         }
@@ -232,55 +248,43 @@ __device__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, DevStatus *dst,
 __device__ void load_tri(Smem &sm, int nb, const float *D, int64_t lda) {
     for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
         const int r = idx % kNB, c = idx / kNB;
-        sm.t.t[c][r] = (r < nb && c < nb) ? __ldcg(D + (int64_t)c * lda + r) : 0.0f;
+        const float v = (r < nb && c < nb) ? __ldcg(D + (int64_t)c * lda + r) : 0.0f;
+        sm.t.t[c][r] = v;
+        sm.t.tt[r][c] = v;
     }
     __syncthreads();
     if (threadIdx.x < nb) sm.t.dinv[threadIdx.x] = 1.0f / sm.t.t[threadIdx.x][threadIdx.x];
     __syncthreads();
 }
 
-// L strip rows [r0, r0 + 256) of B (m x nb): X = B U^{-1}, U = upper part of sm.t.
-__device__ void trsm_rows(Smem &sm, int m, int nb, float *B, int64_t ldb, int r0) {
+// L strip rows [r0, r0 + rows) of B (m x nb), rows <= kCT: X = B U^{-1}, U =
+// upper part of the diagonal block in sm.t.  Right-looking (x_k final, then
+// x_c -= u_kc x_k for c > k): per element the same operations in the same
+// order as the dot-product form, with independent updates instead of one
+// dependent chain per row; u_k. is read four at a time from the row-major copy.
+__device__ void trsm_rows(Smem &sm, int m, int nb, float *B, int64_t ldb, int r0, int rows = kCT) {
     const int i = r0 + threadIdx.x;
-    if (i >= m) return;
+    if (threadIdx.x >= rows || i >= m) return;
     float x[kNB];
 #pragma unroll
     for (int c = 0; c < kNB; ++c) x[c] = (c < nb) ? __ldcg(B + (int64_t)c * ldb + i) : 0.0f;
 #pragma unroll
-    for (int c = 0; c < kNB; ++c) {
-        if (c < nb) {
-            float v = x[c];
+    for (int k = 0; k < kNB; ++k) {
+        if (k < nb) {
+            x[k] *= sm.t.dinv[k];
 #pragma unroll
-            for (int k = 0; k < c; ++k) v -= sm.t.t[c][k] * x[k];
-            x[c] = v * sm.t.dinv[c];
+            for (int c4 = (k + 1) / 4; c4 < kNB / 4; ++c4) {
+                const float4 u = *reinterpret_cast<const float4 *>(&sm.t.tt[k][4 * c4]);
+                if (4 * c4 + 0 > k) x[4 * c4 + 0] = fmaf(-u.x, x[k], x[4 * c4 + 0]);
+                if (4 * c4 + 1 > k) x[4 * c4 + 1] = fmaf(-u.y, x[k], x[4 * c4 + 1]);
+                if (4 * c4 + 2 > k) x[4 * c4 + 2] = fmaf(-u.z, x[k], x[4 * c4 + 2]);
+                if (4 * c4 + 3 > k) x[4 * c4 + 3] = fmaf(-u.w, x[k], x[4 * c4 + 3]);
+            }
         }
     }
 #pragma unroll
     for (int c = 0; c < kNB; ++c)
         if (c < nb) B[(int64_t)c * ldb + i] = x[c];
-}
-
-// U strip columns [c0, c0 + 256) of B (nb x ncols): X = L^{-1} B, L = unit lower
-// part of sm.t; one thread per column, the column's nb values in registers.
-__device__ void trsm_cols(Smem &sm, int ncols, int nb, float *B, int64_t ldb, int c0) {
-    const int j = c0 + threadIdx.x;
-    if (j >= ncols) return;
-    float *bj = B + (int64_t)j * ldb;
-    float x[kNB];
-#pragma unroll
-    for (int k = 0; k < kNB; ++k) x[k] = (k < nb) ? __ldcg(bj + k) : 0.0f;
-#pragma unroll
-    for (int r = 1; r < kNB; ++r) {
-        if (r < nb) {
-            float v = x[r];
-#pragma unroll
-            for (int k = 0; k < r; ++k) v -= sm.t.t[k][r] * x[k];
-            x[r] = v;
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < kNB; ++k)
-        if (k < nb) bj[k] = x[k];
 }
 
 // U strip columns [c0, c0 + 64) of B (nb x ncols): X = L^{-1} B, L = unit lower
@@ -292,18 +296,22 @@ __device__ void trsm_cols64(Smem &sm, int ncols, int nb, float *B, int64_t ldb, 
         sm.t.ub[j][k] = (k < nb && c0 + j < ncols) ? __ldcg(B + (int64_t)(c0 + j) * ldb + k) : 0.0f;
     }
     __syncthreads();
-    if (threadIdx.x < kNB) {
+    if (threadIdx.x < kNB) {  // right-looking: x_r -= l_rk x_k for r > k (l_.k contiguous in sm.t)
         const int j = threadIdx.x;
         float x[kNB];
 #pragma unroll
         for (int k = 0; k < kNB; ++k) x[k] = sm.t.ub[j][k];
 #pragma unroll
-        for (int r = 1; r < kNB; ++r) {
-            if (r < nb) {
-                float v = x[r];
+        for (int k = 0; k < kNB - 1; ++k) {
+            if (k < nb) {
 #pragma unroll
-                for (int k = 0; k < r; ++k) v -= sm.t.t[k][r] * x[k];
-                x[r] = v;
+                for (int r4 = (k + 1) / 4; r4 < kNB / 4; ++r4) {
+                    const float4 l = *reinterpret_cast<const float4 *>(&sm.t.t[k][4 * r4]);
+                    if (4 * r4 + 0 > k) x[4 * r4 + 0] = fmaf(-l.x, x[k], x[4 * r4 + 0]);
+                    if (4 * r4 + 1 > k) x[4 * r4 + 1] = fmaf(-l.y, x[k], x[4 * r4 + 1]);
+                    if (4 * r4 + 2 > k) x[4 * r4 + 2] = fmaf(-l.z, x[k], x[4 * r4 + 2]);
+                    if (4 * r4 + 3 > k) x[4 * r4 + 3] = fmaf(-l.w, x[k], x[4 * r4 + 3]);
+                }
             }
         }
 #pragma unroll

@@ -12,10 +12,10 @@
 // grid barriers:
 //
 //   LU, for each 64-column step j (D_j = diagonal 64 x 64 block):
-//     strips : L strip rows (thread per row, X = B U_jj^{-1}, 256 rows per
-//              item) and U strip columns (thread per column, X = L_jj^{-1} B,
-//              64 columns per item staged through shared memory) against D_j
-//              held in shared memory, items spread over all CTAs;
+//     strips : L strip rows (thread per row, X = B U_jj^{-1}) and U strip
+//              columns (thread per column, X = L_jj^{-1} B, staged through
+//              shared memory), 64 per item, right-looking against D_j held in
+//              shared memory, items spread over all CTAs;
 //     update : trailing rank-64 update in 128 x 128 SIMT tiles.  CTA 0
 //              updates only D_{j+1} (64 x 64) and factors it right away
 //              (look-ahead), so the 64-step serial factor overlaps the rest of
@@ -167,7 +167,8 @@ __device__ void run_jobs(Smem &sm, const Job *jobs, int njobs, int cta, int ncta
 __global__ void __launch_bounds__(kCT, 1)
 diag_factor_kernel(int n, float *A, int64_t lda, float *XU, float *XL, int64_t ldx, float *tmpU,
                    float *tmpL, Ctl ctl, int pivot_base) {
-    __shared__ Smem sm;
+    extern __shared__ __align__(16) unsigned char coop_smem[];
+    Smem &sm = *reinterpret_cast<Smem *>(coop_smem);
     const int G = gridDim.x, cta = blockIdx.x;
     unsigned int epoch = 0;
     const int nsteps = (n + kNB - 1) / kNB;
@@ -184,11 +185,11 @@ diag_factor_kernel(int n, float *A, int64_t lda, float *XU, float *XL, int64_t l
         float *Lstrip = Djj + nbk;
         float *Ustrip = Djj + (int64_t)nbk * lda;
         // strips
-        const int lit = (rem + kCT - 1) / kCT, uit = (rem + kNB - 1) / kNB;
+        const int lit = (rem + kNB - 1) / kNB, uit = (rem + kNB - 1) / kNB;  // 64-row / 64-column items
         if (cta < lit + uit) {
             load_tri(sm, nbk, Djj, lda);
             for (int it = cta; it < lit + uit; it += G) {
-                if (it < lit) trsm_rows(sm, rem, nbk, Lstrip, lda, it * kCT);
+                if (it < lit) trsm_rows(sm, rem, nbk, Lstrip, lda, it * kNB, kNB);
                 else trsm_cols64(sm, rem, nbk, Ustrip, lda, (it - lit) * kNB);
             }
         }
@@ -275,7 +276,8 @@ int coop_grid(int device) {
     if (!cached[device]) {
         int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, diag_factor_kernel, kCT, 0);
+        cudaFuncSetAttribute(diag_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, diag_factor_kernel, kCT, sizeof(Smem));
         cached[device] = per_sm > 0 ? sms : -1;
     }
     return cached[device];
@@ -301,7 +303,8 @@ mxp_status launch_diag_factor(int n, float *A, int64_t lda, float *XU, float *XL
     MXP_CUDA(cudaMemsetAsync(sync_words, 0, 2 * sizeof(unsigned int), st));
     Ctl ctl{sync_words, reinterpret_cast<int *>(sync_words + 1), dst};
     void *args[] = {&n, &A, &lda, &XU, &XL, &ldx, &tmpU, &tmpL, &ctl, &pivot_base};
-    MXP_CUDA(cudaLaunchCooperativeKernel((const void *)diag_factor_kernel, dim3(grid), dim3(kCT), args, 0, st));
+    MXP_CUDA(cudaLaunchCooperativeKernel((const void *)diag_factor_kernel, dim3(grid), dim3(kCT), args,
+                                         sizeof(Smem), st));
     MXP_LAUNCHED();
     return MXP_OK;
 }
