@@ -188,57 +188,54 @@ __device__ void gemm_tile64(Smem &sm, int m, int n, int k, float alpha, const fl
     __syncthreads();
 }
 
-// ---- 64 x 64 no-pivot LU of D (nb <= 64), one row per thread of warps 0-1 ----
+// ---- 64 x 64 no-pivot LU of D (nb <= 64) by warp 0, in registers -------------
 // sgetrf_nopiv_naive order (sgetrf_nopiv.cpp:27-61): scale by the reciprocal
-// pivot, then the rank-1 update.  The two working warps meet at a 64-thread
-// named barrier once per pivot; the rest of the CTA waits at the final
-// __syncthreads.
-__device__ __forceinline__ void bar_sync_rows() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
+// pivot, then the rank-1 update.  Lane l holds rows l and l + 32; the pivot row
+// is broadcast element by element with shuffles, so the 64 steps need no
+// barrier (rows at or above the pivot get a zero multiplier, which leaves them
+// unchanged).  The rest of the CTA waits at the final __syncthreads.
+// Pivot step K of the register LU (template recursion keeps every index static,
+// so the two row arrays stay in registers).
+template <int K>
+__device__ __forceinline__ void getrf64_step(float (&a0)[kNB], float (&a1)[kNB], int l, int nb, DevStatus *dst,
+                                             int pivot_base) {
+    if constexpr (K < kNB) {
+        if (K < nb) {
+            constexpr int src = K & 31;
+            const float piv = __shfl_sync(0xffffffffu, K < 32 ? a0[K] : a1[K], src);
+            if (l == src && (!(piv != 0.0f) || !isfinite(piv))) report(dst, MXP_ZERO_PIVOT, pivot_base + K + 1, 0);
+            const float rcp = __frcp_rn(piv);
+            const bool act0 = l > K && l < nb, act1 = l + 32 > K && l + 32 < nb;
+            const float m0 = act0 ? a0[K] * rcp : 0.0f;
+            const float m1 = act1 ? a1[K] * rcp : 0.0f;
+            if (act0) a0[K] = m0;
+            if (act1) a1[K] = m1;
+#pragma unroll
+            for (int j = K + 1; j < kNB; ++j) {
+                const float p = __shfl_sync(0xffffffffu, K < 32 ? a0[j] : a1[j], src);
+                a0[j] = fmaf(-m0, p, a0[j]);
+                a1[j] = fmaf(-m1, p, a1[j]);
+            }
+            getrf64_step<K + 1>(a0, a1, l, nb, dst, pivot_base);
+        }
+    }
+}
 
 __device__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, DevStatus *dst, int pivot_base) {
-    const int i = threadIdx.x;
-    if (i < kNB) {
-        float a[kNB];
+    (void)sm;
+    if (threadIdx.x < 32) {
+        const int l = threadIdx.x;
+        float a0[kNB], a1[kNB];
 #pragma unroll
-        for (int j = 0; j < kNB; ++j) a[j] = (i < nb && j < nb) ? __ldcg(D + (int64_t)j * lda + i) : 0.0f;
-#pragma unroll
-        for (int k = 0; k < kNB; ++k) {
-            if (k < nb) {  // uniform
-                float *pr = sm.t.prow[k & 1];
-                if (i == k) {  // publish the pivot row, zero at and left of the pivot
-#pragma unroll
-                    for (int j4 = k / 4; j4 < kNB / 4; ++j4) {
-                        float4 v;
-                        v.x = (4 * j4 + 0 > k) ? a[4 * j4 + 0] : 0.0f;
-                        v.y = (4 * j4 + 1 > k) ? a[4 * j4 + 1] : 0.0f;
-                        v.z = (4 * j4 + 2 > k) ? a[4 * j4 + 2] : 0.0f;
-                        v.w = (4 * j4 + 3 > k) ? a[4 * j4 + 3] : 0.0f;
-                        *reinterpret_cast<float4 *>(pr + 4 * j4) = v;
-                    }
-                    sm.t.pivv[k & 1] = a[k];
-                }
-                bar_sync_rows();
-                const float piv = sm.t.pivv[k & 1];
-                if (i == k && (!(piv != 0.0f) || !isfinite(piv))) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
-                const bool act = i > k && i < nb;
-                const float l = act ? a[k] * __frcp_rn(piv) : 0.0f;
-                if (act) a[k] = l;
-                // a(i, j) -= l * u(k, j) for j > k; the zeros of the published row
-                // leave columns <= k untouched (and rows <= k have l = 0)
-#pragma unroll
-                for (int j4 = k / 4; j4 < kNB / 4; ++j4) {
-                    const float4 p = *reinterpret_cast<const float4 *>(pr + 4 * j4);
-                    if (4 * j4 + 0 > k) a[4 * j4 + 0] = fmaf(-l, p.x, a[4 * j4 + 0]);
-                    if (4 * j4 + 1 > k) a[4 * j4 + 1] = fmaf(-l, p.y, a[4 * j4 + 1]);
-                    if (4 * j4 + 2 > k) a[4 * j4 + 2] = fmaf(-l, p.z, a[4 * j4 + 2]);
-                    if (4 * j4 + 3 > k) a[4 * j4 + 3] = fmaf(-l, p.w, a[4 * j4 + 3]);
-                }
-            }
+        for (int j = 0; j < kNB; ++j) {
+            a0[j] = (l < nb && j < nb) ? __ldcg(D + (int64_t)j * lda + l) : 0.0f;
+            a1[j] = (l + 32 < nb && j < nb) ? __ldcg(D + (int64_t)j * lda + l + 32) : 0.0f;
         }
-        if (i < nb) {
+        getrf64_step<0>(a0, a1, l, nb, dst, pivot_base);
 #pragma unroll
-            for (int j = 0; j < kNB; ++j)
-                if (j < nb) D[(int64_t)j * lda + i] = a[j];
+        for (int j = 0; j < kNB; ++j) {
+            if (l < nb && j < nb) D[(int64_t)j * lda + l] = a0[j];
+            if (l + 32 < nb && j < nb) D[(int64_t)j * lda + l + 32] = a1[j];
         }
     }
     __syncthreads();
