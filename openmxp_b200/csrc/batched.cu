@@ -130,37 +130,39 @@ __device__ __forceinline__ void stage_zero_row(uint8_t *base, int nblk, int row,
 // lower part of sm.t.  The 64 x 256 block goes through shared memory (stage:
 // 256 x 65 floats) with coalesced loads and stores; thread j solves column j.
 constexpr size_t kColStageOff = 65536;  // after the Smem union
-constexpr int kStagePitch = kNB + 4;    // 16-byte rows
-constexpr size_t kColStageBytes = sizeof(float) * kCT * kStagePitch;
+constexpr size_t kColStageBytes = sizeof(float) * kCT * (kNB + 1);
 
 __device__ void trsm_cols_staged(Smem &sm, float *stage, int ncols, int nb, float *B, int64_t ldb, int c0) {
-    float(*xs)[kStagePitch] = reinterpret_cast<float(*)[kStagePitch]>(stage);
     for (int idx = threadIdx.x; idx < kNB * kCT; idx += kCT) {
         const int k = idx % kNB, j = idx / kNB;
-        xs[j][k] = (k < nb && c0 + j < ncols) ? __ldcg(B + (int64_t)(c0 + j) * ldb + k) : 0.0f;
+        stage[j * (kNB + 1) + k] = (k < nb && c0 + j < ncols) ? __ldcg(B + (int64_t)(c0 + j) * ldb + k) : 0.0f;
     }
     __syncthreads();
-    {  // right-looking: x_r -= l_rk x_k for r > k (l_.k contiguous in sm.t.t)
+    {  // right-looking: x_r -= l_rk x_k for r > k (l_.k contiguous in sm.t)
         const int j = threadIdx.x;
-#pragma unroll 1
-        for (int k = 0; k < nb - 1; ++k) {
-            const float xk = xs[j][k];
-#pragma unroll 2
-            for (int r4 = (k + 1) >> 2; r4 < kNB / 4; ++r4) {
-                const float4 l = *reinterpret_cast<const float4 *>(&sm.t.t[k][4 * r4]);
-                float4 x = *reinterpret_cast<const float4 *>(&xs[j][4 * r4]);
-                if (4 * r4 + 0 > k) x.x = fmaf(-l.x, xk, x.x);
-                if (4 * r4 + 1 > k) x.y = fmaf(-l.y, xk, x.y);
-                if (4 * r4 + 2 > k) x.z = fmaf(-l.z, xk, x.z);
-                if (4 * r4 + 3 > k) x.w = fmaf(-l.w, xk, x.w);
-                *reinterpret_cast<float4 *>(&xs[j][4 * r4]) = x;
+        float x[kNB];
+#pragma unroll
+        for (int k = 0; k < kNB; ++k) x[k] = stage[j * (kNB + 1) + k];
+#pragma unroll
+        for (int k = 0; k < kNB - 1; ++k) {
+            if (k < nb) {
+#pragma unroll
+                for (int r4 = (k + 1) / 4; r4 < kNB / 4; ++r4) {
+                    const float4 l = *reinterpret_cast<const float4 *>(&sm.t.t[k][4 * r4]);
+                    if (4 * r4 + 0 > k) x[4 * r4 + 0] = fmaf(-l.x, x[k], x[4 * r4 + 0]);
+                    if (4 * r4 + 1 > k) x[4 * r4 + 1] = fmaf(-l.y, x[k], x[4 * r4 + 1]);
+                    if (4 * r4 + 2 > k) x[4 * r4 + 2] = fmaf(-l.z, x[k], x[4 * r4 + 2]);
+                    if (4 * r4 + 3 > k) x[4 * r4 + 3] = fmaf(-l.w, x[k], x[4 * r4 + 3]);
+                }
             }
         }
+#pragma unroll
+        for (int k = 0; k < kNB; ++k) stage[j * (kNB + 1) + k] = x[k];
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < kNB * kCT; idx += kCT) {
         const int k = idx % kNB, j = idx / kNB;
-        if (k < nb && c0 + j < ncols) B[(int64_t)(c0 + j) * ldb + k] = xs[j][k];
+        if (k < nb && c0 + j < ncols) B[(int64_t)(c0 + j) * ldb + k] = stage[j * (kNB + 1) + k];
     }
     __syncthreads();
 }
@@ -179,8 +181,7 @@ __device__ void factor_step(Smem &sm, float *stage, float *A, int n, int k0, int
         const int rem = bk - jb - kNB;
         if (rem <= 0) break;
         load_tri(sm, kNB, Dj, lda);
-        for (int r0 = 0; r0 < rem; r0 += kCT) trsm_rows(sm, rem, kNB, Dj + kNB, lda, r0, kCT, stage);
-        __syncthreads();  // the staged column solve reuses the row buffer
+        for (int r0 = 0; r0 < rem; r0 += kCT) trsm_rows(sm, rem, kNB, Dj + kNB, lda, r0);
         for (int c0 = 0; c0 < rem; c0 += kCT) trsm_cols_staged(sm, stage, rem, kNB, Dj + (int64_t)kNB * lda, lda, c0);
         __syncthreads();
         const int tm = (rem + GBM - 1) / GBM;
@@ -194,7 +195,7 @@ __device__ void factor_step(Smem &sm, float *stage, float *A, int n, int k0, int
     // L strip: X U = B, one 64-column block at a time
     for (int c = 0; c < bk; c += kNB) {
         load_tri(sm, kNB, D + c + (int64_t)c * lda, lda);
-        for (int r0 = 0; r0 < m; r0 += kCT) trsm_rows(sm, m, kNB, Ls + (int64_t)c * lda, lda, r0, kCT, stage);
+        for (int r0 = 0; r0 < m; r0 += kCT) trsm_rows(sm, m, kNB, Ls + (int64_t)c * lda, lda, r0);
         __syncthreads();
         const int rest = bk - c - kNB;
         if (rest > 0) {

@@ -23,7 +23,7 @@ struct SmemGemm {
 struct __align__(16) SmemTri {
     float t[kNB][kNB + 4];   // t[col][row] of a 64 x 64 block (16-byte rows)
     float tt[kNB][kNB + 4];  // tt[row][col]: the same block row-major
-    float ub[kNB][kNB + 4];  // 64 strip rows / columns being solved (16-byte rows)
+    float ub[kNB][kNB + 1];  // staging of 64 U-strip columns, ub[col][row]
     float prow[2][kNB];      // pivot row of the 64 x 64 LU, zero left of the pivot
     float dinv[kNB];
     float pivv[2];
@@ -188,49 +188,58 @@ __device__ void gemm_tile64(Smem &sm, int m, int n, int k, float alpha, const fl
     __syncthreads();
 }
 
-// ---- 64 x 64 no-pivot LU of D (nb <= 64) in shared memory ----------------------
+// ---- 64 x 64 no-pivot LU of D (nb <= 64), one row per thread of warps 0-1 ----
 // sgetrf_nopiv_naive order (sgetrf_nopiv.cpp:27-61): scale by the reciprocal
-// pivot, then the rank-1 update.  The block sits row-major in sm.t.tt; thread
-// r of warps 0-1 owns row r and updates it four columns at a time, the two
-// warps meeting at a 64-thread named barrier once per pivot.  The loops stay
-// rolled: a fully unrolled 64-step factor is thousands of straight-line
-// instructions and runs at the speed of instruction fetch.
+// pivot, then the rank-1 update.  The two working warps meet at a 64-thread
+// named barrier once per pivot; the rest of the CTA waits at the final
+// __syncthreads.
 __device__ __forceinline__ void bar_sync_rows() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
 
 __device__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, DevStatus *dst, int pivot_base) {
-    float(*s)[kNB + 4] = sm.t.tt;
-    for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
-        const int r = idx % kNB, c = idx / kNB;
-        s[r][c] = (r < nb && c < nb) ? __ldcg(D + (int64_t)c * lda + r) : 0.0f;
-    }
-    __syncthreads();
-    if (threadIdx.x < kNB) {
-        const int r = threadIdx.x;
-#pragma unroll 1
-        for (int k = 0; k < nb; ++k) {
-            const float piv = s[k][k];
-            if (r == k && (!(piv != 0.0f) || !isfinite(piv))) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
-            if (r > k && r < nb) {
-                const float m = s[r][k] * __frcp_rn(piv);
-                s[r][k] = m;
-#pragma unroll 2
-                for (int j4 = (k + 1) >> 2; j4 < kNB / 4; ++j4) {
-                    const float4 p = *reinterpret_cast<const float4 *>(&s[k][4 * j4]);
-                    float4 a = *reinterpret_cast<const float4 *>(&s[r][4 * j4]);
-                    if (4 * j4 + 0 > k) a.x = fmaf(-m, p.x, a.x);
-                    if (4 * j4 + 1 > k) a.y = fmaf(-m, p.y, a.y);
-                    if (4 * j4 + 2 > k) a.z = fmaf(-m, p.z, a.z);
-                    if (4 * j4 + 3 > k) a.w = fmaf(-m, p.w, a.w);
-                    *reinterpret_cast<float4 *>(&s[r][4 * j4]) = a;
+    const int i = threadIdx.x;
+    if (i < kNB) {
+        float a[kNB];
+#pragma unroll
+        for (int j = 0; j < kNB; ++j) a[j] = (i < nb && j < nb) ? __ldcg(D + (int64_t)j * lda + i) : 0.0f;
+#pragma unroll
+        for (int k = 0; k < kNB; ++k) {
+            if (k < nb) {  // uniform
+                float *pr = sm.t.prow[k & 1];
+                if (i == k) {  // publish the pivot row, zero at and left of the pivot
+#pragma unroll
+                    for (int j4 = k / 4; j4 < kNB / 4; ++j4) {
+                        float4 v;
+                        v.x = (4 * j4 + 0 > k) ? a[4 * j4 + 0] : 0.0f;
+                        v.y = (4 * j4 + 1 > k) ? a[4 * j4 + 1] : 0.0f;
+                        v.z = (4 * j4 + 2 > k) ? a[4 * j4 + 2] : 0.0f;
+                        v.w = (4 * j4 + 3 > k) ? a[4 * j4 + 3] : 0.0f;
+                        *reinterpret_cast<float4 *>(pr + 4 * j4) = v;
+                    }
+                    sm.t.pivv[k & 1] = a[k];
+                }
+                bar_sync_rows();
+                const float piv = sm.t.pivv[k & 1];
+                if (i == k && (!(piv != 0.0f) || !isfinite(piv))) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
+                const bool act = i > k && i < nb;
+                const float l = act ? a[k] * __frcp_rn(piv) : 0.0f;
+                if (act) a[k] = l;
+                // a(i, j) -= l * u(k, j) for j > k; the zeros of the published row
+                // leave columns <= k untouched (and rows <= k have l = 0)
+#pragma unroll
+                for (int j4 = k / 4; j4 < kNB / 4; ++j4) {
+                    const float4 p = *reinterpret_cast<const float4 *>(pr + 4 * j4);
+                    if (4 * j4 + 0 > k) a[4 * j4 + 0] = fmaf(-l, p.x, a[4 * j4 + 0]);
+                    if (4 * j4 + 1 > k) a[4 * j4 + 1] = fmaf(-l, p.y, a[4 * j4 + 1]);
+                    if (4 * j4 + 2 > k) a[4 * j4 + 2] = fmaf(-l, p.z, a[4 * j4 + 2]);
+                    if (4 * j4 + 3 > k) a[4 * j4 + 3] = fmaf(-l, p.w, a[4 * j4 + 3]);
                 }
             }
-            bar_sync_rows();
         }
-    }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
-        const int r = idx % kNB, c = idx / kNB;
-        if (r < nb && c < nb) D[(int64_t)c * lda + r] = s[r][c];
+        if (i < nb) {
+#pragma unroll
+            for (int j = 0; j < kNB; ++j)
+                if (j < nb) D[(int64_t)j * lda + i] = a[j];
+        }
     }
     __syncthreads();
 }
@@ -248,64 +257,65 @@ __device__ void load_tri(Smem &sm, int nb, const float *D, int64_t lda) {
     __syncthreads();
 }
 
-// L strip rows [r0, r0 + rows) of B (m x nb): X = B U^{-1}, U = upper part of
-// the diagonal block (row-major copy in sm.t.tt).  Right-looking (x_k final,
-// then x_c -= u_kc x_k for c > k): per element the same operations in the same
-// order as the dot-product form, with independent updates.  Each thread's row
-// sits in xbuf (rows x 68 floats, shared memory) and the loops stay rolled.
-__device__ void trsm_rows(Smem &sm, int m, int nb, float *B, int64_t ldb, int r0, int rows, float *xbuf) {
-    float(*xs)[kNB + 4] = reinterpret_cast<float(*)[kNB + 4]>(xbuf);
-    const int t = threadIdx.x, i = r0 + t;
-    const bool act = t < rows && i < m;
-    if (act) {
-#pragma unroll 8
-        for (int c = 0; c < kNB; ++c) xs[t][c] = (c < nb) ? __ldcg(B + (int64_t)c * ldb + i) : 0.0f;
-#pragma unroll 1
-        for (int k = 0; k < nb; ++k) {
-            const float xk = xs[t][k] * sm.t.dinv[k];
-            xs[t][k] = xk;
-#pragma unroll 2
-            for (int c4 = (k + 1) >> 2; c4 < kNB / 4; ++c4) {
+// L strip rows [r0, r0 + rows) of B (m x nb), rows <= kCT: X = B U^{-1}, U =
+// upper part of the diagonal block in sm.t.  Right-looking (x_k final, then
+// x_c -= u_kc x_k for c > k): per element the same operations in the same
+// order as the dot-product form, with independent updates instead of one
+// dependent chain per row; u_k. is read four at a time from the row-major copy.
+__device__ void trsm_rows(Smem &sm, int m, int nb, float *B, int64_t ldb, int r0, int rows = kCT) {
+    const int i = r0 + threadIdx.x;
+    if (threadIdx.x >= rows || i >= m) return;
+    float x[kNB];
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) x[c] = (c < nb) ? __ldcg(B + (int64_t)c * ldb + i) : 0.0f;
+#pragma unroll
+    for (int k = 0; k < kNB; ++k) {
+        if (k < nb) {
+            x[k] *= sm.t.dinv[k];
+#pragma unroll
+            for (int c4 = (k + 1) / 4; c4 < kNB / 4; ++c4) {
                 const float4 u = *reinterpret_cast<const float4 *>(&sm.t.tt[k][4 * c4]);
-                float4 x = *reinterpret_cast<const float4 *>(&xs[t][4 * c4]);
-                if (4 * c4 + 0 > k) x.x = fmaf(-u.x, xk, x.x);
-                if (4 * c4 + 1 > k) x.y = fmaf(-u.y, xk, x.y);
-                if (4 * c4 + 2 > k) x.z = fmaf(-u.z, xk, x.z);
-                if (4 * c4 + 3 > k) x.w = fmaf(-u.w, xk, x.w);
-                *reinterpret_cast<float4 *>(&xs[t][4 * c4]) = x;
+                if (4 * c4 + 0 > k) x[4 * c4 + 0] = fmaf(-u.x, x[k], x[4 * c4 + 0]);
+                if (4 * c4 + 1 > k) x[4 * c4 + 1] = fmaf(-u.y, x[k], x[4 * c4 + 1]);
+                if (4 * c4 + 2 > k) x[4 * c4 + 2] = fmaf(-u.z, x[k], x[4 * c4 + 2]);
+                if (4 * c4 + 3 > k) x[4 * c4 + 3] = fmaf(-u.w, x[k], x[4 * c4 + 3]);
             }
         }
-#pragma unroll 8
-        for (int c = 0; c < nb; ++c) B[(int64_t)c * ldb + i] = xs[t][c];
     }
+#pragma unroll
+    for (int c = 0; c < kNB; ++c)
+        if (c < nb) B[(int64_t)c * ldb + i] = x[c];
 }
 
 // U strip columns [c0, c0 + 64) of B (nb x ncols): X = L^{-1} B, L = unit lower
-// part of the diagonal block (column-major copy in sm.t.t).  The 64 x 64 block
-// moves through sm.t.ub with coalesced loads and stores; thread j solves column
-// j right-looking (x_r -= l_rk x_k for r > k) with rolled loops.
+// part of sm.t.  The 64 x 64 block moves through shared memory with coalesced
+// loads and stores; threads 0..63 solve one column each.
 __device__ void trsm_cols64(Smem &sm, int ncols, int nb, float *B, int64_t ldb, int c0) {
     for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
         const int k = idx % kNB, j = idx / kNB;
         sm.t.ub[j][k] = (k < nb && c0 + j < ncols) ? __ldcg(B + (int64_t)(c0 + j) * ldb + k) : 0.0f;
     }
     __syncthreads();
-    if (threadIdx.x < kNB) {
+    if (threadIdx.x < kNB) {  // right-looking: x_r -= l_rk x_k for r > k (l_.k contiguous in sm.t)
         const int j = threadIdx.x;
-#pragma unroll 1
-        for (int k = 0; k < nb - 1; ++k) {
-            const float xk = sm.t.ub[j][k];
-#pragma unroll 2
-            for (int r4 = (k + 1) >> 2; r4 < kNB / 4; ++r4) {
-                const float4 l = *reinterpret_cast<const float4 *>(&sm.t.t[k][4 * r4]);
-                float4 x = *reinterpret_cast<const float4 *>(&sm.t.ub[j][4 * r4]);
-                if (4 * r4 + 0 > k) x.x = fmaf(-l.x, xk, x.x);
-                if (4 * r4 + 1 > k) x.y = fmaf(-l.y, xk, x.y);
-                if (4 * r4 + 2 > k) x.z = fmaf(-l.z, xk, x.z);
-                if (4 * r4 + 3 > k) x.w = fmaf(-l.w, xk, x.w);
-                *reinterpret_cast<float4 *>(&sm.t.ub[j][4 * r4]) = x;
+        float x[kNB];
+#pragma unroll
+        for (int k = 0; k < kNB; ++k) x[k] = sm.t.ub[j][k];
+#pragma unroll
+        for (int k = 0; k < kNB - 1; ++k) {
+            if (k < nb) {
+#pragma unroll
+                for (int r4 = (k + 1) / 4; r4 < kNB / 4; ++r4) {
+                    const float4 l = *reinterpret_cast<const float4 *>(&sm.t.t[k][4 * r4]);
+                    if (4 * r4 + 0 > k) x[4 * r4 + 0] = fmaf(-l.x, x[k], x[4 * r4 + 0]);
+                    if (4 * r4 + 1 > k) x[4 * r4 + 1] = fmaf(-l.y, x[k], x[4 * r4 + 1]);
+                    if (4 * r4 + 2 > k) x[4 * r4 + 2] = fmaf(-l.z, x[k], x[4 * r4 + 2]);
+                    if (4 * r4 + 3 > k) x[4 * r4 + 3] = fmaf(-l.w, x[k], x[4 * r4 + 3]);
+                }
             }
         }
+#pragma unroll
+        for (int k = 0; k < kNB; ++k) sm.t.ub[j][k] = x[k];
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {

@@ -189,10 +189,7 @@ diag_factor_kernel(int n, float *A, int64_t lda, float *XU, float *XL, int64_t l
         if (cta < lit + uit) {
             load_tri(sm, nbk, Djj, lda);
             for (int it = cta; it < lit + uit; it += G) {
-                if (it < lit) {
-                    trsm_rows(sm, rem, nbk, Lstrip, lda, it * kNB, kNB, &sm.t.ub[0][0]);
-                    __syncthreads();  // the next item reuses sm.t.ub
-                }
+                if (it < lit) trsm_rows(sm, rem, nbk, Lstrip, lda, it * kNB, kNB);
                 else trsm_cols64(sm, rem, nbk, Ustrip, lda, (it - lit) * kNB);
             }
         }
