@@ -245,6 +245,8 @@ def _solve_arm(args, form_name, p, dev, dist, local, e2e_on):
     form = mxp.FORMS[form_name]
     n, b = args.n, args.b
     ws = mxp.Workspace(n, b, form, device=local, trsm_tensor=(args.trsm == "tensor"))
+    if args.trsm_pair:
+        ws.set_option(mxp.OPT_TRSM_PAIR, 1)
     method = mxp.IR_GMRES if args.ir == "gmres" else mxp.IR_CLASSIC
     x = torch.empty(n, dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream()
@@ -658,6 +660,7 @@ def parse(argv=None):
                     help="time one kernel alone at m=--n, k=--b (for profiler captures)")
     ap.add_argument("--micro-seconds", type=float, default=0.0,
                     help="micro: run the launch this long before timing (sustained clocks)")
+    ap.add_argument("--trsm-pair", action="store_true", help="TRSM-by-inverse products on the 2-SM kernel")
     ap.add_argument("--batched", action="store_true",
                     help="the batched form: --batch-count systems of orders 128*{2..32}")
     ap.add_argument("--batch-count", type=int, default=2048)

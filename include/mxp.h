@@ -104,9 +104,10 @@ typedef enum {
                                    panels k and k+1 to the trailing matrix in one K = 2b pass */
     MXP_OPT_SCHUR_PAIR = 5,     /* 1: tensor-core products on pairs of SMs (2-SM MMA, 256 x 256
                                    tiles); 0 (default): one SM per 128 x 256 tile */
-    MXP_OPT_DIAG_COOP = 6       /* 1 (default): diagonal-block LU (and the triangular inverses of
+    MXP_OPT_DIAG_COOP = 6,      /* 1 (default): diagonal-block LU (and the triangular inverses of
                                    the tensor-core TRSM) in one cooperative launch with grid
                                    barriers; 0: one launch per 64-column step */
+    MXP_OPT_TRSM_PAIR = 7       /* 1: TRSM-by-inverse products on the 2-SM kernel; 0 (default): 1-SM */
 } mxp_option;
 mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int value);
 mxp_status mxp_workspace_destroy(mxp_workspace *ws);

@@ -155,6 +155,7 @@ OPT_GMRES_TOL_EXP = 3
 OPT_MERGE_PANELS = 4
 OPT_SCHUR_PAIR = 5
 OPT_DIAG_COOP = 6
+OPT_TRSM_PAIR = 7
 
 
 class Workspace:

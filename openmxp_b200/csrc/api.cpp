@@ -82,7 +82,8 @@ struct mxp_workspace {
     int64_t kp = 0;          // K extent of one panel (b, or 3b for BF16X2)
     int sc_ld = 0;           // FP8 scale-table row stride (tiles): two panels side by side
     int merge = 1;           // merged look-ahead: two panels per trailing pass
-    int pair = 0;            // Schur / panel products on the 2-SM (cta_group::2) kernel
+    int pair = 0;            // trailing Schur products on the 2-SM (cta_group::2) kernel
+    int trsm_pair = 0;       // TRSM-by-inverse products on the 2-SM kernel
     size_t esize = 2;        // panel element size
     void *lpanel[2] = {nullptr, nullptr};
     void *rpanel[2] = {nullptr, nullptr};
@@ -240,6 +241,9 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
             return MXP_OK;
         case MXP_OPT_DIAG_COOP:
             ws->coop = value ? 1 : 0;
+            return MXP_OK;
+        case MXP_OPT_TRSM_PAIR:
+            ws->trsm_pair = value ? 1 : 0;
             return MXP_OK;
         case MXP_OPT_GMRES_RESTART:
             if (value < 1 || value > 30) return fail(MXP_INVALID_ARG, "set_option: GMRES restart must be 1..30");
@@ -453,14 +457,14 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
             pt.mark(PH_TGEMM);
             if (q == MXP_OK)
                 q = launch_schur(bf, m, b, b, ws->split_big, ws->ldk3, nullptr, ws->split_u, ws->ldk3,
-                                 nullptr, Lcol, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/1, ws->pair);
+                                 nullptr, Lcol, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/1, ws->trsm_pair);
             pt.mark(PH_CAST);
             if (q == MXP_OK) q = launch_cast_left(bf, b, b, ws->tinv_l, b, ws->split_l, ws->ldk3, nullptr, st);
             if (q == MXP_OK) q = launch_cast_right(bf, m, b, Urow, lda, ws->split_big, ws->ldk3, nullptr, st);
             pt.mark(PH_TGEMM);
             if (q == MXP_OK)
                 q = launch_schur(bf, b, m, b, ws->split_l, ws->ldk3, nullptr, ws->split_big, ws->ldk3,
-                                 nullptr, Urow, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/2, ws->pair);
+                                 nullptr, Urow, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/2, ws->trsm_pair);
         } else {
             q = launch_trsm_runn(m, b, Akk, lda, Lcol, lda, st);
             if (q == MXP_OK) q = launch_trsm_llnu(b, m, Akk, lda, Urow, lda, st);

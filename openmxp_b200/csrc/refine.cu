@@ -115,7 +115,7 @@ __device__ __forceinline__ void st_release(int *p, int v) {
 //   * Minv = inverse of the diagonal block (FP64, from the FP32 factor) and
 //     P = Minv * A_adj, A_adj the off-diagonal block next in the chain;
 //   * the products of all other off-diagonal blocks with their (already
-//     solved) x, streamed with one column block of look-ahead;
+//     solved) x, streamed with four column blocks of loads in flight;
 //   * w = Minv (r_b - those products).
 // When the predecessor publishes its x, the block finishes with one 64 x 64
 // FP64 matrix-vector product, x_b = w - P x_adj, and publishes its own x.
@@ -203,8 +203,8 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
     const int64_t grow = row0 + r;
     const bool row_ok = r < nrows;
     const int nstream = has_adj ? ncb - 1 : 0;
-    float lv[16], lnext[16];
     auto load_l = [&](int q, float *d) {
+        if (q >= nstream) return;
         const int cb = LOWER ? q : nrb - 1 - q;
         const int64_t c0 = (int64_t)cb * kRB + cph * 16;
         const int clen = (int)imin64(16, n - c0);
@@ -220,9 +220,8 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
         }
         return true;
     };
-    if (nstream > 0) load_l(0, lv);
-    for (int q = 0; q < nstream && !timed_out; ++q) {
-        if (q + 1 < nstream) load_l(q + 1, lnext);
+    // one column block: wait until its x is published, then accumulate
+    auto consume = [&](int q, const float *lv) {
         const int cb = LOWER ? q : nrb - 1 - q;
         const bool need = LOWER ? (cb > known) : (cb < known);
         if (need) {
@@ -233,7 +232,6 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
                 known = cb;
             }
         }
-        if (timed_out) break;
         const int64_t c0 = (int64_t)cb * kRB + cph * 16;
         const int clen = (int)imin64(16, n - c0);
         double xv[16];
@@ -241,8 +239,26 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
         for (int cc = 0; cc < 16; ++cc) xv[cc] = (cc < clen) ? __ldcg(x + c0 + cc) : 0.0;
 #pragma unroll
         for (int cc = 0; cc < 16; ++cc) acc = __fma_rn((double)lv[cc], xv[cc], acc);
-#pragma unroll
-        for (int cc = 0; cc < 16; ++cc) lv[cc] = lnext[cc];
+    };
+    // factor values do not depend on other blocks: keep four column blocks of
+    // loads in flight (a register ring, unrolled so its indices stay static)
+    float b0[16], b1[16], b2[16], b3[16];
+    load_l(0, b0);
+    load_l(1, b1);
+    load_l(2, b2);
+    load_l(3, b3);
+    for (int q = 0; q < nstream && !timed_out; q += 4) {
+        consume(q, b0);
+        load_l(q + 4, b0);
+        if (q + 1 >= nstream || timed_out) break;
+        consume(q + 1, b1);
+        load_l(q + 5, b1);
+        if (q + 2 >= nstream || timed_out) break;
+        consume(q + 2, b2);
+        load_l(q + 6, b2);
+        if (q + 3 >= nstream || timed_out) break;
+        consume(q + 3, b3);
+        load_l(q + 7, b3);
     }
     part[cph][r] = acc;
     __syncthreads();
