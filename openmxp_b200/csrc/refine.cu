@@ -212,20 +212,38 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
 #pragma unroll
         for (int cc = 0; cc < 16; ++cc) d[cc] = (row_ok && cc < clen) ? col[cc * lda] : 0.0f;
     };
+    // Flags are polled by lane 0 of each warp only (every thread spinning on the
+    // same lines slows the producer's release) and the outcome is shared by a
+    // shuffle; the warp barrier orders the lanes' later loads after the acquire.
+    const bool lead = (tid & 31) == 0;
     auto wait_flag = [&](int b) -> bool {
-        const unsigned long long t0 = globaltimer_ns();
-        uint32_t it = 0;
-        while (!ld_acquire(&flags[b])) {
-            if ((++it & 255u) == 0u && globaltimer_ns() - t0 > kWaitTimeoutNs) return false;
+        int ok = 1;
+        if (lead) {
+            const unsigned long long t0 = globaltimer_ns();
+            uint32_t it = 0;
+            while (!ld_acquire(&flags[b])) {
+                if ((++it & 63u) == 0u && globaltimer_ns() - t0 > kWaitTimeoutNs) {
+                    ok = 0;
+                    break;
+                }
+            }
         }
-        return true;
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        __syncwarp();
+        return ok != 0;
+    };
+    auto probe_flag = [&](int b) -> bool {
+        int v = lead ? ld_acquire(&flags[b]) : 0;
+        v = __shfl_sync(0xffffffffu, v, 0);
+        __syncwarp();
+        return v != 0;
     };
     // one column block: wait until its x is published, then accumulate
     auto consume = [&](int q, const float *lv) {
         const int cb = LOWER ? q : nrb - 1 - q;
         const bool need = LOWER ? (cb > known) : (cb < known);
         if (need) {
-            if (ld_acquire(&flags[adj - (LOWER ? 1 : -1)])) {
+            if (probe_flag(adj - (LOWER ? 1 : -1))) {
                 known = adj - (LOWER ? 1 : -1);  // blocks complete in chain order
             } else {
                 timed_out = !wait_flag(cb);
