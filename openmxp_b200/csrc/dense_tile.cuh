@@ -325,6 +325,149 @@ __device__ void trsm_cols64(Smem &sm, int ncols, int nb, float *B, int64_t ldb, 
     __syncthreads();
 }
 
+// Inverse of the 64 x 64 diagonal block `blk` of an upper non-unit (upper = true)
+// or unit-lower triangle; row i of the inverse solves x T = e_i.
+__device__ void inv_diag_block(Smem &sm, int n, const float *T, int64_t ldt, float *X, int64_t ldx,
+                               int blk, bool upper) {
+    const int r0 = blk * kNB;
+    const int nb = min(kNB, n - r0);
+    for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
+        const int r = idx % kNB, c = idx / kNB;
+        sm.t.t[c][r] = (r < nb && c < nb) ? __ldcg(T + (int64_t)(r0 + c) * ldt + r0 + r) : 0.0f;
+    }
+    __syncthreads();
+    const int i = threadIdx.x;
+    if (i < nb) {
+        float x[kNB];
+        if (upper) {
+#pragma unroll
+            for (int j = 0; j < kNB; ++j) {
+                float v = (j == i) ? 1.0f : 0.0f;
+#pragma unroll
+                for (int q = 0; q < j; ++q) v -= x[q] * sm.t.t[j][q];
+                x[j] = (j >= i && j < nb) ? v / sm.t.t[j][j] : 0.0f;
+            }
+        } else {
+#pragma unroll
+            for (int jj = 0; jj < kNB; ++jj) {
+                const int j = kNB - 1 - jj;
+                float v = (j == i) ? 1.0f : 0.0f;
+#pragma unroll
+                for (int q = j + 1; q < kNB; ++q) v -= x[q] * sm.t.t[j][q];
+                x[j] = (j <= i) ? v : 0.0f;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kNB; ++j)
+            if (j < nb) X[(int64_t)(r0 + j) * ldx + r0 + i] = x[j];
+    }
+    __syncthreads();
+}
+
+// One batched GEMM of an inverse level.  tri: which operand is triangular, so
+// its zero half is skipped along K: 1 A upper, 2 A lower, 3 B upper, 4 B lower.
+struct Job {
+    int m, n, K, batch, tri;
+    float alpha;
+    const float *A;
+    int64_t lda, sA;
+    const float *B;
+    int64_t ldb, sB;
+    float *C;
+    int64_t ldc, sC;
+};
+
+__device__ void run_jobs(Smem &sm, const Job *jobs, int njobs, int cta, int ncta) {
+    int tiles[4] = {0, 0, 0, 0}, total = 0;
+    for (int q = 0; q < njobs; ++q) {
+        tiles[q] = ((jobs[q].m + GBM - 1) / GBM) * ((jobs[q].n + GBN - 1) / GBN) * jobs[q].batch;
+        total += tiles[q];
+    }
+    for (int it = cta; it < total; it += ncta) {
+        int q = 0, r = it;
+        while (r >= tiles[q]) r -= tiles[q++];
+        const Job &J = jobs[q];
+        const int tm = (J.m + GBM - 1) / GBM, tn = (J.n + GBN - 1) / GBN;
+        const int z = r / (tm * tn);
+        const int rt = r % (tm * tn);
+        const int m0 = (rt % tm) * GBM, n0 = (rt / tm) * GBN;
+        int kb = 0, ke = J.K;
+        if (J.tri == 1) kb = m0;
+        if (J.tri == 2) ke = min(J.K, m0 + GBM);
+        if (J.tri == 3) ke = min(J.K, n0 + GBN);
+        if (J.tri == 4) kb = n0;
+        gemm_tile(sm, J.m, J.n, kb, ke, J.alpha, J.A + J.sA * z, J.lda, J.B + J.sB * z, J.ldb, false,
+                  J.C + J.sC * z, J.ldc, m0, n0);
+    }
+}
+
+// inv(U) -> XU and inv(L) -> XL (unit lower) of the factored n x n block A, by
+// recursive doubling: 64 x 64 diagonal blocks first, then for adjacent
+// S-blocks the off-diagonal block of the inverse is -inv(A) B inv(C), two GEMM
+// phases per level with both triangles in the same phases and the zero half of
+// every triangular operand skipped along K.  Work items are spread over
+// (cta, ncta); sync(where) separates the phases (a grid barrier across CTAs or
+// __syncthreads in a single CTA) and returns false to stop.  tmpU / tmpL hold
+// n*n/2 + 64 n floats each.
+template <typename Sync>
+__device__ bool tri_inverses(Smem &sm, int n, const float *A, int64_t lda, float *XU, float *XL, int64_t ldx,
+                             float *tmpU, float *tmpL, int cta, int G, Sync sync) {
+    const int nsteps = (n + kNB - 1) / kNB;
+    // invert the diagonal 64 x 64 blocks and zero the opposite block-triangle
+    const int nblk = nsteps;
+    for (int it = cta; it < 2 * nblk; it += G)
+        inv_diag_block(sm, n, A, lda, it < nblk ? XU : XL, ldx, it % nblk, it < nblk);
+    for (int64_t idx = (int64_t)cta * kCT + threadIdx.x; idx < (int64_t)n * n; idx += (int64_t)G * kCT) {
+        const int r = (int)(idx % n), c = (int)(idx / n);
+        if (r / kNB > c / kNB) XU[(int64_t)c * ldx + r] = 0.0f;
+        if (r / kNB < c / kNB) XL[(int64_t)c * ldx + r] = 0.0f;
+    }
+    if (!sync(23)) return false;
+
+    const float *U = A, *L = A;
+    const int64_t ldu = lda, ldl = lda;
+    for (int S = kNB; S < n; S *= 2) {
+        const int np = n / (2 * S);
+        const int rem = n - np * 2 * S;
+        const int c = rem - S;  // ragged last pair (when > 0)
+        const int64_t r0 = (int64_t)np * 2 * S;
+        const int64_t stepX = 2 * (int64_t)S * (1 + ldx), stepA = 2 * (int64_t)S * (1 + lda);
+        const int64_t SS = (int64_t)S * S;
+        Job jb[4];
+        int nj = 0;
+        // phase a:  T_U = U12 inv(U22);  T_L = L21 inv(L11)
+        if (np > 0) {
+            jb[nj++] = Job{S, S, S, np, 3, 1.0f, U + (int64_t)S * ldu, ldu, stepA, XU + S + (int64_t)S * ldx,
+                           ldx, stepX, tmpU, S, SS};
+            jb[nj++] = Job{S, S, S, np, 4, 1.0f, L + S, ldl, stepA, XL, ldx, stepX, tmpL, S, SS};
+        }
+        if (c > 0) {
+            jb[nj++] = Job{S, c, c, 1, 3, 1.0f, U + r0 + (r0 + S) * ldu, ldu, 0,
+                           XU + (r0 + S) + (r0 + S) * ldx, ldx, 0, tmpU + np * SS, S, 0};
+            jb[nj++] = Job{c, S, S, 1, 4, 1.0f, L + (r0 + S) + r0 * ldl, ldl, 0, XL + r0 + r0 * ldx, ldx, 0,
+                           tmpL + np * SS, c, 0};
+        }
+        run_jobs(sm, jb, nj, cta, G);
+        if (!sync(24)) return false;
+        // phase b:  X12 = -inv(U11) T_U;  X21 = -inv(L22) T_L
+        nj = 0;
+        if (np > 0) {
+            jb[nj++] = Job{S, S, S, np, 1, -1.0f, XU, ldx, stepX, tmpU, S, SS, XU + (int64_t)S * ldx, ldx, stepX};
+            jb[nj++] = Job{S, S, S, np, 2, -1.0f, XL + S + (int64_t)S * ldx, ldx, stepX, tmpL, S, SS, XL + S,
+                           ldx, stepX};
+        }
+        if (c > 0) {
+            jb[nj++] = Job{S, c, S, 1, 1, -1.0f, XU + r0 + r0 * ldx, ldx, 0, tmpU + np * SS, S, 0,
+                           XU + r0 + (r0 + S) * ldx, ldx, 0};
+            jb[nj++] = Job{c, S, c, 1, 2, -1.0f, XL + (r0 + S) + (r0 + S) * ldx, ldx, 0, tmpL + np * SS, c, 0,
+                           XL + (r0 + S) + r0 * ldx, ldx, 0};
+        }
+        run_jobs(sm, jb, nj, cta, G);
+        if (!sync(25)) return false;
+    }
+    return true;
+}
+
 }  // namespace
 }  // namespace dt
 }  // namespace mxp
