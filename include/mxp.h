@@ -107,7 +107,11 @@ typedef enum {
     MXP_OPT_DIAG_COOP = 6,      /* 1 (default): diagonal-block LU (and the triangular inverses of
                                    the tensor-core TRSM) in one cooperative launch with grid
                                    barriers; 0: one launch per 64-column step */
-    MXP_OPT_TRSM_PAIR = 7       /* 1: TRSM-by-inverse products on the 2-SM kernel; 0 (default): 1-SM */
+    MXP_OPT_TRSM_PAIR = 7,      /* 1: TRSM-by-inverse products on the 2-SM kernel; 0 (default): 1-SM */
+    MXP_OPT_TEST_WITHHOLD_FLAG = 8  /* test of the bounded device waits: the next mxp_lu_solve never
+                                       publishes the completion flag of this 64-row block of the
+                                       forward solve, so the blocks waiting for it give up after
+                                       the 2 s bound and the call returns MXP_TIMEOUT (-1: off) */
 } mxp_option;
 mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int value);
 mxp_status mxp_workspace_destroy(mxp_workspace *ws);
@@ -223,7 +227,8 @@ mxp_status mxp_otf_gemv_noalloc(int n, uint64_t seed, const double *d_d, double 
 
 /* trsvL_h + trsvU_h (panel_trsv.hpp:308-597): x <- U^{-1} L^{-1} x with
  * the FP32 factors of mxp_panel_lu, vectors in FP64, exact block
- * substitution. */
+ * substitution.  Blocking: reads the workspace status word (MXP_TIMEOUT when a
+ * bounded wait between row blocks gave up). */
 mxp_status mxp_lu_solve(int n, const float *d_LU, int64_t lda, double *d_x, mxp_workspace *ws,
                         void *stream);
 

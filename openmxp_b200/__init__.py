@@ -156,6 +156,7 @@ OPT_MERGE_PANELS = 4
 OPT_SCHUR_PAIR = 5
 OPT_DIAG_COOP = 6
 OPT_TRSM_PAIR = 7
+OPT_TEST_WITHHOLD_FLAG = 8
 
 
 class Workspace:

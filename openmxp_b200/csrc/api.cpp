@@ -84,6 +84,7 @@ struct mxp_workspace {
     int merge = 1;           // merged look-ahead: two panels per trailing pass
     int pair = 0;            // trailing Schur products on the 2-SM (cta_group::2) kernel
     int trsm_pair = 0;       // TRSM-by-inverse products on the 2-SM kernel
+    int withhold = -1;       // test: row block whose TRSV flag the next mxp_lu_solve withholds
     size_t esize = 2;        // panel element size
     void *lpanel[2] = {nullptr, nullptr};
     void *rpanel[2] = {nullptr, nullptr};
@@ -244,6 +245,9 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
             return MXP_OK;
         case MXP_OPT_TRSM_PAIR:
             ws->trsm_pair = value ? 1 : 0;
+            return MXP_OK;
+        case MXP_OPT_TEST_WITHHOLD_FLAG:
+            ws->withhold = value;
             return MXP_OK;
         case MXP_OPT_GMRES_RESTART:
             if (value < 1 || value > 30) return fail(MXP_INVALID_ARG, "set_option: GMRES restart must be 1..30");
@@ -547,9 +551,11 @@ extern "C" mxp_status mxp_lu_solve(int n, const float *d_LU, int64_t lda, double
     if (!ws) return fail(MXP_INVALID_ARG, "lu_solve: workspace is NULL");
     if (n > ws->n) return fail(MXP_INVALID_ARG, "lu_solve: n larger than the workspace");
     cudaStream_t st = as_stream(stream);
-    mxp_status s = launch_lu_solve(n, d_LU, lda, d_x, ws->flags, ws->status, st);
+    const int withhold = ws->withhold;
+    ws->withhold = -1;  // one call only
+    mxp_status s = launch_lu_solve(n, d_LU, lda, d_x, ws->flags, ws->status, st, withhold);
     if (s != MXP_OK) return s;
-    return MXP_OK;
+    return read_status(ws, st);  // bounded-wait timeouts surface here
 }
 
 extern "C" mxp_status mxp_infnorm(int n, const double *d_x, double *h_out, mxp_workspace *ws,

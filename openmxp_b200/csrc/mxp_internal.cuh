@@ -166,8 +166,10 @@ mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ld
 mxp_status launch_otf_gemv(int n, uint64_t seed, const double *d, double alpha, const double *x,
                            double beta, double *y, double *partials, int max_splits,
                            cudaStream_t st);
+// withhold >= 0: the forward solve never publishes that row block's flag, so
+// the blocks that need it give up after the bounded wait (tests of MXP_TIMEOUT).
 mxp_status launch_lu_solve(int n, const float *LU, int64_t lda, double *x, int *flags,
-                           DevStatus *dst, cudaStream_t st);
+                           DevStatus *dst, cudaStream_t st, int withhold = -1);
 size_t lu_solve_flag_ints(int n);
 
 mxp_status launch_infnorm(int n, const double *x, double *out, cudaStream_t st);

@@ -129,7 +129,7 @@ constexpr size_t kTrsvSmem = 2 * sizeof(double) * kRB * (kRB + 1) + sizeof(float
 template <bool LOWER>
 __global__ void __launch_bounds__(kTrsvThreads)
 trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *flags,
-            DevStatus *dst) {
+            DevStatus *dst, int withhold) {
     extern __shared__ __align__(16) unsigned char trsv_smem[];
     double(*minv)[kRB + 1] = reinterpret_cast<double(*)[kRB + 1]>(trsv_smem);
     double(*pm)[kRB + 1] = minv + kRB;
@@ -310,7 +310,9 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
     if (ph == 0 && pi < nrows) __stcg(x + row0 + pi, w);
     __threadfence();
     __syncthreads();
-    if (tid == 0) st_release(&flags[rb], 1);  // published even after a timeout: successors never stall
+    // published even after a timeout, so successors never stall; `withhold` (a
+    // test of the bounded waits) leaves one block's flag unset
+    if (tid == 0 && rb != withhold) st_release(&flags[rb], 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -397,16 +399,16 @@ mxp_status launch_otf_gemv(int n, uint64_t seed, const double *d, double alpha, 
 size_t lu_solve_flag_ints(int n) { return 2 * ((size_t)cdiv(n, kRB) + 1); }
 
 mxp_status launch_lu_solve(int n, const float *LU, int64_t lda, double *x, int *flags,
-                           DevStatus *dst, cudaStream_t st) {
+                           DevStatus *dst, cudaStream_t st, int withhold) {
     if (n <= 0) return MXP_OK;
     if (lda < n) return fail(MXP_INVALID_ARG, "lu_solve: lda < n");
     const int nrb = (int)cdiv(n, kRB);
     MXP_CUDA(cudaMemsetAsync(flags, 0, lu_solve_flag_ints(n) * sizeof(int), st));
     MXP_CUDA(cudaFuncSetAttribute(trsv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
     MXP_CUDA(cudaFuncSetAttribute(trsv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
-    trsv_kernel<true><<<nrb, kTrsvThreads, kTrsvSmem, st>>>(n, LU, lda, x, flags, dst);
+    trsv_kernel<true><<<nrb, kTrsvThreads, kTrsvSmem, st>>>(n, LU, lda, x, flags, dst, withhold);
     MXP_LAUNCHED();
-    trsv_kernel<false><<<nrb, kTrsvThreads, kTrsvSmem, st>>>(n, LU, lda, x, flags + nrb + 1, dst);
+    trsv_kernel<false><<<nrb, kTrsvThreads, kTrsvSmem, st>>>(n, LU, lda, x, flags + nrb + 1, dst, -1);
     MXP_LAUNCHED();
     return MXP_OK;
 }
