@@ -64,6 +64,9 @@ typedef struct {
     int schur_launches;  /* tcgen05 Schur kernel launches */
     double ms_trsm_inv;  /* part of ms_trsm: FP32 triangular inverses */
     double ms_trsm_gemm; /* part of ms_trsm: tensor-core products against the inverses */
+    int overlapped_diag; /* diagonal factorisations run beside a trailing pass (not in ms_diag_lu;
+                            their time is inside ms_schur) */
+    int pad;
 } mxp_lu_stats;
 
 typedef struct {
@@ -108,10 +111,16 @@ typedef enum {
                                    the tensor-core TRSM) in one cooperative launch with grid
                                    barriers; 0: one launch per 64-column step */
     MXP_OPT_TRSM_PAIR = 7,      /* 1: TRSM-by-inverse products on the 2-SM kernel; 0 (default): 1-SM */
-    MXP_OPT_TEST_WITHHOLD_FLAG = 8  /* test of the bounded device waits: the next mxp_lu_solve never
+    MXP_OPT_TEST_WITHHOLD_FLAG = 8, /* test of the bounded device waits: the next mxp_lu_solve never
                                        publishes the completion flag of this 64-row block of the
                                        forward solve, so the blocks waiting for it give up after
                                        the 2 s bound and the call returns MXP_TIMEOUT (-1: off) */
+    MXP_OPT_OVERLAP_DIAG = 9,   /* merged schedule: > 0 factors the diagonal block of the next pair
+                                   on this many SMs on a second stream while the trailing pass
+                                   runs on the others (which take over its share of tiles when
+                                   it ends); 0 (default): in sequence */
+    MXP_OPT_OVERLAP_MIN = 10    /* overlap only while the trailing matrix of the pair has at least
+                                   this many blocks of rows (default 6) */
 } mxp_option;
 mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int value);
 mxp_status mxp_workspace_destroy(mxp_workspace *ws);

@@ -35,10 +35,11 @@ class MxpError(RuntimeError):
 class LuStats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_diag_lu", C.c_double), ("ms_trsm", C.c_double),
                 ("ms_cast", C.c_double), ("ms_schur", C.c_double), ("info", C.c_int),
-                ("schur_launches", C.c_int), ("ms_trsm_inv", C.c_double), ("ms_trsm_gemm", C.c_double)]
+                ("schur_launches", C.c_int), ("ms_trsm_inv", C.c_double), ("ms_trsm_gemm", C.c_double),
+                ("overlapped_diag", C.c_int), ("pad", C.c_int)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
 
 
 class IrStats(C.Structure):
@@ -157,12 +158,15 @@ OPT_SCHUR_PAIR = 5
 OPT_DIAG_COOP = 6
 OPT_TRSM_PAIR = 7
 OPT_TEST_WITHHOLD_FLAG = 8
+OPT_OVERLAP_DIAG = 9
+OPT_OVERLAP_MIN = 10
 
 
 class Workspace:
     def __init__(self, n: int, b: int, form: int | str = FORM_FP16, device: int = 0,
                  trsm_tensor: bool = True, merge_panels: bool = True, schur_pair: bool = False,
-                 diag_coop: bool = True):
+                 diag_coop: bool = True, overlap_diag: int | None = None,
+                 overlap_min: int | None = None):
         if isinstance(form, str):
             form = FORMS[form]
         self.n, self.b, self.form, self.device = n, b, form, device
@@ -173,6 +177,10 @@ class Workspace:
         self.set_option(OPT_MERGE_PANELS, int(merge_panels))
         self.set_option(OPT_SCHUR_PAIR, int(schur_pair))
         self.set_option(OPT_DIAG_COOP, int(diag_coop))
+        if overlap_diag is not None:
+            self.set_option(OPT_OVERLAP_DIAG, int(overlap_diag))
+        if overlap_min is not None:
+            self.set_option(OPT_OVERLAP_MIN, int(overlap_min))
 
     def set_option(self, key: int, value: int) -> None:
         check(lib().mxp_workspace_set_option(self.handle, key, value))

@@ -85,6 +85,12 @@ struct mxp_workspace {
     int pair = 0;            // trailing Schur products on the 2-SM (cta_group::2) kernel
     int trsm_pair = 0;       // TRSM-by-inverse products on the 2-SM kernel
     int withhold = -1;       // test: row block whose TRSV flag the next mxp_lu_solve withholds
+    // diagonal factorisation of the next pair overlapped with the trailing pass
+    int overlap = 0;         // SMs given to it (0: off)
+    int overlap_min = 6;     // minimum trailing size, in blocks
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    int *tile_ctr = nullptr;  // shared tile counter of the split trailing pass
     size_t esize = 2;        // panel element size
     void *lpanel[2] = {nullptr, nullptr};
     void *rpanel[2] = {nullptr, nullptr};
@@ -152,8 +158,12 @@ extern "C" mxp_status mxp_workspace_destroy(mxp_workspace *ws) {
     int cur = 0;
     cudaGetDevice(&cur);
     cudaSetDevice(ws->device);
+    if (ws->side) cudaStreamSynchronize(ws->side);
     for (void *p : ws->allocs) cudaFree(p);
     if (ws->h_scal) cudaFreeHost(ws->h_scal);
+    if (ws->ev_fork) cudaEventDestroy(ws->ev_fork);
+    if (ws->ev_join) cudaEventDestroy(ws->ev_join);
+    if (ws->side) cudaStreamDestroy(ws->side);
     cudaSetDevice(cur);
     delete ws;
     return MXP_OK;
@@ -199,11 +209,19 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
         ok = ok && (ws->tinv_tmp = (float *)alloc(((size_t)b * b / 4 + 64 * (size_t)b) * 4));
         ok = ok && (ws->coop_tmp = (float *)alloc(2 * diag_factor_tmp_floats(b) * 4));
         ok = ok && (ws->coop_sync = (unsigned int *)alloc(256));
+        if (ok) ws->tile_ctr = reinterpret_cast<int *>(ws->coop_sync + 32);
         ok = ok && (ws->split_big = alloc((size_t)rows * ws->ldk3 * 2 + 1024));
         ok = ok && (ws->split_u = alloc((size_t)b * ws->ldk3 * 2 + 1024));
         ok = ok && (ws->split_l = alloc((size_t)b * ws->ldk3 * 2 + 1024));
     }
     if (ok) ok = cudaMallocHost(&ws->h_scal, 64 * sizeof(double)) == cudaSuccess;
+    if (ok) {
+        int least = 0, greatest = 0;
+        ok = cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess &&
+             cudaStreamCreateWithPriority(&ws->side, cudaStreamNonBlocking, greatest) == cudaSuccess &&
+             cudaEventCreateWithFlags(&ws->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&ws->ev_join, cudaEventDisableTiming) == cudaSuccess;
+    }
     if (!ok) {
         cudaGetLastError();
         mxp_workspace_destroy(ws);
@@ -248,6 +266,15 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
             return MXP_OK;
         case MXP_OPT_TEST_WITHHOLD_FLAG:
             ws->withhold = value;
+            return MXP_OK;
+        case MXP_OPT_OVERLAP_DIAG:
+            if (value < 0 || value > num_sms() / 2)
+                return fail(MXP_INVALID_ARG, "set_option: overlap SMs must be 0..half the SM count");
+            ws->overlap = value;
+            return MXP_OK;
+        case MXP_OPT_OVERLAP_MIN:
+            if (value < 2) return fail(MXP_INVALID_ARG, "set_option: overlap minimum must be >= 2 blocks");
+            ws->overlap_min = value;
             return MXP_OK;
         case MXP_OPT_GMRES_RESTART:
             if (value < 1 || value > 30) return fail(MXP_INVALID_ARG, "set_option: GMRES restart must be 1..30");
@@ -419,27 +446,39 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
     // merged schedule needs FP8 scale tiles aligned to the block size
     const bool merge = ws->merge && (!fp8 || b % 128 == 0);
     auto schur = [&](int64_t mrows, int64_t ncols, int kfac, int64_t lrow, int64_t rrow, float *C,
-                     int store) -> mxp_status {
+                     int store, const SchurSched *sched = nullptr,
+                     cudaStream_t on = nullptr) -> mxp_status {
         ++schur_launches;
         return launch_schur(form, (int)mrows, (int)ncols, b * kfac, Lb + lrow * ldk * es, ldk,
                             fp8 ? Ls + (lrow / 128) * scl : nullptr, Rb + rrow * ldk * es, ldk,
-                            fp8 ? Rs + (rrow / 128) * scl : nullptr, C, lda, ws->status, st, store,
-                            scl, scl, 0, ws->pair);
+                            fp8 ? Rs + (rrow / 128) * scl : nullptr, C, lda, ws->status,
+                            on ? on : st, store, scl, scl, 0, ws->pair, sched);
     };
-    // Factor the diagonal block of step kk, solve its two panels, and cast them
-    // into panel slot `slot` (0 or 1) of the buffers at buffer row `row0`.
-    auto factor_panel = [&](int64_t kk, int slot, int64_t row0) -> mxp_status {
+    // LU of the diagonal block at kk and, for the tensor-core TRSM, the
+    // inverses of both triangles: one cooperative launch on `on`, at most
+    // max_grid CTAs (0: all SMs).
+    auto factor_diag = [&](int64_t kk, cudaStream_t on, int max_grid) -> mxp_status {
         float *Akk = d_A + kk + kk * lda;
-        pt.mark(PH_DIAG);
         const int m = n - (int)kk - b;
-        // one cooperative launch: LU of the diagonal block and, for the
-        // tensor-core TRSM, the inverses of both triangles
         const bool coop_inv = ws->coop && ws->trsm_tc && m > 0;
         float *tmpU = ws->coop_tmp, *tmpL = ws->coop_tmp + diag_factor_tmp_floats(b);
-        mxp_status q = ws->coop ? launch_diag_factor(b, Akk, lda, coop_inv ? ws->tinv_u : nullptr,
-                                                     coop_inv ? ws->tinv_l : nullptr, b, tmpU, tmpL,
-                                                     ws->coop_sync, ws->status, (int)kk, st)
-                                : launch_getrf_blocked(b, Akk, lda, ws->status, (int)kk, st);
+        return ws->coop ? launch_diag_factor(b, Akk, lda, coop_inv ? ws->tinv_u : nullptr,
+                                             coop_inv ? ws->tinv_l : nullptr, b, tmpU, tmpL,
+                                             ws->coop_sync, ws->status, (int)kk, on, max_grid)
+                        : launch_getrf_blocked(b, Akk, lda, ws->status, (int)kk, on);
+    };
+    // Factor the diagonal block of step kk (unless diag_done: it was factored
+    // on the side stream), solve its two panels, and cast them into panel slot
+    // `slot` (0 or 1) of the buffers at buffer row `row0`.
+    auto factor_panel = [&](int64_t kk, int slot, int64_t row0, bool diag_done) -> mxp_status {
+        float *Akk = d_A + kk + kk * lda;
+        const int m = n - (int)kk - b;
+        const bool coop_inv = ws->coop && ws->trsm_tc && m > 0;
+        mxp_status q = MXP_OK;
+        if (!diag_done) {
+            pt.mark(PH_DIAG);
+            q = factor_diag(kk, st, 0);
+        }
         if (q != MXP_OK || m <= 0) return q;
         float *Lcol = Akk + b;
         float *Urow = Akk + (int64_t)b * lda;
@@ -485,12 +524,19 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
         return q;
     };
 
+    // Overlap of the next pair's diagonal factorisation with the trailing pass
+    // (single-SM Schur kernel, cooperative diagonal kernel, whole tiles).
+    const int ovl_sms = ws->overlap > 0 && !ws->pair && ws->coop && b % 256 == 0
+                            ? std::min(ws->overlap, num_sms() / 2) : 0;
+    int overlapped = 0;
+    bool diag_done = false;
     int k = 0;
     while (k < nb && s == MXP_OK) {
         const int64_t kk = (int64_t)k * b;
         const int64_t base = kk + b;            // global row of buffer row 0
         const int64_t m = n - base;
-        s = factor_panel(kk, 0, 0);
+        s = factor_panel(kk, 0, 0, diag_done);
+        diag_done = false;
         if (s != MXP_OK || m <= 0) break;
         if (!merge || m == b) {
             // one panel per trailing pass (the reference's step structure)
@@ -505,14 +551,43 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
         s = schur(m, b, 1, 0, 0, d_A + base + base * lda, 0);                     // column block k+1
         if (s == MXP_OK) s = schur(b, m - b, 1, 0, b, d_A + base + (base + b) * lda, 0);  // row block k+1
         if (s != MXP_OK) break;
-        s = factor_panel(base, 1, b);
+        s = factor_panel(base, 1, b, false);
         if (s != MXP_OK) break;
         pt.mark(PH_SCHUR);
-        s = schur(m - b, m - b, 2, b, b, d_A + (base + b) + (base + b) * lda, 0);
+        const int64_t mt = m - b;                        // trailing size after the pair
+        float *T = d_A + (base + b) + (base + b) * lda;  // its leading element
+        if (ovl_sms == 0 || mt <= b || mt < (int64_t)ws->overlap_min * b) {
+            s = schur(mt, mt, 2, b, b, T, 0);
+            k += 2;
+            continue;
+        }
+        // The next diagonal block first (b x b corner of T), then, at the same
+        // time: its factorisation on ovl_sms SMs (side stream) and the rest of
+        // T on the other SMs; when the factorisation ends, a second launch on
+        // those SMs claims the tiles still left from the shared counter.
+        s = schur(b, b, 2, b, b, T, 0);
+        if (s != MXP_OK) break;
+        SchurSched main_part, late_part;
+        main_part.grid = num_sms() - ovl_sms;
+        late_part.grid = ovl_sms;
+        main_part.counter = late_part.counter = ws->tile_ctr;
+        main_part.skip_rows = late_part.skip_rows = b;
+        main_part.skip_cols = late_part.skip_cols = b;
+        MXP_CUDA(cudaMemsetAsync(ws->tile_ctr, 0, sizeof(int), st));
+        MXP_CUDA(cudaEventRecord(ws->ev_fork, st));
+        MXP_CUDA(cudaStreamWaitEvent(ws->side, ws->ev_fork, 0));
+        s = factor_diag(base + b, ws->side, ovl_sms);
+        if (s == MXP_OK) s = schur(mt, mt, 2, b, b, T, 0, &main_part);
+        if (s == MXP_OK) s = schur(mt, mt, 2, b, b, T, 0, &late_part, ws->side);
+        MXP_CUDA(cudaEventRecord(ws->ev_join, ws->side));
+        MXP_CUDA(cudaStreamWaitEvent(st, ws->ev_join, 0));
+        diag_done = true;
+        ++overlapped;
         k += 2;
     }
     pt.mark(PH_END);
     if (s != MXP_OK) {
+        cudaStreamSynchronize(ws->side);
         pt.collect(nullptr, 0);
         return s;
     }
@@ -530,6 +605,8 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
         stats->ms_total = ms[0] + ms[1] + ms[2] + ms[3] + ms[4] + ms[5];
         stats->info = h.code == MXP_ZERO_PIVOT ? h.info0 : 0;
         stats->schur_launches = schur_launches;
+        stats->overlapped_diag = overlapped;
+        stats->pad = 0;
     }
     return rs;
 }

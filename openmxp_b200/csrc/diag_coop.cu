@@ -163,7 +163,7 @@ size_t diag_factor_tmp_floats(int n) { return (size_t)n * n / 2 + (size_t)64 * n
 
 mxp_status launch_diag_factor(int n, float *A, int64_t lda, float *XU, float *XL, int64_t ldx,
                               float *tmpU, float *tmpL, unsigned int *sync_words, DevStatus *dst,
-                              int pivot_base, cudaStream_t st) {
+                              int pivot_base, cudaStream_t st, int max_grid) {
     if (n <= 0) return MXP_OK;
     if (lda < n || (XU && ldx < n)) return fail(MXP_INVALID_ARG, "diag_factor: bad leading dimension");
     if ((XU == nullptr) != (XL == nullptr)) return fail(MXP_INVALID_ARG, "diag_factor: both inverses or none");
@@ -174,6 +174,7 @@ mxp_status launch_diag_factor(int n, float *A, int64_t lda, float *XU, float *XL
     if (sms <= 0) return fail(MXP_UNSUPPORTED, "diag_factor: kernel cannot be made resident");
     const int tm = (n + GBM - 1) / GBM;
     int grid = min(sms, max(2, tm * tm));
+    if (max_grid > 0) grid = min(grid, max(2, max_grid));
     MXP_CUDA(cudaMemsetAsync(sync_words, 0, 2 * sizeof(unsigned int), st));
     Ctl ctl{sync_words, reinterpret_cast<int *>(sync_words + 1), dst};
     void *args[] = {&n, &A, &lda, &XU, &XL, &ldx, &tmpU, &tmpL, &ctl, &pivot_base};

@@ -125,9 +125,11 @@ inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s
 // (ld ldx).  tmpU/tmpL: diag_factor_tmp_floats(n) floats each; sync_words: 2
 // words of device memory (zeroed on the stream before the launch).
 size_t diag_factor_tmp_floats(int n);
+// max_grid > 0 caps the number of CTAs (the kernel then shares the GPU with
+// work launched on another stream).
 mxp_status launch_diag_factor(int n, float *A, int64_t lda, float *XU, float *XL, int64_t ldx,
                               float *tmpU, float *tmpL, unsigned int *sync_words, DevStatus *dst,
-                              int pivot_base, cudaStream_t st);
+                              int pivot_base, cudaStream_t st, int max_grid = 0);
 mxp_status launch_matgen_f64(int n, uint64_t seed, int diag_rule, double *A, int64_t lda,
                              cudaStream_t st);
 mxp_status launch_matgen(int n, uint64_t seed, int diag_rule, float *A, int64_t lda, double *d,
@@ -158,10 +160,23 @@ mxp_status launch_half_left_ref(const float *C, int m, int b, int64_t plda, uint
 mxp_status launch_half_right_trans_ref(const float *C, int b, int m, int64_t plda, uint16_t *rp,
                                        int64_t rplda, cudaStream_t st);
 
+// How one Schur launch takes its tiles (single-SM kernels only).  grid: CTAs
+// to launch (0: one per SM, at most the tile count).  counter: a device int,
+// zeroed before the first launch of a pass, from which every CTA of every
+// launch that shares it claims tiles (nullptr: static round robin).
+// skip_rows x skip_cols: leading corner of C that the pass leaves alone
+// (multiples of 128 and 256).
+struct SchurSched {
+    int grid = 0;
+    int *counter = nullptr;
+    int skip_rows = 0, skip_cols = 0;
+};
+
 mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ldl,
                         const uint8_t *lsc, const void *R, int64_t ldr, const uint8_t *rsc,
                         float *C, int64_t ldc, DevStatus *dst, cudaStream_t st, int store = 0,
-                        int lsc_ld = 0, int rsc_ld = 0, int tri_mode = 0, int pair = 0);
+                        int lsc_ld = 0, int rsc_ld = 0, int tri_mode = 0, int pair = 0,
+                        const SchurSched *sched = nullptr);
 
 mxp_status launch_otf_gemv(int n, uint64_t seed, const double *d, double alpha, const double *x,
                            double beta, double *y, double *partials, int max_splits,

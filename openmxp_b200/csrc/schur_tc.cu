@@ -46,7 +46,8 @@ constexpr int kStageBytesB = kBN * 128;
 constexpr int kEpiWarps = 8;
 constexpr int kThreads = 64 + 32 * kEpiWarps;  // 2 control warps + epilogue
 constexpr int kTmemCols = 512;
-constexpr int kSmemBytes = 1024 /*align slack*/ + kStages * (kStageBytesA + kStageBytesB) + 256;
+constexpr int kRing = 8;  // tile-index ring between the producer and the consumers
+constexpr int kSmemBytes = 1024 /*align slack*/ + kStages * (kStageBytesA + kStageBytesB) + 512;
 
 __host__ __device__ constexpr uint32_t idesc_f16(uint32_t ab_fmt) { return idesc_f16_mn(ab_fmt, kBM, kBN); }
 
@@ -62,10 +63,98 @@ struct TileMap {
     }
 };
 
+// Where a CTA's tiles come from.  counter == nullptr: static round robin
+// (blockIdx.x, + gridDim.x, ...).  Otherwise every tile is claimed from a
+// device counter (zeroed before the first launch that uses it), so several
+// launches with the same arguments can share one pass: a launch whose CTAs
+// start late simply claims fewer tiles.  Tiles with tm < skip_m and
+// tn < skip_n are not computed (a corner updated by another launch).
+struct TileSrc {
+    int *counter;
+    int skip_m, skip_n;
+};
+
+// Producer side: the next tile of this CTA, or -1 when the pass is done.
+__device__ __forceinline__ int fetch_tile(const TileMap &tiles, const TileSrc &src, int total,
+                                          int &t_static) {
+    for (;;) {
+        int t;
+        if (src.counter) {
+            t = atomicAdd(src.counter, 1);
+        } else {
+            t = t_static;
+            t_static += gridDim.x;
+        }
+        if (t >= total) return -1;
+        if (src.skip_m > 0) {
+            int tm, tn;
+            tiles.get(t, tm, tn);
+            if (tm < src.skip_m && tn < src.skip_n) continue;
+        }
+        return t;
+    }
+}
+
+// The ring: slot s holds a tile index; sfull[s] (count 1) is arrived by the
+// producer after writing it, sempty[s] (count 1 + kEpiWarps) by the MMA lane
+// and each epilogue warp after reading it.
+struct TileRing {
+    uint64_t *sfull, *sempty;
+    volatile int *ids;
+};
+
+__device__ __forceinline__ bool ring_put(const TileRing &r, int &slot, uint32_t &phase, int t,
+                                         volatile int *abort_flag) {
+    if (!mbar_wait(smem_u32(&r.sempty[slot]), phase ^ 1u, abort_flag)) return false;
+    r.ids[slot] = t;
+    mbar_arrive(smem_u32(&r.sfull[slot]));
+    if (++slot == kRing) {
+        slot = 0;
+        phase ^= 1u;
+    }
+    return true;
+}
+
+// Single-thread consumer (the MMA lane).
+__device__ __forceinline__ bool ring_take1(const TileRing &r, int &slot, uint32_t &phase, int &t,
+                                           volatile int *abort_flag) {
+    if (!mbar_wait(smem_u32(&r.sfull[slot]), phase, abort_flag)) return false;
+    t = r.ids[slot];
+    mbar_arrive(smem_u32(&r.sempty[slot]));
+    if (++slot == kRing) {
+        slot = 0;
+        phase ^= 1u;
+    }
+    return true;
+}
+
+// Whole-warp consumer (an epilogue warp): every lane waits and reads, the
+// warp agrees on success, lane 0 releases the slot.
+__device__ __forceinline__ bool ring_take_warp(const TileRing &r, int &slot, uint32_t &phase, int &t,
+                                               volatile int *abort_flag) {
+    const bool got = mbar_wait(smem_u32(&r.sfull[slot]), phase, abort_flag);
+    if (!__all_sync(0xffffffffu, got)) return false;
+    t = r.ids[slot];
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(smem_u32(&r.sempty[slot]));
+    if (++slot == kRing) {
+        slot = 0;
+        phase ^= 1u;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void ring_init(const TileRing &r) {
+    for (int s = 0; s < kRing; ++s) {
+        mbar_init(smem_u32(&r.sfull[s]), 1);
+        mbar_init(smem_u32(&r.sempty[s]), 1 + kEpiWarps);
+    }
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
 schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                     int M, int N, int K, float *__restrict__ C, int64_t ldc, uint32_t idesc,
-                    TileMap tiles, int store, int tri_mode, int seg, DevStatus *dst) {
+                    TileMap tiles, TileSrc src, int store, int tri_mode, int seg, DevStatus *dst) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                 ~uintptr_t(1023));
@@ -76,7 +165,9 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
     uint64_t *empty = bars + kStages;          // [kStages]
     uint64_t *tfull = bars + 2 * kStages;      // [2]
     uint64_t *tempty = bars + 2 * kStages + 2; // [2]
-    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 4);
+    const TileRing ring{bars + 2 * kStages + 4, bars + 2 * kStages + 4 + kRing,
+                        reinterpret_cast<volatile int *>(bars + 2 * kStages + 4 + 2 * kRing)};
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 4 + 2 * kRing) + kRing;
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_holder + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -100,6 +191,7 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             mbar_init(smem_u32(&tfull[a]), 1);
             mbar_init(smem_u32(&tempty[a]), kEpiWarps);
         }
+        ring_init(ring);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -121,8 +213,16 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
         if (lane == 0) {
             int stage = 0;
             uint32_t phase = 0;
+            int rslot = 0, t_static = blockIdx.x;
+            uint32_t rphase = 0;
             bool ok = true;
-            for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
+            while (ok) {
+                const int t = fetch_tile(tiles, src, total_tiles, t_static);
+                if (!ring_put(ring, rslot, rphase, t, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                if (t < 0) break;
                 int tm, tn;
                 tiles.get(t, tm, tn);
                 for (int kb = 0; kb < nk; ++kb) {
@@ -152,8 +252,16 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             int stage = 0;
             uint32_t phase = 0;
             uint32_t it = 0;
+            int rslot = 0;
+            uint32_t rphase = 0;
             bool ok = true;
-            for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x, ++it) {
+            for (;; ++it) {
+                int t;
+                if (!ring_take1(ring, rslot, rphase, t, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                if (t < 0) break;
                 int tm, tn;
                 tiles.get(t, tm, tn);
                 const uint32_t acc = it & 1u, acc_phase = (it >> 1) & 1u;
@@ -199,12 +307,20 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
         const int quarter = warp & 3;        // TMEM lane quarter this warp may access
         const int col_half = ew >> 2;        // which 128 columns of the 256
         uint32_t it = 0;
+        int rslot = 0;
+        uint32_t rphase = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
+        for (;; ++it) {
+            int t;
+            if (!ring_take_warp(ring, rslot, rphase, t, abort_flag)) {
+                ok = false;
+                break;
+            }
+            if (t < 0) break;
             int tm, tn;
             tiles.get(t, tm, tn);
             const uint32_t acc = it & 1u, acc_phase = (it >> 1) & 1u;
-            if (!mbar_wait(smem_u32(&tfull[acc]), acc_phase, abort_flag)) {
+            if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&tfull[acc]), acc_phase, abort_flag))) {
                 ok = false;
                 break;
             }
@@ -286,7 +402,7 @@ constexpr int kF8StageB = kF8BN * 128;
 constexpr int kF8StageSF = 2048;  // SFA 512 B + SFB 1024 B, padded
 constexpr int kF8StageBytes = kF8StageA + kF8StageB + kF8StageSF;
 constexpr int kF8Stages = 4;
-constexpr int kF8SmemBytes = 1024 + kF8Stages * kF8StageBytes + 256;
+constexpr int kF8SmemBytes = 1024 + kF8Stages * kF8StageBytes + 512;
 constexpr int kF8SfCol0 = 256;
 
 __device__ __forceinline__ void tc_cp_32x128b_x4(uint32_t taddr, uint64_t sdesc) {
@@ -327,7 +443,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                     int M, int N, int K, const uint8_t *__restrict__ lsc,
                     const uint8_t *__restrict__ rsc, int lsc_ld, int rsc_ld, float *__restrict__ C,
-                    int64_t ldc, TileMap tiles, DevStatus *dst) {
+                    int64_t ldc, TileMap tiles, TileSrc src, DevStatus *dst) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                 ~uintptr_t(1023));
@@ -336,7 +452,9 @@ schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
     uint64_t *empty = bars + kF8Stages;
     uint64_t *tfull = bars + 2 * kF8Stages;
     uint64_t *tempty = bars + 2 * kF8Stages + 1;
-    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + 2 * kF8Stages + 2);
+    const TileRing ring{bars + 2 * kF8Stages + 2, bars + 2 * kF8Stages + 2 + kRing,
+                        reinterpret_cast<volatile int *>(bars + 2 * kF8Stages + 2 + 2 * kRing)};
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + 2 * kF8Stages + 2 + 2 * kRing) + kRing;
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_holder + 1);
     auto stA = [&](int s) { return smem + s * kF8StageBytes; };
     auto stB = [&](int s) { return smem + s * kF8StageBytes + kF8StageA; };
@@ -354,6 +472,7 @@ schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
         }
         mbar_init(smem_u32(tfull), 1);
         mbar_init(smem_u32(tempty), kEpiWarps);
+        ring_init(ring);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -374,11 +493,40 @@ schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
         // ---------------- producer: scale factors (whole warp) + TMA (lane 0) ----------------
         int stage = 0;
         uint32_t phase = 0;
+        int rslot = 0, t_static = blockIdx.x;
+        uint32_t rphase = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
+        while (ok) {
+            int t = 0, put = 1;
+            if (lane == 0) {
+                t = fetch_tile(tiles, src, total_tiles, t_static);
+                put = ring_put(ring, rslot, rphase, t, abort_flag) ? 1 : 0;
+            }
+            t = __shfl_sync(0xffffffffu, t, 0);
+            if (!__shfl_sync(0xffffffffu, put, 0)) {
+                ok = false;
+                break;
+            }
+            if (t < 0) break;
             int tm, tn;
             tiles.get(t, tm, tn);
+            // Scale bytes of 64 stages at a time, lane i holding stages i and
+            // 32 + i: loaded before the slot wait, so the global-load latency
+            // stays off the per-stage path to the TMA issue.
+            uint32_t ra[2] = {0u, 0u}, rb0[2] = {0u, 0u}, rb1[2] = {127u, 127u};
+            const bool has_b1 = 2 * tn + 1 < rtiles;
             for (int kb = 0; kb < nk; ++kb) {
+                if ((kb & 63) == 0) {
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) {
+                        const int kx = kb + 32 * j + lane;
+                        if (kx < nk) {
+                            ra[j] = lsc[(int64_t)tm * lsc_ld + kx];
+                            rb0[j] = rsc[(int64_t)(2 * tn) * rsc_ld + kx];
+                            rb1[j] = has_b1 ? rsc[(int64_t)(2 * tn + 1) * rsc_ld + kx] : 127u;
+                        }
+                    }
+                }
                 int got = 1;
                 if (lane == 0) got = mbar_wait(smem_u32(&empty[stage]), phase ^ 1u, abort_flag) ? 1 : 0;
                 got = __shfl_sync(0xffffffffu, got, 0);
@@ -386,9 +534,19 @@ schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                     ok = false;
                     break;
                 }
-                const uint32_t sa = lsc[(int64_t)tm * lsc_ld + kb];
-                const uint32_t sb0 = rsc[(int64_t)(2 * tn) * rsc_ld + kb];
-                const uint32_t sb1 = (2 * tn + 1 < rtiles) ? rsc[(int64_t)(2 * tn + 1) * rsc_ld + kb] : 127u;
+                const bool hi = (kb & 32) != 0;
+                const int src_lane = kb & 31;
+                const uint32_t sa = __shfl_sync(0xffffffffu, hi ? ra[1] : ra[0], src_lane);
+                const uint32_t sb0 = __shfl_sync(0xffffffffu, hi ? rb0[1] : rb0[0], src_lane);
+                const uint32_t sb1 = __shfl_sync(0xffffffffu, hi ? rb1[1] : rb1[0], src_lane);
+                // operand tiles first (the barrier expects their bytes), then the
+                // stage's scale factors; the single arrival comes after both
+                const uint32_t fb = smem_u32(&full[stage]);
+                if (lane == 0) {
+                    mbar_expect_tx_only(fb, kF8StageA + kF8StageB);
+                    tma_load_2d(smem_u32(stA(stage)), &tmA, kb * 128, tm * kBM, fb);
+                    tma_load_2d(smem_u32(stB(stage)), &tmB, kb * 128, tn * kF8BN, fb);
+                }
                 const uint32_t wa = sa * 0x01010101u, wb0 = sb0 * 0x01010101u, wb1 = sb1 * 0x01010101u;
                 uint4 *sf = reinterpret_cast<uint4 *>(stSF(stage));
                 sf[lane] = make_uint4(wa, wa, wa, wa);             // SFA: rows 0..127
@@ -396,12 +554,7 @@ schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                 sf[64 + lane] = make_uint4(wb1, wb1, wb1, wb1);    // SFB atom 1: rows 128..255
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncwarp();
-                if (lane == 0) {
-                    const uint32_t fb = smem_u32(&full[stage]);
-                    mbar_expect_tx(fb, kF8StageA + kF8StageB);
-                    tma_load_2d(smem_u32(stA(stage)), &tmA, kb * 128, tm * kBM, fb);
-                    tma_load_2d(smem_u32(stB(stage)), &tmB, kb * 128, tn * kF8BN, fb);
-                }
+                if (lane == 0) mbar_arrive(fb);
                 if (++stage == kF8Stages) {
                     stage = 0;
                     phase ^= 1u;
@@ -418,8 +571,16 @@ schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             int stage = 0;
             uint32_t phase = 0;
             uint32_t it = 0;
+            int rslot = 0;
+            uint32_t rphase = 0;
             bool ok = true;
-            for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x, ++it) {
+            for (;; ++it) {
+                int t;
+                if (!ring_take1(ring, rslot, rphase, t, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                if (t < 0) break;
                 if (!mbar_wait(smem_u32(tempty), (it & 1u) ^ 1u, abort_flag)) {
                     ok = false;
                     break;
@@ -464,11 +625,19 @@ schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
         const int quarter = warp & 3;
         const int col_half = ew >> 2;
         uint32_t it = 0;
+        int rslot = 0;
+        uint32_t rphase = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
+        for (;; ++it) {
+            int t;
+            if (!ring_take_warp(ring, rslot, rphase, t, abort_flag)) {
+                ok = false;
+                break;
+            }
+            if (t < 0) break;
             int tm, tn;
             tiles.get(t, tm, tn);
-            if (!mbar_wait(smem_u32(tfull), it & 1u, abort_flag)) {
+            if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(tfull), it & 1u, abort_flag))) {
                 ok = false;
                 break;
             }
@@ -573,10 +742,12 @@ mxp_status launch_schur2(int form, int m, int n, int k, const void *L, int64_t l
 mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ldl,
                         const uint8_t *lsc, const void *R, int64_t ldr, const uint8_t *rsc,
                         float *C, int64_t ldc, DevStatus *dst, cudaStream_t st, int store,
-                        int lsc_ld, int rsc_ld, int tri_mode, int pair) {
-    if (pair)
+                        int lsc_ld, int rsc_ld, int tri_mode, int pair, const SchurSched *sched) {
+    if (pair) {
+        if (sched) return fail(MXP_UNSUPPORTED, "schur: tile schedules are single-SM only");
         return launch_schur2(form, m, n, k, L, ldl, lsc, R, ldr, rsc, C, ldc, dst, st, store, lsc_ld,
                              rsc_ld, tri_mode);
+    }
     if (m < 0 || n < 0 || k < 0) return fail(MXP_INVALID_ARG, "schur: negative size");
     if (m == 0 || n == 0 || k == 0) return MXP_OK;
     if (ldc < m) return fail(MXP_INVALID_ARG, "schur: ldc < m");
@@ -590,8 +761,20 @@ mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ld
     tiles.tiles_n = (int)cdiv(n, form == MXP_FORM_FP8 ? kF8BN : kBN);
     tiles.group_m = 16;
     const int64_t total = (int64_t)tiles.tiles_m * tiles.tiles_n;
-    if (total > (int64_t)1 << 31) return fail(MXP_INVALID_ARG, "schur: too many tiles");
-    const int grid = (int)(total < num_sms() ? total : num_sms());
+    if (total > (int64_t)1 << 30) return fail(MXP_INVALID_ARG, "schur: too many tiles");
+    const int bn = form == MXP_FORM_FP8 ? kF8BN : kBN;
+    TileSrc src{nullptr, 0, 0};
+    int grid = (int)(total < num_sms() ? total : num_sms());
+    if (sched) {
+        if (sched->grid < 0 || sched->skip_rows < 0 || sched->skip_cols < 0)
+            return fail(MXP_INVALID_ARG, "schur: bad tile schedule");
+        if (sched->skip_rows % kBM != 0 || sched->skip_cols % bn != 0)
+            return fail(MXP_INVALID_ARG, "schur: skipped corner must be whole tiles");
+        if (sched->grid > 0) grid = (int)imin64(grid, sched->grid);
+        src.counter = sched->counter;
+        src.skip_m = sched->skip_rows / kBM;
+        src.skip_n = sched->skip_cols / bn;
+    }
     CUtensorMap mapA, mapB;
     if (form == MXP_FORM_FP8) {
         if (!lsc || !rsc) return fail(MXP_INVALID_ARG, "schur: FP8 form needs both scale tables");
@@ -609,7 +792,7 @@ mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ld
         const int kt = (int)cdiv(K, 128);
         schur_tc_fp8_kernel<<<grid, kThreads, kF8SmemBytes, st>>>(
             mapA, mapB, m, n, (int)K, lsc, rsc, lsc_ld > 0 ? lsc_ld : kt, rsc_ld > 0 ? rsc_ld : kt, C,
-            ldc, tiles, dst);
+            ldc, tiles, src, dst);
         MXP_LAUNCHED();
         return MXP_OK;
     }
@@ -629,7 +812,7 @@ mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ld
     // the triangular skip needs whole stages inside one K segment
     if (tri_mode != 0 && (k % 64 != 0)) tri_mode = 0;
     schur_tc_f16_kernel<<<grid, kThreads, kSmemBytes, st>>>(mapA, mapB, m, n, (int)K, C, ldc, idesc,
-                                                            tiles, store, tri_mode, k, dst);
+                                                            tiles, src, store, tri_mode, k, dst);
     MXP_LAUNCHED();
     return MXP_OK;
 }
