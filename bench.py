@@ -227,7 +227,7 @@ def workload_config(args):
             "n": args.n, "b": args.b, "seed": args.seed, "form": args.form,
             "compare": args.compare,
             "diag_rule": "rowsum" if args.diag_rule == 0 else "0.55*rowsum+1",
-            "ir": args.ir, "trsm": args.trsm,
+            "ir": args.ir, "trsm": args.trsm, "compare_trsm": args.compare_trsm,
             "parallelism": "replicas (one independent system per GPU)",
             "l2": f"inputs larger than L2 (A = {args.n * args.n * 4 / 1e9:.1f} GB per GPU)"}
 
@@ -235,7 +235,7 @@ def workload_config(args):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
-def _solve_arm(args, form_name, p, dev, dist, local, e2e_on):
+def _solve_arm(args, form_name, p, dev, dist, local, e2e_on, trsm=None):
     """Warm up, then time args.steps solves of form `form_name` on problem p."""
     import torch
 
@@ -244,7 +244,9 @@ def _solve_arm(args, form_name, p, dev, dist, local, e2e_on):
     ws_n = dist_env()[0]
     form = mxp.FORMS[form_name]
     n, b = args.n, args.b
-    ws = mxp.Workspace(n, b, form, device=local, trsm_tensor=(args.trsm == "tensor"))
+    trsm = args.trsm if trsm is None else trsm
+    ws = mxp.Workspace(n, b, form, device=local, trsm_tensor=(trsm != "simt"),
+                       trsm_single=(trsm == "single"))
     if args.trsm_pair:
         ws.set_option(mxp.OPT_TRSM_PAIR, 1)
     if args.overlap_diag is not None:
@@ -388,7 +390,7 @@ def run_gpu(args):
     arm = _solve_arm(args, args.form, p, dev, dist, local, not args.no_e2e)
     plain = None
     if args.compare not in ("none", args.form):
-        plain = _solve_arm(args, args.compare, p, dev, dist, local, False)
+        plain = _solve_arm(args, args.compare, p, dev, dist, local, False, trsm=args.compare_trsm)
     rhs = p.rhs.clone()
     del p
     torch.cuda.empty_cache()
@@ -658,7 +660,12 @@ def parse(argv=None):
     ap.add_argument("--diag-rule", type=int, default=0)
     ap.add_argument("--maxit", type=int, default=50)
     ap.add_argument("--ir", choices=["classic", "gmres"], default="classic")
-    ap.add_argument("--trsm", choices=["tensor", "simt"], default="tensor")
+    ap.add_argument("--trsm", choices=["auto", "tensor", "single", "simt"], default="auto",
+                    help="panel TRSM: tensor-core by inverse in three split-BF16 products (near FP32), "
+                         "one BF16 product, or SIMT FP32; auto = single for the FP8 form "
+                         "(its panels are E4M3 next), tensor otherwise")
+    ap.add_argument("--compare-trsm", choices=["tensor", "single", "simt"], default="tensor",
+                    help="panel TRSM of the --compare arm (the plain method: FP32-accurate)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -685,6 +692,8 @@ def parse(argv=None):
 
 def main(argv=None):
     args = parse(argv)
+    if args.trsm == "auto":
+        args.trsm = "single" if args.form == "fp8" else "tensor"
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":

@@ -119,8 +119,12 @@ typedef enum {
                                    on this many SMs on a second stream while the trailing pass
                                    runs on the others (which take over its share of tiles when
                                    it ends); 0 (default): in sequence */
-    MXP_OPT_OVERLAP_MIN = 10    /* overlap only while the trailing matrix of the pair has at least
+    MXP_OPT_OVERLAP_MIN = 10,   /* overlap only while the trailing matrix of the pair has at least
                                    this many blocks of rows (default 6) */
+    MXP_OPT_TRSM_SINGLE = 11    /* tensor-core TRSM by inverse: 0 (default) three split-BF16 products
+                                   (hi*hi + hi*lo + lo*hi, near FP32); 1: one BF16 product, K = b
+                                   (relative error ~2^-9, the reference's Alt-TRSM idea with BF16's
+                                   range in place of FP16's) */
 } mxp_option;
 mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int value);
 mxp_status mxp_workspace_destroy(mxp_workspace *ws);

@@ -160,13 +160,14 @@ OPT_TRSM_PAIR = 7
 OPT_TEST_WITHHOLD_FLAG = 8
 OPT_OVERLAP_DIAG = 9
 OPT_OVERLAP_MIN = 10
+OPT_TRSM_SINGLE = 11
 
 
 class Workspace:
     def __init__(self, n: int, b: int, form: int | str = FORM_FP16, device: int = 0,
                  trsm_tensor: bool = True, merge_panels: bool = True, schur_pair: bool = False,
                  diag_coop: bool = True, overlap_diag: int | None = None,
-                 overlap_min: int | None = None):
+                 overlap_min: int | None = None, trsm_single: bool | None = None):
         if isinstance(form, str):
             form = FORMS[form]
         self.n, self.b, self.form, self.device = n, b, form, device
@@ -181,6 +182,8 @@ class Workspace:
             self.set_option(OPT_OVERLAP_DIAG, int(overlap_diag))
         if overlap_min is not None:
             self.set_option(OPT_OVERLAP_MIN, int(overlap_min))
+        if trsm_single is not None:
+            self.set_option(OPT_TRSM_SINGLE, int(trsm_single))
 
     def set_option(self, key: int, value: int) -> None:
         check(lib().mxp_workspace_set_option(self.handle, key, value))

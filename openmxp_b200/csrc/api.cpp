@@ -104,6 +104,7 @@ struct mxp_workspace {
     int *flags = nullptr;
     // tensor-core panel TRSM: FP32 triangular inverses and split-BF16 operands
     int trsm_tc = 1;
+    int trsm_single = 0;     // one BF16 product instead of three split products
     int64_t ldk3 = 0;
     float *tinv_u = nullptr, *tinv_l = nullptr, *tinv_tmp = nullptr;
     // cooperative diagonal-block factorisation (LU + inverses in one launch)
@@ -271,6 +272,9 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
             if (value < 0 || value > num_sms() / 2)
                 return fail(MXP_INVALID_ARG, "set_option: overlap SMs must be 0..half the SM count");
             ws->overlap = value;
+            return MXP_OK;
+        case MXP_OPT_TRSM_SINGLE:
+            ws->trsm_single = value ? 1 : 0;
             return MXP_OK;
         case MXP_OPT_OVERLAP_MIN:
             if (value < 2) return fail(MXP_INVALID_ARG, "set_option: overlap minimum must be >= 2 blocks");
@@ -488,7 +492,7 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
             // lo*hi) tensor-core products against FP32 triangular inverses; the same
             // TRSM-by-inverse idea as the reference's -alt path (panel_trf_gdirect.hpp:73-142)
             // at near-FP32 accuracy instead of FP16.
-            const int bf = MXP_FORM_BF16X2;
+            const int bf = ws->trsm_single ? kFormBf16 : MXP_FORM_BF16X2;
             if (!coop_inv) {
                 pt.mark(PH_TINV);
                 q = launch_tri_inv_upper(b, Akk, lda, ws->tinv_u, b, ws->tinv_tmp, st);

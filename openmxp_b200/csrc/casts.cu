@@ -14,6 +14,8 @@
 //   BF16X2  : hi = bf16(x), lo = bf16(x - hi); the K-major row is laid out
 //             as three K segments (left: hi|hi|lo, right: hi|lo|hi) so one
 //             GEMM with K' = 3b accumulates hi*hi + hi*lo + lo*hi.
+//   BF16    : (internal, kFormBf16) bf16(x) only, K = b: the operands of the
+//             single-product TRSM by inverse.
 //   FP8     : E4M3 (satfinite) of x * 2^e with one power-of-two scale per
 //             128 x 128 tile of the panel, e the largest exponent keeping the
 //             tile's amax <= 448; the UE8M0 byte 127 - e (value 2^-e) is
@@ -36,6 +38,8 @@ __device__ __forceinline__ void store_lowp(void *out, int64_t ldk, int64_t row, 
                                            float x, bool is_right) {
     if (FORM == MXP_FORM_FP16) {
         reinterpret_cast<__half *>(out)[row * ldk + k] = __float2half_rn(x);
+    } else if (FORM == kFormBf16) {
+        reinterpret_cast<__nv_bfloat16 *>(out)[row * ldk + k] = __float2bfloat16_rn(x);
     } else {  // BF16X2
         __nv_bfloat16 *o = reinterpret_cast<__nv_bfloat16 *>(out) + row * ldk;
         const __nv_bfloat16 hi = __float2bfloat16_rn(x);
@@ -64,6 +68,12 @@ __device__ __forceinline__ void store8(void *out, int64_t ldk, int64_t row, int 
         uint4 w = make_uint4(pack_h2(v[0], v[1]), pack_h2(v[2], v[3]), pack_h2(v[4], v[5]),
                              pack_h2(v[6], v[7]));
         *reinterpret_cast<uint4 *>(reinterpret_cast<__half *>(out) + row * ldk + k0) = w;
+    } else if (FORM == kFormBf16) {
+        __nv_bfloat16 h[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16_rn(v[q]);
+        *reinterpret_cast<uint4 *>(reinterpret_cast<__nv_bfloat16 *>(out) + row * ldk + k0) =
+            make_uint4(pack_bf2(h[0], h[1]), pack_bf2(h[2], h[3]), pack_bf2(h[4], h[5]), pack_bf2(h[6], h[7]));
     } else {
         __nv_bfloat16 hi[8], lo[8];
 #pragma unroll
@@ -325,7 +335,7 @@ static mxp_status check_cast_args(int form, int m, int b, int64_t lda, int64_t l
     if (lda < 1) return fail(MXP_INVALID_ARG, "panel cast: bad lda");
     const int64_t K = (form == MXP_FORM_BF16X2) ? 3 * (int64_t)b : b;
     if (ldk < K) return fail(MXP_INVALID_ARG, "panel cast: ldk smaller than the K extent");
-    if (form != MXP_FORM_FP16 && form != MXP_FORM_BF16X2 && form != MXP_FORM_FP8)
+    if (form != MXP_FORM_FP16 && form != MXP_FORM_BF16X2 && form != MXP_FORM_FP8 && form != kFormBf16)
         return fail(MXP_INVALID_ARG, "panel cast: unknown form");
     return MXP_OK;
 }
@@ -345,6 +355,8 @@ mxp_status launch_cast_left(int form, int m, int b, const float *A, int64_t lda,
         dim3 grid((unsigned)cdiv(m, kTile), (unsigned)cdiv(b, kTile));
         if (form == MXP_FORM_FP16)
             cast_left_kernel<MXP_FORM_FP16><<<grid, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk, vec);
+        else if (form == kFormBf16)
+            cast_left_kernel<kFormBf16><<<grid, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk, vec);
         else
             cast_left_kernel<MXP_FORM_BF16X2><<<grid, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk, vec);
     }
@@ -368,6 +380,8 @@ mxp_status launch_cast_right(int form, int m, int b, const float *A, int64_t lda
         const unsigned blocks = (unsigned)cdiv(threads, kCastThreads);
         if (form == MXP_FORM_FP16)
             cast_right_kernel<MXP_FORM_FP16><<<blocks, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk, vec);
+        else if (form == kFormBf16)
+            cast_right_kernel<kFormBf16><<<blocks, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk, vec);
         else
             cast_right_kernel<MXP_FORM_BF16X2><<<blocks, kCastThreads, 0, st>>>(m, b, A, lda, out,
                                                                                  ldk, vec);

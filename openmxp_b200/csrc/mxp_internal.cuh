@@ -119,6 +119,10 @@ __host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { retur
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Internal operand form of the panel casts and the tensor-core GEMM: one BF16
+// value per element, K = b (the single-product TRSM by inverse).
+constexpr int kFormBf16 = 3;
+
 // Launchers implemented in the individual translation units ---------------
 // Cooperative diagonal-block factorisation (diag_coop.cu): in-place no-pivot LU
 // of the n x n block A and, when XU/XL are given, inv(U) -> XU and inv(L) -> XL

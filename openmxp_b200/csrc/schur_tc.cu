@@ -751,7 +751,7 @@ mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ld
     if (m < 0 || n < 0 || k < 0) return fail(MXP_INVALID_ARG, "schur: negative size");
     if (m == 0 || n == 0 || k == 0) return MXP_OK;
     if (ldc < m) return fail(MXP_INVALID_ARG, "schur: ldc < m");
-    if (form != MXP_FORM_FP16 && form != MXP_FORM_BF16X2 && form != MXP_FORM_FP8)
+    if (form != MXP_FORM_FP16 && form != MXP_FORM_BF16X2 && form != MXP_FORM_FP8 && form != kFormBf16)
         return fail(MXP_INVALID_ARG, "schur: unknown form");
     if (m > (1 << 30) || n > (1 << 30)) return fail(MXP_INVALID_ARG, "schur: size too large");
     const int64_t K = (form == MXP_FORM_BF16X2) ? 3 * (int64_t)k : k;
