@@ -141,7 +141,7 @@ cast_left_kernel(int m, int b, const float *__restrict__ A, int64_t lda, void *o
 template <int FORM>
 __global__ void __launch_bounds__(kCastThreads)
 cast_right_kernel(int m, int b, const float *__restrict__ A, int64_t lda, void *out, int64_t ldk,
-                  bool vec) {
+                  bool vec, bool vec_in) {
     const int64_t gid = (int64_t)blockIdx.x * kCastThreads + threadIdx.x;
     const int kchunks = (b + 7) / 8;
     const int64_t j = gid / kchunks;
@@ -150,8 +150,15 @@ cast_right_kernel(int m, int b, const float *__restrict__ A, int64_t lda, void *
     const float *src = A + j * lda;
     if (vec && k0 + 8 <= b) {
         float v[8];
+        if (vec_in) {  // two 16-byte loads (column start 16-byte aligned, k0 % 8 == 0)
+            const float4 a = *reinterpret_cast<const float4 *>(src + k0);
+            const float4 c = *reinterpret_cast<const float4 *>(src + k0 + 4);
+            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+            v[4] = c.x; v[5] = c.y; v[6] = c.z; v[7] = c.w;
+        } else {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) v[q] = src[k0 + q];
+            for (int q = 0; q < 8; ++q) v[q] = src[k0 + q];
+        }
         store8<FORM>(out, ldk, j, k0, b, v, true);
         return;
     }
@@ -246,48 +253,57 @@ cast_left_fp8_kernel(int m, int b, const float *__restrict__ A, int64_t lda, uin
     }
 }
 
-// R panel (U^T rows), FP8: one CTA per 128 (rows j) x 128 (k) tile.
+// R panel (U^T rows), FP8: one CTA per 128 (rows j) x 128 (k) tile.  Column j
+// of U holds the 128 k of the tile contiguously, and so does row j of R: warp
+// w takes the 16 columns j0 + 16w .. +15, reading each as one 512-byte float4
+// load across its lanes (lane l: k = 4l .. 4l+3) and writing it as one
+// 128-byte row of E4M3 (one 32-bit word per lane).  vec4: A and lda keep
+// every column start 16-byte aligned and out rows 4-byte aligned.
 __global__ void __launch_bounds__(kCastThreads)
 cast_right_fp8_kernel(int m, int b, const float *__restrict__ A, int64_t lda, uint8_t *out,
-                      int64_t ldk, uint8_t *scales, int sc_ld) {
+                      int64_t ldk, uint8_t *scales, int sc_ld, bool vec4) {
     __shared__ float red[kCastThreads / 32];
     const int j0 = blockIdx.x * kF8Tile, k0 = blockIdx.y * kF8Tile;
-    const int t = threadIdx.x;
-    const int jj = t / 2, half = t % 2;
-    const int64_t j = j0 + jj;
-    float v[64];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kl = k0 + 4 * lane;  // first of this lane's 4 k
+    float4 v[16];
     float amax = 0.0f;
-    const float *src = A + j * lda + k0 + half * 64;
 #pragma unroll
-    for (int q = 0; q < 64; ++q) {
-        const int k = k0 + half * 64 + q;
-        v[q] = (j < m && k < b) ? src[q] : 0.0f;
-        amax = fmaxf(amax, fabsf(v[q]));
+    for (int c = 0; c < 16; ++c) {
+        const int64_t j = j0 + 16 * warp + c;
+        const float *src = A + j * lda + kl;
+        float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (j < m) {
+            if (vec4 && kl + 4 <= b) {
+                x = *reinterpret_cast<const float4 *>(src);
+            } else {
+                if (kl + 0 < b) x.x = src[0];
+                if (kl + 1 < b) x.y = src[1];
+                if (kl + 2 < b) x.z = src[2];
+                if (kl + 3 < b) x.w = src[3];
+            }
+        }
+        v[c] = x;
+        amax = fmaxf(amax, fmaxf(fmaxf(fabsf(x.x), fabsf(x.y)), fmaxf(fabsf(x.z), fabsf(x.w))));
     }
     amax = block_max_256(amax, red);
     const int e = e4m3_scale_exp(amax);
     const float up = __int_as_float((e + 127) << 23);
-    if (t == 0) scales[(int64_t)blockIdx.x * sc_ld + blockIdx.y] = (uint8_t)(127 - e);
-    if (j >= m) return;
-    uint8_t *dst = out + j * ldk + k0 + half * 64;
-    const int kvalid = min(64, b - (k0 + half * 64));
-    if (kvalid <= 0) return;
-    if (kvalid == 64) {
+    if (threadIdx.x == 0) scales[(int64_t)blockIdx.x * sc_ld + blockIdx.y] = (uint8_t)(127 - e);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            uint32_t w[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                uint32_t x = 0;
-#pragma unroll
-                for (int s = 0; s < 4; ++s)
-                    x |= (uint32_t)to_e4m3(__fmul_rn(v[16 * q + 4 * r + s], up)) << (8 * s);
-                w[r] = x;
-            }
-            reinterpret_cast<uint4 *>(dst)[q] = make_uint4(w[0], w[1], w[2], w[3]);
+    for (int c = 0; c < 16; ++c) {
+        const int64_t j = j0 + 16 * warp + c;
+        if (j >= m || kl >= b) continue;
+        const float4 x = v[c];
+        const uint32_t w = (uint32_t)to_e4m3(__fmul_rn(x.x, up)) | ((uint32_t)to_e4m3(__fmul_rn(x.y, up)) << 8) |
+                           ((uint32_t)to_e4m3(__fmul_rn(x.z, up)) << 16) |
+                           ((uint32_t)to_e4m3(__fmul_rn(x.w, up)) << 24);
+        uint8_t *dst = out + j * ldk + kl;
+        if (vec4 && kl + 4 <= b) {
+            *reinterpret_cast<uint32_t *>(dst) = w;
+        } else {
+            for (int q = 0; q < 4 && kl + q < b; ++q) dst[q] = (uint8_t)(w >> (8 * q));
         }
-    } else {
-        for (int q = 0; q < kvalid; ++q) dst[q] = to_e4m3(__fmul_rn(v[q], up));
     }
 }
 
@@ -372,19 +388,23 @@ mxp_status launch_cast_right(int form, int m, int b, const float *A, int64_t lda
     if (form == MXP_FORM_FP8) {
         if (!scales) return fail(MXP_INVALID_ARG, "FP8 cast needs a scale buffer");
         dim3 grid((unsigned)cdiv(m, kF8Tile), (unsigned)cdiv(b, kF8Tile));
+        const bool vec4 = (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (lda % 4 == 0) &&
+                          (reinterpret_cast<uintptr_t>(out) % 4 == 0) && (ldk % 4 == 0);
         cast_right_fp8_kernel<<<grid, kCastThreads, 0, st>>>(m, b, A, lda, (uint8_t *)out, ldk,
-                                                             scales, sc_ld > 0 ? sc_ld : (int)grid.y);
+                                                             scales, sc_ld > 0 ? sc_ld : (int)grid.y, vec4);
     } else {
         const bool vec = vec_ok(out, ldk, b);
+        const bool vec_in = (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (lda % 4 == 0);
         const int64_t threads = (int64_t)m * ((b + 7) / 8);
         const unsigned blocks = (unsigned)cdiv(threads, kCastThreads);
         if (form == MXP_FORM_FP16)
-            cast_right_kernel<MXP_FORM_FP16><<<blocks, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk, vec);
+            cast_right_kernel<MXP_FORM_FP16><<<blocks, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk, vec,
+                                                                              vec_in);
         else if (form == kFormBf16)
-            cast_right_kernel<kFormBf16><<<blocks, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk, vec);
+            cast_right_kernel<kFormBf16><<<blocks, kCastThreads, 0, st>>>(m, b, A, lda, out, ldk, vec, vec_in);
         else
             cast_right_kernel<MXP_FORM_BF16X2><<<blocks, kCastThreads, 0, st>>>(m, b, A, lda, out,
-                                                                                 ldk, vec);
+                                                                                 ldk, vec, vec_in);
     }
     MXP_LAUNCHED();
     return MXP_OK;
