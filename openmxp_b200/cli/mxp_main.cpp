@@ -9,8 +9,10 @@
 //
 // P x Q must be 1 x 1 (one GPU).  -alt 0 solves the panels with the SIMT TRSM
 // (the reference's "Default Trsm"), 1 and 2 with the tensor-core TRSM by
-// inverse (its "Alt-Trsm" family).  Options the single-GPU path does not
-// have are reported as ignored, as the reference does with unknown options.
+// inverse (its "Alt-Trsm" family): 1 as three split-BF16 products (near FP32),
+// 2 as one BF16 product (the low-precision GEMM of the reference's alt 2).
+// Options the single-GPU path does not have are reported as ignored, as the
+// reference does with unknown options.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -133,6 +135,7 @@ int main(int argc, char **argv) {
     mxp_status s = mxp_workspace_create(n, b, a.form, 0, &ws);
     if (s != MXP_OK) return die("workspace_create", s);
     mxp_workspace_set_option(ws, MXP_OPT_TRSM_TENSOR, a.alt == 0 ? 0 : 1);
+    mxp_workspace_set_option(ws, MXP_OPT_TRSM_SINGLE, a.alt == 2 ? 1 : 0);
     std::printf("\tjobid=%d\n", a.jobid);
     std::printf("\tn=%d ln=%d b=%d r=%d c=%d epoch_size=%d\n", n, n, b, 0, 0, b);
 
