@@ -228,6 +228,7 @@ def workload_config(args):
             "compare": args.compare,
             "diag_rule": "rowsum" if args.diag_rule == 0 else "0.55*rowsum+1",
             "ir": args.ir, "trsm": args.trsm, "compare_trsm": args.compare_trsm,
+            "merge_depth": args.merge_depth if args.merge_depth is not None else 3,
             "parallelism": "replicas (one independent system per GPU)",
             "l2": f"inputs larger than L2 (A = {args.n * args.n * 4 / 1e9:.1f} GB per GPU)"}
 
@@ -249,6 +250,8 @@ def _solve_arm(args, form_name, p, dev, dist, local, e2e_on, trsm=None):
                        trsm_single=(trsm == "single"))
     if args.trsm_pair:
         ws.set_option(mxp.OPT_TRSM_PAIR, 1)
+    if args.merge_depth is not None:
+        ws.set_option(mxp.OPT_MERGE_DEPTH, args.merge_depth)
     if args.overlap_diag is not None:
         ws.set_option(mxp.OPT_OVERLAP_DIAG, args.overlap_diag)
     if args.overlap_min is not None:
@@ -332,14 +335,15 @@ def _solve_arm(args, form_name, p, dev, dist, local, e2e_on, trsm=None):
 SCHUR_TRAFFIC_RATIO = {"schur_tc_f16_kernel": 2.853 / 2.315, "schur_tc_fp8_kernel": 2.857 / 2.315}
 
 
-def _schur_launch_bytes(n, b, es, kmul):
-    """Average algorithmic bytes of one trailing Schur launch of the merged schedule."""
+def _schur_launch_bytes(n, b, es, kmul, depth=3):
+    """Average algorithmic bytes of one trailing Schur launch of the merged
+    schedule (groups of `depth` panels, K = depth * b)."""
     tot, cnt = 0.0, 0
-    for k in range(0, n // b, 2):
-        m = n - (k + 2) * b
+    for k in range(0, n // b, depth):
+        m = n - (k + depth) * b
         if m <= 0:
             break
-        K = 2 * b * kmul
+        K = depth * b * kmul
         tot += 8.0 * m * m + 2.0 * m * K * es
         cnt += 1
     return tot / max(cnt, 1)
@@ -364,14 +368,18 @@ def _roofline(args, arm):
         peak, src = bf16, f"{peak_kind} bf16 dense sustained (MEASURED_PEAKS.json)"
         kern = "schur_tc_f16_kernel"
     achieved = sflops / (schur_ms / 1e3) / 1e12 if schur_ms > 0 else None
-    alg = _schur_launch_bytes(args.n, args.b, es, kmul)
+    depth = args.merge_depth if args.merge_depth is not None else 3
+    alg = _schur_launch_bytes(args.n, args.b, es, kmul, depth)
     return {"bound": "tensor", "kernel": kern, "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
             "peak_source": src,
             "traffic": SCHUR_TRAFFIC_RATIO[kern] * alg if kern in SCHUR_TRAFFIC_RATIO else None,
             "traffic_note": ("bytes per average trailing launch: ncu DRAM/algorithmic ratio at "
                              "m=16384 times the launch's algorithmic bytes"),
-            "algorithmic_per_launch": "2*m_k^2*K flops, m_k = N-(k+1)B, K = B (x3 for bf16x2)"}
+            "algorithmic_per_launch": ("achieved: sum over steps of 2*m_k^2*B flops (x3 for bf16x2), "
+                                       "m_k = N-(k+1)B, over the Schur phase's event time; traffic: "
+                                       "C read + write 8*m^2 plus panels m*K per trailing pass, "
+                                       f"K = {depth}B")}
 
 
 def run_gpu(args):
@@ -674,6 +682,8 @@ def parse(argv=None):
     ap.add_argument("--micro-seconds", type=float, default=0.0,
                     help="micro: run the launch this long before timing (sustained clocks)")
     ap.add_argument("--trsm-pair", action="store_true", help="TRSM-by-inverse products on the 2-SM kernel")
+    ap.add_argument("--merge-depth", type=int, default=None,
+                    help="panels per trailing Schur pass, 1..3 (library default 3)")
     ap.add_argument("--overlap-diag", type=int, default=None,
                     help="SMs for the diagonal factorisation run beside the trailing pass (0: off)")
     ap.add_argument("--overlap-min", type=int, default=None,

@@ -103,8 +103,8 @@ typedef enum {
     MXP_OPT_TRSM_TENSOR = 1,
     MXP_OPT_GMRES_RESTART = 2,  /* Arnoldi steps per GMRES correction, 1..30 (default 30) */
     MXP_OPT_GMRES_TOL_EXP = 3,  /* inner tolerance 10^-value on the preconditioned residual (default 10) */
-    MXP_OPT_MERGE_PANELS = 4,   /* 1 (default): update panel k+1 with step k, factor it, then apply
-                                   panels k and k+1 to the trailing matrix in one K = 2b pass */
+    MXP_OPT_MERGE_PANELS = 4,   /* 1 (default): merged look-ahead, MXP_OPT_MERGE_DEPTH panels per
+                                   trailing pass (3); 0: one panel per step, as the reference */
     MXP_OPT_SCHUR_PAIR = 5,     /* 1: tensor-core products on pairs of SMs (2-SM MMA, 256 x 256
                                    tiles); 0 (default): one SM per 128 x 256 tile */
     MXP_OPT_DIAG_COOP = 6,      /* 1 (default): diagonal-block LU (and the triangular inverses of
@@ -121,10 +121,14 @@ typedef enum {
                                    it ends); 0 (default): in sequence */
     MXP_OPT_OVERLAP_MIN = 10,   /* overlap only while the trailing matrix of the pair has at least
                                    this many blocks of rows (default 6) */
-    MXP_OPT_TRSM_SINGLE = 11    /* tensor-core TRSM by inverse: 0 (default) three split-BF16 products
+    MXP_OPT_TRSM_SINGLE = 11,   /* tensor-core TRSM by inverse: 0 (default) three split-BF16 products
                                    (hi*hi + hi*lo + lo*hi, near FP32); 1: one BF16 product, K = b
                                    (relative error ~2^-9, the reference's Alt-TRSM idea with BF16's
                                    range in place of FP16's) */
+    MXP_OPT_MERGE_DEPTH = 12    /* panels per trailing pass, 1..3 (default 3): each panel of a group
+                                   updates the column and row blocks of the group's later panels,
+                                   then one pass with K = depth * b applies the whole group
+                                   (MXP_OPT_MERGE_PANELS 0 / 1 = depth 1 / 3) */
 } mxp_option;
 mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int value);
 mxp_status mxp_workspace_destroy(mxp_workspace *ws);

@@ -161,13 +161,15 @@ OPT_TEST_WITHHOLD_FLAG = 8
 OPT_OVERLAP_DIAG = 9
 OPT_OVERLAP_MIN = 10
 OPT_TRSM_SINGLE = 11
+OPT_MERGE_DEPTH = 12
 
 
 class Workspace:
     def __init__(self, n: int, b: int, form: int | str = FORM_FP16, device: int = 0,
                  trsm_tensor: bool = True, merge_panels: bool = True, schur_pair: bool = False,
                  diag_coop: bool = True, overlap_diag: int | None = None,
-                 overlap_min: int | None = None, trsm_single: bool | None = None):
+                 overlap_min: int | None = None, trsm_single: bool | None = None,
+                 merge_depth: int | None = None):
         if isinstance(form, str):
             form = FORMS[form]
         self.n, self.b, self.form, self.device = n, b, form, device
@@ -184,6 +186,8 @@ class Workspace:
             self.set_option(OPT_OVERLAP_MIN, int(overlap_min))
         if trsm_single is not None:
             self.set_option(OPT_TRSM_SINGLE, int(trsm_single))
+        if merge_depth is not None:
+            self.set_option(OPT_MERGE_DEPTH, int(merge_depth))
 
     def set_option(self, key: int, value: int) -> None:
         check(lib().mxp_workspace_set_option(self.handle, key, value))

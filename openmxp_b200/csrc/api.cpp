@@ -76,12 +76,16 @@ mxp_status launch_sqrt(const double *in, double *out, cudaStream_t st);
 // ---------------------------------------------------------------------------
 // workspace
 // ---------------------------------------------------------------------------
+// Panel slots of the workspace buffers: at most this many panels per trailing
+// pass (K = kMaxMerge * b).
+constexpr int kMaxMerge = 3;
+
 struct mxp_workspace {
     int n = 0, b = 0, form = 0, device = 0;
-    int64_t ldk = 0;         // K-major panel row stride (elements): two panels side by side
+    int64_t ldk = 0;         // K-major panel row stride (elements): kMaxMerge panel slots side by side
     int64_t kp = 0;          // K extent of one panel (b, or 3b for BF16X2)
-    int sc_ld = 0;           // FP8 scale-table row stride (tiles): two panels side by side
-    int merge = 1;           // merged look-ahead: two panels per trailing pass
+    int sc_ld = 0;           // FP8 scale-table row stride (tiles): kMaxMerge panel slots side by side
+    int merge = kMaxMerge;   // panels per trailing pass (merged look-ahead), 1..kMaxMerge
     int pair = 0;            // trailing Schur products on the 2-SM (cta_group::2) kernel
     int trsm_pair = 0;       // TRSM-by-inverse products on the 2-SM kernel
     int withhold = -1;       // test: row block whose TRSV flag the next mxp_lu_solve withholds
@@ -139,8 +143,8 @@ static size_t ws_layout(int n, int b, int form, size_t *panel_bytes, size_t *sca
     const int64_t ldk = panel_ldk(b, form);
     const int64_t esize = form == MXP_FORM_FP8 ? 1 : 2;
     const int64_t rows = n > b ? n - b : 1;
-    *panel_bytes = (size_t)(rows * 2 * ldk * esize + 1024) / 256 * 256 + 256;
-    *scale_bytes = (size_t)(cdiv(rows, 128) * 2 * cdiv(b, 128) + 256) / 256 * 256 + 256;
+    *panel_bytes = (size_t)(rows * kMaxMerge * ldk * esize + 1024) / 256 * 256 + 256;
+    *scale_bytes = (size_t)(cdiv(rows, 128) * kMaxMerge * cdiv(b, 128) + 256) / 256 * 256 + 256;
     *vec_doubles = (size_t)n * (4 + 16) + 64;
     *flag_ints = lu_solve_flag_ints(n) + 64;
     *vec_doubles += (size_t)31 * n + 64 * 32 + 2 * 31 * 64 + 31 * (size_t)(2 * 148 + 2) + 1024;
@@ -185,8 +189,8 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
     ws->form = form;
     ws->device = device;
     ws->kp = form == MXP_FORM_BF16X2 ? 3 * (int64_t)b : b;
-    ws->ldk = 2 * panel_ldk(b, form);
-    ws->sc_ld = 2 * (int)cdiv(b, 128);
+    ws->ldk = kMaxMerge * panel_ldk(b, form);
+    ws->sc_ld = kMaxMerge * (int)cdiv(b, 128);
     ws->esize = form == MXP_FORM_FP8 ? 1 : 2;
     size_t pb, sb, vd, fi;
     ws_layout(n, b, form, &pb, &sb, &vd, &fi);
@@ -254,7 +258,11 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
             ws->trsm_tc = value ? 1 : 0;
             return MXP_OK;
         case MXP_OPT_MERGE_PANELS:
-            ws->merge = value ? 1 : 0;
+            ws->merge = value ? kMaxMerge : 1;
+            return MXP_OK;
+        case MXP_OPT_MERGE_DEPTH:
+            if (value < 1 || value > kMaxMerge) return fail(MXP_INVALID_ARG, "set_option: merge depth must be 1..3");
+            ws->merge = value;
             return MXP_OK;
         case MXP_OPT_SCHUR_PAIR:
             ws->pair = value ? 1 : 0;
@@ -447,15 +455,19 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
     uint8_t *Ls = ws->lscale[0], *Rs = ws->rscale[0];
     const int scl = ws->sc_ld;
     const bool fp8 = form == MXP_FORM_FP8;
-    // merged schedule needs FP8 scale tiles aligned to the block size
-    const bool merge = ws->merge && (!fp8 || b % 128 == 0);
+    // panels per trailing pass; merging needs FP8 scale tiles aligned to the block size
+    const int depth = (!fp8 || b % 128 == 0) ? ws->merge : 1;
+    const int64_t sct = cdiv(b, 128);  // scale tiles per panel slot (FP8)
+    // C -= L R^T over panel slots slot0 .. slot0+kfac-1 (K = kfac * b), L rows
+    // from buffer row lrow, R rows from buffer row rrow.
     auto schur = [&](int64_t mrows, int64_t ncols, int kfac, int64_t lrow, int64_t rrow, float *C,
-                     int store, const SchurSched *sched = nullptr,
-                     cudaStream_t on = nullptr) -> mxp_status {
+                     int store, const SchurSched *sched = nullptr, cudaStream_t on = nullptr,
+                     int slot0 = 0) -> mxp_status {
         ++schur_launches;
-        return launch_schur(form, (int)mrows, (int)ncols, b * kfac, Lb + lrow * ldk * es, ldk,
-                            fp8 ? Ls + (lrow / 128) * scl : nullptr, Rb + rrow * ldk * es, ldk,
-                            fp8 ? Rs + (rrow / 128) * scl : nullptr, C, lda, ws->status,
+        return launch_schur(form, (int)mrows, (int)ncols, b * kfac, Lb + (lrow * ldk + slot0 * kp) * es, ldk,
+                            fp8 ? Ls + (lrow / 128) * scl + slot0 * sct : nullptr,
+                            Rb + (rrow * ldk + slot0 * kp) * es, ldk,
+                            fp8 ? Rs + (rrow / 128) * scl + slot0 * sct : nullptr, C, lda, ws->status,
                             on ? on : st, store, scl, scl, 0, ws->pair, sched);
     };
     // LU of the diagonal block at kk and, for the tensor-core TRSM, the
@@ -473,7 +485,7 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
     };
     // Factor the diagonal block of step kk (unless diag_done: it was factored
     // on the side stream), solve its two panels, and cast them into panel slot
-    // `slot` (0 or 1) of the buffers at buffer row `row0`.
+    // `slot` (0 .. kMaxMerge-1) of the buffers at buffer row `row0`.
     auto factor_panel = [&](int64_t kk, int slot, int64_t row0, bool diag_done) -> mxp_status {
         float *Akk = d_A + kk + kk * lda;
         const int m = n - (int)kk - b;
@@ -528,48 +540,56 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
         return q;
     };
 
-    // Overlap of the next pair's diagonal factorisation with the trailing pass
+    // Overlap of the next group's diagonal factorisation with the trailing pass
     // (single-SM Schur kernel, cooperative diagonal kernel, whole tiles).
     const int ovl_sms = ws->overlap > 0 && !ws->pair && ws->coop && b % 256 == 0
                             ? std::min(ws->overlap, num_sms() / 2) : 0;
     int overlapped = 0;
     bool diag_done = false;
     int k = 0;
+    // Groups of `depth` panels (the reference's look-ahead generalised):
+    // buffer row 0 is global row (k+1)*b; panel k+j goes to slot j from buffer
+    // row j*b.  After panel k+j is factored it updates the column and row
+    // blocks of the group's later panels (K = b, its slot alone); one trailing
+    // pass with K = D*b then applies the whole group.
     while (k < nb && s == MXP_OK) {
-        const int64_t kk = (int64_t)k * b;
-        const int64_t base = kk + b;            // global row of buffer row 0
-        const int64_t m = n - base;
-        s = factor_panel(kk, 0, 0, diag_done);
-        diag_done = false;
-        if (s != MXP_OK || m <= 0) break;
-        if (!merge || m == b) {
-            // one panel per trailing pass (the reference's step structure)
+        const int D = std::min(depth, nb - k);
+        const int64_t base = (int64_t)(k + 1) * b;  // global row of buffer row 0
+        for (int j = 0; j < D && s == MXP_OK; ++j) {
+            const int64_t kk = (int64_t)(k + j) * b;
+            s = factor_panel(kk, j, (int64_t)j * b, j == 0 && diag_done);
+            if (s != MXP_OK) break;
+            const int rem = D - 1 - j;                // later panels of the group
+            const int64_t r0 = kk + b;                // first row below panel k+j
+            if (rem == 0 || r0 >= n) continue;
             pt.mark(PH_SCHUR);
-            s = schur(m, m, 1, 0, 0, d_A + base + base * lda, 0);
-            ++k;
-            continue;
+            // column blocks of the later panels: rows r0..n, columns r0..r0+rem*b
+            s = schur(n - r0, (int64_t)rem * b, 1, (int64_t)j * b, (int64_t)j * b, d_A + r0 + r0 * lda, 0,
+                      nullptr, nullptr, j);
+            // their row blocks: rows r0..r0+rem*b, columns right of the group
+            const int64_t c0 = r0 + (int64_t)rem * b;
+            if (s == MXP_OK && c0 < n)
+                s = schur((int64_t)rem * b, n - c0, 1, (int64_t)j * b, (int64_t)j * b + (int64_t)rem * b,
+                          d_A + r0 + c0 * lda, 0, nullptr, nullptr, j);
         }
-        // merged look-ahead: bring panel k+1 up to date with step k, factor it,
-        // then apply both panels to the rest of the trailing matrix in one pass.
-        pt.mark(PH_SCHUR);
-        s = schur(m, b, 1, 0, 0, d_A + base + base * lda, 0);                     // column block k+1
-        if (s == MXP_OK) s = schur(b, m - b, 1, 0, b, d_A + base + (base + b) * lda, 0);  // row block k+1
+        diag_done = false;
         if (s != MXP_OK) break;
-        s = factor_panel(base, 1, b, false);
-        if (s != MXP_OK) break;
+        const int64_t t0 = (int64_t)(k + D) * b;     // trailing matrix: rows / columns t0..n
+        const int64_t mt = n - t0;
+        k += D;
+        if (mt <= 0) break;
         pt.mark(PH_SCHUR);
-        const int64_t mt = m - b;                        // trailing size after the pair
-        float *T = d_A + (base + b) + (base + b) * lda;  // its leading element
-        if (ovl_sms == 0 || mt <= b || mt < (int64_t)ws->overlap_min * b) {
-            s = schur(mt, mt, 2, b, b, T, 0);
-            k += 2;
+        const int64_t trow = t0 - base;               // its first buffer row
+        float *T = d_A + t0 + t0 * lda;
+        if (ovl_sms == 0 || D < 2 || mt <= b || mt < (int64_t)ws->overlap_min * b) {
+            s = schur(mt, mt, D, trow, trow, T, 0);
             continue;
         }
         // The next diagonal block first (b x b corner of T), then, at the same
         // time: its factorisation on ovl_sms SMs (side stream) and the rest of
         // T on the other SMs; when the factorisation ends, a second launch on
         // those SMs claims the tiles still left from the shared counter.
-        s = schur(b, b, 2, b, b, T, 0);
+        s = schur(b, b, D, trow, trow, T, 0);
         if (s != MXP_OK) break;
         SchurSched main_part, late_part;
         main_part.grid = num_sms() - ovl_sms;
@@ -580,14 +600,13 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
         MXP_CUDA(cudaMemsetAsync(ws->tile_ctr, 0, sizeof(int), st));
         MXP_CUDA(cudaEventRecord(ws->ev_fork, st));
         MXP_CUDA(cudaStreamWaitEvent(ws->side, ws->ev_fork, 0));
-        s = factor_diag(base + b, ws->side, ovl_sms);
-        if (s == MXP_OK) s = schur(mt, mt, 2, b, b, T, 0, &main_part);
-        if (s == MXP_OK) s = schur(mt, mt, 2, b, b, T, 0, &late_part, ws->side);
+        s = factor_diag(t0, ws->side, ovl_sms);
+        if (s == MXP_OK) s = schur(mt, mt, D, trow, trow, T, 0, &main_part);
+        if (s == MXP_OK) s = schur(mt, mt, D, trow, trow, T, 0, &late_part, ws->side);
         MXP_CUDA(cudaEventRecord(ws->ev_join, ws->side));
         MXP_CUDA(cudaStreamWaitEvent(st, ws->ev_join, 0));
         diag_done = true;
         ++overlapped;
-        k += 2;
     }
     pt.mark(PH_END);
     if (s != MXP_OK) {

@@ -24,13 +24,24 @@ def _lu(mxp, n, b, seed, rule, form, **opts):
 @pytest.mark.parametrize("n,b,seed,rule,sms", [(3072, 256, 42, 0, 16), (4096, 256, 7, 1, 8),
                                                (5120, 512, 11, 0, 32), (2816, 256, 3, 0, 74)])
 def test_overlap_bit_identical(mxp, torch_cuda, form, n, b, seed, rule, sms):
-    ref, st0 = _lu(mxp, n, b, seed, rule, form)
-    got, st1 = _lu(mxp, n, b, seed, rule, form, overlap_diag=sms, overlap_min=2)
+    ref, st0 = _lu(mxp, n, b, seed, rule, form, merge_depth=2)
+    got, st1 = _lu(mxp, n, b, seed, rule, form, merge_depth=2, overlap_diag=sms, overlap_min=2)
     assert st0["overlapped_diag"] == 0
     # pairs (k, k+1) whose trailing matrix has >= 2 blocks beyond the pair
     nb = n // b
     expect = sum(1 for k in range(0, nb, 2) if nb - k - 2 >= 2)
     assert st1["overlapped_diag"] == expect
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("form", [0, 2])
+def test_overlap_depth3_bit_identical(mxp, torch_cuda, form):
+    n, b = 4096, 256
+    ref, _ = _lu(mxp, n, b, 17, 0, form, merge_depth=3)
+    got, st = _lu(mxp, n, b, 17, 0, form, merge_depth=3, overlap_diag=24, overlap_min=2)
+    # groups (0,1,2), (3,4,5), ... with >= 2 blocks of trailing matrix after them
+    nb = n // b
+    assert st["overlapped_diag"] == sum(1 for k in range(0, nb, 3) if nb - k - 3 >= 2)
     assert np.array_equal(got, ref)
 
 
