@@ -123,8 +123,10 @@ __device__ __forceinline__ void st_release(int *p, int v) {
 // (panel_trsv.hpp:308-597: FP64 solve of each upcast diagonal block, FP32 x
 // FP64 products for the rest) with the diagonal solve applied as a product
 // with its inverse.
+constexpr int kXChunk = 8;  // column blocks whose x is staged in shared memory at a time
 constexpr size_t kTrsvSmem = 2 * sizeof(double) * kRB * (kRB + 1) + sizeof(float) * kRB * (kRB + 1) +
-                             sizeof(double) * kRB + sizeof(double) * 4 * kRB + 16;
+                             sizeof(double) * kRB + sizeof(double) * 4 * kRB +
+                             sizeof(double) * 2 * kXChunk * kRB + 16;
 
 template <bool LOWER>
 __global__ void __launch_bounds__(kTrsvThreads)
@@ -136,7 +138,8 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
     float(*blk)[kRB + 1] = reinterpret_cast<float(*)[kRB + 1]>(pm + kRB);   // blk[col][row]
     double *zs = reinterpret_cast<double *>(blk + kRB);
     double(*part)[kRB] = reinterpret_cast<double(*)[kRB]>(zs + kRB);
-    int *s_ticket = reinterpret_cast<int *>(part + 4);
+    double(*xs)[kXChunk * kRB] = reinterpret_cast<double(*)[kXChunk * kRB]>(part + 4);  // 2 buffers
+    int *s_ticket = reinterpret_cast<int *>(xs + 2);
 
     const int nrb = (n + kRB - 1) / kRB;
     const int tid = threadIdx.x;
@@ -238,23 +241,12 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
         __syncwarp();
         return v != 0;
     };
-    // one column block: wait until its x is published, then accumulate
-    auto consume = [&](int q, const float *lv) {
-        const int cb = LOWER ? q : nrb - 1 - q;
-        const bool need = LOWER ? (cb > known) : (cb < known);
-        if (need) {
-            if (probe_flag(adj - (LOWER ? 1 : -1))) {
-                known = adj - (LOWER ? 1 : -1);  // blocks complete in chain order
-            } else {
-                timed_out = !wait_flag(cb);
-                known = cb;
-            }
-        }
-        const int64_t c0 = (int64_t)cb * kRB + cph * 16;
-        const int clen = (int)imin64(16, n - c0);
-        double xv[16];
-#pragma unroll
-        for (int cc = 0; cc < 16; ++cc) xv[cc] = (cc < clen) ? __ldcg(x + c0 + cc) : 0.0;
+    // The x of the streamed column blocks is staged in shared memory kXChunk
+    // blocks at a time (one coalesced load per thread and one barrier per
+    // chunk, double-buffered) instead of one L2 round trip per column block:
+    // the stream, not the chain, bounds the late blocks of a large solve.
+    auto consume = [&](int buf, int qq, const float *lv) {
+        const double *xv = xs[buf] + qq * kRB + cph * 16;
 #pragma unroll
         for (int cc = 0; cc < 16; ++cc) acc = __fma_rn((double)lv[cc], xv[cc], acc);
     };
@@ -265,18 +257,36 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
     load_l(1, b1);
     load_l(2, b2);
     load_l(3, b3);
-    for (int q = 0; q < nstream && !timed_out; q += 4) {
-        consume(q, b0);
-        load_l(q + 4, b0);
-        if (q + 1 >= nstream || timed_out) break;
-        consume(q + 1, b1);
-        load_l(q + 5, b1);
-        if (q + 2 >= nstream || timed_out) break;
-        consume(q + 2, b2);
-        load_l(q + 6, b2);
-        if (q + 3 >= nstream || timed_out) break;
-        consume(q + 3, b3);
-        load_l(q + 7, b3);
+    int buf = 0;
+    for (int q0 = 0; q0 < nstream; q0 += kXChunk, buf ^= 1) {
+        const int qn = min(kXChunk, nstream - q0);
+        const int cb_last = LOWER ? q0 + qn - 1 : nrb - 1 - (q0 + qn - 1);
+        // blocks complete in chain order: once the chunk's last block (or the
+        // block before the predecessor) is published, so is the whole chunk
+        if (!timed_out && (LOWER ? (cb_last > known) : (cb_last < known))) {
+            if (probe_flag(adj - (LOWER ? 1 : -1))) {
+                known = adj - (LOWER ? 1 : -1);
+            } else {
+                timed_out = !wait_flag(cb_last);
+                known = cb_last;
+            }
+        }
+        for (int e = tid; e < qn * kRB; e += kTrsvThreads) {
+            const int qq = e / kRB, cc = e % kRB;
+            const int cb = LOWER ? q0 + qq : nrb - 1 - (q0 + qq);
+            const int64_t col = (int64_t)cb * kRB + cc;
+            xs[buf][e] = (col < n) ? __ldcg(x + col) : 0.0;
+        }
+        // a wait that gave up anywhere in the CTA ends the stream everywhere
+        timed_out = __syncthreads_or(timed_out) != 0;
+        if (timed_out) break;
+#pragma unroll
+        for (int qq = 0; qq < kXChunk; qq += 4) {
+            if (qq + 0 < qn) { consume(buf, qq + 0, b0); load_l(q0 + qq + 4, b0); }
+            if (qq + 1 < qn) { consume(buf, qq + 1, b1); load_l(q0 + qq + 5, b1); }
+            if (qq + 2 < qn) { consume(buf, qq + 2, b2); load_l(q0 + qq + 6, b2); }
+            if (qq + 3 < qn) { consume(buf, qq + 3, b3); load_l(q0 + qq + 7, b3); }
+        }
     }
     part[cph][r] = acc;
     __syncthreads();
