@@ -387,13 +387,17 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
 // Same pipeline with 128-byte K stages (128 FP8 values).  Each 128 x 128 tile
 // of a panel carries one UE8M0 scale (2^-e, e from the tile amax); a stage of
 // K = 128 covers exactly one scale tile, so the stage's scale factors are
-// uniform per 128 rows.  Warp 0 writes them to shared memory in the MX
-// scale-factor atom layout (32 rows x 16 bytes, row r / k-block kb at byte
-// (r%32)*16 + (r/32)*4 + kb) next to the TMA tiles; the MMA lane moves them to
-// TMEM with tcgen05.cp (32x128b, replicated to the four lane quarters) and
-// issues tcgen05.mma ... kind::mxf8f6f4.block_scale, which applies the scales
-// inside the MMA.  TMEM: one 256-column accumulator (cols 0..255) plus a
-// 4-slot scale-factor ring (cols 256..319).  The epilogue copies the whole
+// uniform per 128 rows.  Once per four stages warp 0 writes them to shared
+// memory in the MX scale-factor atom layout (32 rows x 16 bytes; row r's
+// 32-bit word for its lane quarter at byte (r%32)*16 + (r/32)*4), byte g of
+// the word holding the scale of the group's stage g, next to the TMA tiles;
+// the MMA lane moves them to TMEM with tcgen05.cp (32x128b, replicated to the
+// four lane quarters) and issues tcgen05.mma ... kind::mxf8f6f4.block_scale
+// with sf_id = the stage's byte, which applies the scales inside the MMA.
+// Copying per group rather than per stage issues a quarter of the copies
+// (measured neutral in throughput: the kernel is power-bound).  TMEM: one
+// 256-column accumulator (cols 0..255) plus
+// two scale-factor slots (cols 256..287).  The epilogue copies the whole
 // accumulator to registers first and releases TMEM, so its C update overlaps
 // the next tile's main loop.
 constexpr int kF8BN = 256;
@@ -404,6 +408,11 @@ constexpr int kF8StageBytes = kF8StageA + kF8StageB + kF8StageSF;
 constexpr int kF8Stages = 4;
 constexpr int kF8SmemBytes = 1024 + kF8Stages * kF8StageBytes + 512;
 constexpr int kF8SfCol0 = 256;
+// Stages whose scale factors share one TMEM copy: a tile's scale is uniform
+// over its 128 x 128 block, so the four K blocks of a stage use one byte of
+// the 32-bit scale word and one word carries four stages (byte = stage % 4,
+// selected by sf_id).  Two TMEM slots (16 columns each) alternate by group.
+constexpr int kF8SfGroup = 4;
 
 __device__ __forceinline__ void tc_cp_32x128b_x4(uint32_t taddr, uint64_t sdesc) {
     asm volatile("tcgen05.cp.cta_group::1.32x128b.warpx4 [%0], %1;" ::"r"(taddr), "l"(sdesc)
@@ -534,25 +543,37 @@ schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                     ok = false;
                     break;
                 }
-                const bool hi = (kb & 32) != 0;
-                const int src_lane = kb & 31;
-                const uint32_t sa = __shfl_sync(0xffffffffu, hi ? ra[1] : ra[0], src_lane);
-                const uint32_t sb0 = __shfl_sync(0xffffffffu, hi ? rb0[1] : rb0[0], src_lane);
-                const uint32_t sb1 = __shfl_sync(0xffffffffu, hi ? rb1[1] : rb1[0], src_lane);
-                // operand tiles first (the barrier expects their bytes), then the
-                // stage's scale factors; the single arrival comes after both
+                // operand tiles first (the barrier expects their bytes), then, at
+                // the first stage of a group, the group's scale factors; the
+                // single arrival comes after both
                 const uint32_t fb = smem_u32(&full[stage]);
                 if (lane == 0) {
                     mbar_expect_tx_only(fb, kF8StageA + kF8StageB);
                     tma_load_2d(smem_u32(stA(stage)), &tmA, kb * 128, tm * kBM, fb);
                     tma_load_2d(smem_u32(stB(stage)), &tmB, kb * 128, tn * kF8BN, fb);
                 }
-                const uint32_t wa = sa * 0x01010101u, wb0 = sb0 * 0x01010101u, wb1 = sb1 * 0x01010101u;
-                uint4 *sf = reinterpret_cast<uint4 *>(stSF(stage));
-                sf[lane] = make_uint4(wa, wa, wa, wa);             // SFA: rows 0..127
-                sf[32 + lane] = make_uint4(wb0, wb0, wb0, wb0);    // SFB atom 0: rows 0..127
-                sf[64 + lane] = make_uint4(wb1, wb1, wb1, wb1);    // SFB atom 1: rows 128..255
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                if ((kb & (kF8SfGroup - 1)) == 0) {
+                    // byte g of each scale word = the scale of stage kb + g (2^0 past K)
+                    uint32_t wa = 0u, wb0 = 0u, wb1 = 0u;
+#pragma unroll
+                    for (int g = 0; g < kF8SfGroup; ++g) {
+                        const int kx = kb + g;
+                        const bool hi = (kx & 32) != 0;
+                        const int src_lane = kx & 31;
+                        uint32_t va = __shfl_sync(0xffffffffu, hi ? ra[1] : ra[0], src_lane);
+                        uint32_t v0 = __shfl_sync(0xffffffffu, hi ? rb0[1] : rb0[0], src_lane);
+                        uint32_t v1 = __shfl_sync(0xffffffffu, hi ? rb1[1] : rb1[0], src_lane);
+                        if (kx >= nk) va = v0 = v1 = 127u;
+                        wa |= va << (8 * g);
+                        wb0 |= v0 << (8 * g);
+                        wb1 |= v1 << (8 * g);
+                    }
+                    uint4 *sf = reinterpret_cast<uint4 *>(stSF(stage));
+                    sf[lane] = make_uint4(wa, wa, wa, wa);             // SFA: rows 0..127
+                    sf[32 + lane] = make_uint4(wb0, wb0, wb0, wb0);    // SFB atom 0: rows 0..127
+                    sf[64 + lane] = make_uint4(wb1, wb1, wb1, wb1);    // SFB atom 1: rows 128..255
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(fb);
                 if (++stage == kF8Stages) {
@@ -571,6 +592,7 @@ schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             int stage = 0;
             uint32_t phase = 0;
             uint32_t it = 0;
+            uint32_t groups = 0;  // scale-factor groups copied so far (their TMEM slot alternates)
             int rslot = 0;
             uint32_t rphase = 0;
             bool ok = true;
@@ -592,18 +614,23 @@ schur_tc_fp8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t sfa_t = tmem_base + kF8SfCol0 + 16u * stage;
+                    const uint32_t gpos = (uint32_t)(kb & (kF8SfGroup - 1));
+                    if (gpos == 0) ++groups;
+                    const uint32_t sfa_t = tmem_base + kF8SfCol0 + 16u * (groups & 1u);
                     const uint32_t sfb_t = sfa_t + 4u;
-                    const uint32_t sf0 = smem_u32(stSF(stage));
-                    tc_cp_32x128b_x4(sfa_t, smem_desc_sf(sf0));
-                    tc_cp_32x128b_x4(sfb_t, smem_desc_sf(sf0 + 512));
-                    tc_cp_32x128b_x4(sfb_t + 4u, smem_desc_sf(sf0 + 1024));
+                    if (gpos == 0) {  // the group's scales, written with its first stage
+                        const uint32_t sf0 = smem_u32(stSF(stage));
+                        tc_cp_32x128b_x4(sfa_t, smem_desc_sf(sf0));
+                        tc_cp_32x128b_x4(sfb_t, smem_desc_sf(sf0 + 512));
+                        tc_cp_32x128b_x4(sfb_t + 4u, smem_desc_sf(sf0 + 1024));
+                    }
                     const uint32_t a0 = smem_u32(stA(stage));
                     const uint32_t b0 = smem_u32(stB(stage));
+                    // the stage's four K blocks share its tile scale: byte gpos
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         tc_mma_mxf8(tmem_base, smem_desc_sw128(a0 + 32 * k), smem_desc_sw128(b0 + 32 * k),
-                                    idesc_mxf8((uint32_t)k), sfa_t, sfb_t, (kb > 0 || k > 0) ? 1u : 0u);
+                                    idesc_mxf8(gpos), sfa_t, sfb_t, (kb > 0 || k > 0) ? 1u : 0u);
                     }
                     tc_commit(smem_u32(&empty[stage]));
                     if (++stage == kF8Stages) {

@@ -84,15 +84,17 @@ def _tiles(rng, rows, cols, scales):
     return a
 
 
+@pytest.mark.parametrize("K", [384, 640, 1152])
 @pytest.mark.parametrize("pair", [True, False])
-def test_schur_fp8_exact_tile_scales(mxp, orc, torch_cuda, pair):
+def test_schur_fp8_exact_tile_scales(mxp, orc, torch_cuda, pair, K):
     """FP8 with different power-of-two scales per 128x128 tile: every value is
     exact in E4M3 after scaling, every product and sum exact in FP32, so the
     block-scaled MMA must reproduce C - L U^T bit for bit.  Pins the scale-
-    factor layout (rows, k-blocks, both operands)."""
+    factor layout (rows, k-blocks, both operands, stage groups: 3, 5 and 9
+    K stages)."""
     torch = torch_cuda
     rng = np.random.default_rng(3)
-    m, n, K = 384, 512, 384
+    m, n = 384, 512
     L = _tiles(rng, m, K, [1.0, 0.125, 0.25, 2.0])
     Ut = _tiles(rng, n, K, [0.5, 1.0, 4.0])      # R = U^T, rows n
     U = np.asfortranarray(Ut.T)
@@ -102,8 +104,9 @@ def test_schur_fp8_exact_tile_scales(mxp, orc, torch_cuda, pair):
     dC = from_np_colmajor(torch, Cm)
     Lp = torch.zeros(m * K, dtype=torch.uint8, device="cuda")
     Rp = torch.zeros(n * K, dtype=torch.uint8, device="cuda")
-    ls = torch.zeros(3 * 3 + 16, dtype=torch.uint8, device="cuda")
-    rs = torch.zeros(4 * 3 + 16, dtype=torch.uint8, device="cuda")
+    kt = -(-K // 128)
+    ls = torch.zeros(3 * kt + 16, dtype=torch.uint8, device="cuda")
+    rs = torch.zeros(4 * kt + 16, dtype=torch.uint8, device="cuda")
     ws = mxp.Workspace(1024, 128, 2, schur_pair=pair)
     mxp.panel_cast_left(2, m, K, dL, m, Lp, K, ls)
     mxp.panel_cast_right(2, n, K, dU, K, Rp, K, rs)
