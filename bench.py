@@ -252,6 +252,8 @@ def _solve_arm(args, form_name, p, dev, dist, local, e2e_on, trsm=None):
         ws.set_option(mxp.OPT_TRSM_PAIR, 1)
     if args.merge_depth is not None:
         ws.set_option(mxp.OPT_MERGE_DEPTH, args.merge_depth)
+    if args.inv_tc is not None:
+        ws.set_option(mxp.OPT_INV_TC, args.inv_tc)
     if args.overlap_diag is not None:
         ws.set_option(mxp.OPT_OVERLAP_DIAG, args.overlap_diag)
     if args.overlap_min is not None:
@@ -497,6 +499,8 @@ def run_micro(args):
         res = {}
         for coop in (True, False):
             ws = mxp.Workspace(n, n, 0, diag_coop=coop)
+            if args.inv_tc is not None:
+                ws.set_option(mxp.OPT_INV_TC, args.inv_tc)
             for inv in (False, True):
                 tot = 0.0
                 for it in range(args.warmup + args.steps):
@@ -684,6 +688,9 @@ def parse(argv=None):
     ap.add_argument("--trsm-pair", action="store_true", help="TRSM-by-inverse products on the 2-SM kernel")
     ap.add_argument("--merge-depth", type=int, default=None,
                     help="panels per trailing Schur pass, 1..3 (library default 3)")
+    ap.add_argument("--inv-tc", type=int, default=None,
+                    help="triangular-inverse doubling levels from this block size on the tensor cores "
+                         "(library default 1024; 0: all SIMT FP32)")
     ap.add_argument("--overlap-diag", type=int, default=None,
                     help="SMs for the diagonal factorisation run beside the trailing pass (0: off)")
     ap.add_argument("--overlap-min", type=int, default=None,

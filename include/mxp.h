@@ -125,10 +125,14 @@ typedef enum {
                                    (hi*hi + hi*lo + lo*hi, near FP32); 1: one BF16 product, K = b
                                    (relative error ~2^-9, the reference's Alt-TRSM idea with BF16's
                                    range in place of FP16's) */
-    MXP_OPT_MERGE_DEPTH = 12    /* panels per trailing pass, 1..3 (default 3): each panel of a group
+    MXP_OPT_MERGE_DEPTH = 12,   /* panels per trailing pass, 1..3 (default 3): each panel of a group
                                    updates the column and row blocks of the group's later panels,
                                    then one pass with K = depth * b applies the whole group
                                    (MXP_OPT_MERGE_PANELS 0 / 1 = depth 1 / 3) */
+    MXP_OPT_INV_TC = 13         /* triangular inverses of the diagonal block: doubling levels that
+                                   join blocks of this size and larger run as tensor-core products
+                                   in the TRSM's precision (default 1024; 0: all in the cooperative
+                                   kernel, SIMT FP32) */
 } mxp_option;
 mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int value);
 mxp_status mxp_workspace_destroy(mxp_workspace *ws);

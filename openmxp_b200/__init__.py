@@ -162,6 +162,7 @@ OPT_OVERLAP_DIAG = 9
 OPT_OVERLAP_MIN = 10
 OPT_TRSM_SINGLE = 11
 OPT_MERGE_DEPTH = 12
+OPT_INV_TC = 13
 
 
 class Workspace:

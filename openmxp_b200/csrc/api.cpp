@@ -109,6 +109,7 @@ struct mxp_workspace {
     // tensor-core panel TRSM: FP32 triangular inverses and split-BF16 operands
     int trsm_tc = 1;
     int trsm_single = 0;     // one BF16 product instead of three split products
+    int inv_tc = 1024;       // inverse doubling levels from this block size on the tensor cores (0: none)
     int64_t ldk3 = 0;
     float *tinv_u = nullptr, *tinv_l = nullptr, *tinv_tmp = nullptr;
     // cooperative diagonal-block factorisation (LU + inverses in one launch)
@@ -284,6 +285,11 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
         case MXP_OPT_TRSM_SINGLE:
             ws->trsm_single = value ? 1 : 0;
             return MXP_OK;
+        case MXP_OPT_INV_TC:
+            if (value != 0 && (value < 128 || (value & (value - 1)) != 0))
+                return fail(MXP_INVALID_ARG, "set_option: inverse level must be 0 or a power of two >= 128");
+            ws->inv_tc = value;
+            return MXP_OK;
         case MXP_OPT_OVERLAP_MIN:
             if (value < 2) return fail(MXP_INVALID_ARG, "set_option: overlap minimum must be >= 2 blocks");
             ws->overlap_min = value;
@@ -334,6 +340,53 @@ extern "C" mxp_status mxp_matgen_f64(int n, uint64_t seed, int diag_rule, double
     return launch_matgen_f64(n, seed, diag_rule, d_A, lda, as_stream(stream));
 }
 
+// The doubling levels of the triangular inverses from blocks of size s_start
+// up, as tensor-core products (the cooperative kernel stops before them): for
+// adjacent diagonal blocks of sizes S and s2, the off-diagonal block of
+// inv(U) is -inv(U11) (U12 inv(U22)) and that of inv(L) is
+// -inv(L22) (L21 inv(L11)), the same recursion as the kernel's SIMT levels.
+// form: MXP_FORM_BF16X2 (three split products, near FP32) or kFormBf16 (one
+// product).  T: S * s2 floats of scratch; the operands go through the
+// workspace's split buffers.
+static mxp_status finish_inverses_tc(int n, const float *A, int64_t lda, float *XU, float *XL, int64_t ldx,
+                                     int s_start, int form, float *T, mxp_workspace *ws, cudaStream_t st) {
+    // C (m x nn) = P (m x K) Q (K x nn), or its negative; column-major FP32
+    auto gemm = [&](int m, int nn, int K, const float *P, int64_t ldp, const float *Q, int64_t ldq, float *C,
+                    int64_t ldc, bool neg) -> mxp_status {
+        mxp_status q = launch_cast_left(form, m, K, P, ldp, ws->split_l, ws->ldk3, nullptr, st);
+        if (q == MXP_OK) q = launch_cast_right(form, nn, K, Q, ldq, ws->split_u, ws->ldk3, nullptr, st);
+        if (q == MXP_OK)
+            q = launch_schur(form, m, nn, K, ws->split_l, ws->ldk3, nullptr, ws->split_u, ws->ldk3, nullptr, C, ldc,
+                             ws->status, st, neg ? 2 : 1, 0, 0, 0, 0);
+        return q;
+    };
+    mxp_status q = MXP_OK;
+    for (int S = s_start; S < n && q == MXP_OK; S *= 2) {
+        const int np = n / (2 * S);
+        const int c = n - np * 2 * S - S;  // second block of a ragged last pair
+        for (int p = 0; p <= np && q == MXP_OK; ++p) {
+            const int s2 = p < np ? S : c;
+            if (s2 <= 0) break;
+            const int64_t r0 = (int64_t)p * 2 * S, r1 = r0 + S;
+            // U: T = U12 inv(U22) (S x s2), then X12 = -inv(U11) T
+            q = gemm(S, s2, s2, A + r0 + r1 * lda, lda, XU + r1 + r1 * ldx, ldx, T, S, false);
+            if (q == MXP_OK) q = gemm(S, s2, S, XU + r0 + r0 * ldx, ldx, T, S, XU + r0 + r1 * ldx, ldx, true);
+            // L: T = L21 inv(L11) (s2 x S), then X21 = -inv(L22) T
+            if (q == MXP_OK) q = gemm(s2, S, S, A + r1 + r0 * lda, lda, XL + r0 + r0 * ldx, ldx, T, s2, false);
+            if (q == MXP_OK)
+                q = gemm(s2, S, s2, XL + r1 + r1 * ldx, ldx, T, s2, XL + r1 + r0 * ldx, ldx, true);
+        }
+    }
+    return q;
+}
+
+// Tensor-core inverse levels apply from this block size (0: none), when the
+// block is large enough for them to matter and the split buffers hold it.
+static int inv_tc_start(const mxp_workspace *ws, int n) {
+    if (ws->inv_tc <= 0 || n > ws->b || 2 * ws->inv_tc > n) return 0;
+    return ws->inv_tc;
+}
+
 extern "C" mxp_status mxp_getrf_nopiv(int n, float *d_A, int64_t lda, mxp_workspace *ws,
                                       void *stream) {
     if (!ws) return fail(MXP_INVALID_ARG, "getrf: workspace is NULL");
@@ -353,8 +406,13 @@ extern "C" mxp_status mxp_getrf_nopiv_inv(int n, float *d_A, int64_t lda, float 
     cudaStream_t st = as_stream(stream);
     mxp_status s;
     if (ws->coop) {
+        const int tc = inv_tc_start(ws, n);
         s = launch_diag_factor(n, d_A, lda, d_XU, d_XL, ldx, ws->coop_tmp,
-                               ws->coop_tmp + diag_factor_tmp_floats(ws->b), ws->coop_sync, ws->status, 0, st);
+                               ws->coop_tmp + diag_factor_tmp_floats(ws->b), ws->coop_sync, ws->status, 0, st, 0,
+                               tc);
+        if (s == MXP_OK && tc > 0)
+            s = finish_inverses_tc(n, d_A, lda, d_XU, d_XL, ldx, tc,
+                                   ws->trsm_single ? kFormBf16 : MXP_FORM_BF16X2, ws->coop_tmp, ws, st);
     } else {
         s = launch_getrf_blocked(n, d_A, lda, ws->status, 0, st);
         if (s == MXP_OK) s = launch_tri_inv_upper(n, d_A, lda, d_XU, ldx, ws->tinv_tmp, st);
@@ -478,10 +536,17 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
         const int m = n - (int)kk - b;
         const bool coop_inv = ws->coop && ws->trsm_tc && m > 0;
         float *tmpU = ws->coop_tmp, *tmpL = ws->coop_tmp + diag_factor_tmp_floats(b);
-        return ws->coop ? launch_diag_factor(b, Akk, lda, coop_inv ? ws->tinv_u : nullptr,
-                                             coop_inv ? ws->tinv_l : nullptr, b, tmpU, tmpL,
-                                             ws->coop_sync, ws->status, (int)kk, on, max_grid)
-                        : launch_getrf_blocked(b, Akk, lda, ws->status, (int)kk, on);
+        if (!ws->coop) return launch_getrf_blocked(b, Akk, lda, ws->status, (int)kk, on);
+        // the large doubling levels of the inverses on the tensor cores (same
+        // stream; not beside a trailing pass, whose SMs they would share)
+        const int tc = coop_inv && max_grid == 0 ? inv_tc_start(ws, b) : 0;
+        mxp_status q = launch_diag_factor(b, Akk, lda, coop_inv ? ws->tinv_u : nullptr,
+                                          coop_inv ? ws->tinv_l : nullptr, b, tmpU, tmpL, ws->coop_sync,
+                                          ws->status, (int)kk, on, max_grid, tc);
+        if (q == MXP_OK && tc > 0)
+            q = finish_inverses_tc(b, Akk, lda, ws->tinv_u, ws->tinv_l, b, tc,
+                                   ws->trsm_single ? kFormBf16 : MXP_FORM_BF16X2, tmpU, ws, on);
+        return q;
     };
     // Factor the diagonal block of step kk (unless diag_done: it was factored
     // on the side stream), solve its two panels, and cast them into panel slot

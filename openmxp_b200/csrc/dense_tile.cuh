@@ -408,10 +408,11 @@ __device__ void run_jobs(Smem &sm, const Job *jobs, int njobs, int cta, int ncta
 // every triangular operand skipped along K.  Work items are spread over
 // (cta, ncta); sync(where) separates the phases (a grid barrier across CTAs or
 // __syncthreads in a single CTA) and returns false to stop.  tmpU / tmpL hold
-// n*n/2 + 64 n floats each.
+// n*n/2 + 64 n floats each.  s_stop > 0: stop before the level that joins
+// blocks of size s_stop (the caller finishes those levels elsewhere).
 template <typename Sync>
 __device__ bool tri_inverses(Smem &sm, int n, const float *A, int64_t lda, float *XU, float *XL, int64_t ldx,
-                             float *tmpU, float *tmpL, int cta, int G, Sync sync) {
+                             float *tmpU, float *tmpL, int cta, int G, Sync sync, int s_stop = 0) {
     const int nsteps = (n + kNB - 1) / kNB;
     // invert the diagonal 64 x 64 blocks and zero the opposite block-triangle
     const int nblk = nsteps;
@@ -426,7 +427,7 @@ __device__ bool tri_inverses(Smem &sm, int n, const float *A, int64_t lda, float
 
     const float *U = A, *L = A;
     const int64_t ldu = lda, ldl = lda;
-    for (int S = kNB; S < n; S *= 2) {
+    for (int S = kNB; S < n && (s_stop <= 0 || S < s_stop); S *= 2) {
         const int np = n / (2 * S);
         const int rem = n - np * 2 * S;
         const int c = rem - S;  // ragged last pair (when > 0)

@@ -90,7 +90,7 @@ __device__ bool grid_sync(const Ctl &c, unsigned int &epoch, int where) {
 
 __global__ void __launch_bounds__(kCT, 1)
 diag_factor_kernel(int n, float *A, int64_t lda, float *XU, float *XL, int64_t ldx, float *tmpU,
-                   float *tmpL, Ctl ctl, int pivot_base) {
+                   float *tmpL, Ctl ctl, int pivot_base, int inv_stop) {
     extern __shared__ __align__(16) unsigned char coop_smem[];
     Smem &sm = *reinterpret_cast<Smem *>(coop_smem);
     const int G = gridDim.x, cta = blockIdx.x;
@@ -141,7 +141,7 @@ diag_factor_kernel(int n, float *A, int64_t lda, float *XU, float *XL, int64_t l
 
     // ---------------- triangular inverses ----------------
     auto gsync = [&](int where) { return grid_sync(ctl, epoch, where); };
-    tri_inverses(sm, n, A, lda, XU, XL, ldx, tmpU, tmpL, cta, G, gsync);
+    tri_inverses(sm, n, A, lda, XU, XL, ldx, tmpU, tmpL, cta, G, gsync, inv_stop);
 }
 
 int coop_grid(int device) {
@@ -163,7 +163,7 @@ size_t diag_factor_tmp_floats(int n) { return (size_t)n * n / 2 + (size_t)64 * n
 
 mxp_status launch_diag_factor(int n, float *A, int64_t lda, float *XU, float *XL, int64_t ldx,
                               float *tmpU, float *tmpL, unsigned int *sync_words, DevStatus *dst,
-                              int pivot_base, cudaStream_t st, int max_grid) {
+                              int pivot_base, cudaStream_t st, int max_grid, int inv_stop) {
     if (n <= 0) return MXP_OK;
     if (lda < n || (XU && ldx < n)) return fail(MXP_INVALID_ARG, "diag_factor: bad leading dimension");
     if ((XU == nullptr) != (XL == nullptr)) return fail(MXP_INVALID_ARG, "diag_factor: both inverses or none");
@@ -177,7 +177,7 @@ mxp_status launch_diag_factor(int n, float *A, int64_t lda, float *XU, float *XL
     if (max_grid > 0) grid = min(grid, max(2, max_grid));
     MXP_CUDA(cudaMemsetAsync(sync_words, 0, 2 * sizeof(unsigned int), st));
     Ctl ctl{sync_words, reinterpret_cast<int *>(sync_words + 1), dst};
-    void *args[] = {&n, &A, &lda, &XU, &XL, &ldx, &tmpU, &tmpL, &ctl, &pivot_base};
+    void *args[] = {&n, &A, &lda, &XU, &XL, &ldx, &tmpU, &tmpL, &ctl, &pivot_base, &inv_stop};
     MXP_CUDA(cudaLaunchCooperativeKernel((const void *)diag_factor_kernel, dim3(grid), dim3(kCT), args,
                                          sizeof(Smem), st));
     MXP_LAUNCHED();

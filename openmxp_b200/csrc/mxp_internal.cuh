@@ -130,10 +130,12 @@ constexpr int kFormBf16 = 3;
 // words of device memory (zeroed on the stream before the launch).
 size_t diag_factor_tmp_floats(int n);
 // max_grid > 0 caps the number of CTAs (the kernel then shares the GPU with
-// work launched on another stream).
+// work launched on another stream).  inv_stop > 0: the inverses stop before
+// the doubling level that joins blocks of that size (finish_inverses_tc
+// completes them).
 mxp_status launch_diag_factor(int n, float *A, int64_t lda, float *XU, float *XL, int64_t ldx,
                               float *tmpU, float *tmpL, unsigned int *sync_words, DevStatus *dst,
-                              int pivot_base, cudaStream_t st, int max_grid = 0);
+                              int pivot_base, cudaStream_t st, int max_grid = 0, int inv_stop = 0);
 mxp_status launch_matgen_f64(int n, uint64_t seed, int diag_rule, double *A, int64_t lda,
                              cudaStream_t st);
 mxp_status launch_matgen(int n, uint64_t seed, int diag_rule, float *A, int64_t lda, double *d,

@@ -337,10 +337,11 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                     float *cp = C + col0 * ldc + row;
                     float cv[32];
                     const int ncol = (int)imin64(32, (int64_t)N - col0);
-                    if (store) {  // C = acc (panel solves)
+                    if (store) {  // C = acc (panel solves), or C = -acc (store == 2)
+                        const float sg = store == 2 ? -1.0f : 1.0f;
 #pragma unroll
                         for (int j = 0; j < 32; ++j)
-                            if (j < ncol) __stcs(cp + j * ldc, __uint_as_float(r[j]));
+                            if (j < ncol) __stcs(cp + j * ldc, sg * __uint_as_float(r[j]));
                     } else if (ncol >= 32) {
 #pragma unroll
                         for (int j = 0; j < 32; ++j) cv[j] = __ldcs(cp + j * ldc);

@@ -33,6 +33,7 @@ def test_getrf_nopiv_inv(mxp, orc, torch_cuda, n, coop):
     XU = torch.full((n * n,), float("nan"), dtype=torch.float32, device="cuda")
     XL = torch.full((n * n,), float("nan"), dtype=torch.float32, device="cuda")
     ws = mxp.Workspace(max(n, 128), n, 0, diag_coop=coop)
+    ws.set_option(mxp.OPT_INV_TC, 0)  # every level in FP32 (the tensor-core levels: below)
     mxp.getrf_nopiv_inv(dA, n, n, XU, XL, n, ws)
     LU = to_np_colmajor(dA, n, n, n).astype(np.float64)
     U = np.triu(LU)
@@ -92,3 +93,41 @@ def test_trsm_left_lower_unit(mxp, orc, torch_cuda, m, n):
     ref = np.asfortranarray(B.copy())
     orc.lib().orc_trsm_llnu(m, n, Lm.ctypes.data, m, ref.ctypes.data, m)
     assert rel_fro(got, ref) < 1e-6
+
+
+@pytest.mark.parametrize("n,start,single", [(512, 128, False), (1000, 128, False), (2560, 1024, False),
+                                            (2560, 512, False), (1536, 256, True)])
+def test_getrf_nopiv_inv_tensor_levels(mxp, orc, torch_cuda, n, start, single):
+    """The large doubling levels of the inverses as tensor-core products
+    (MXP_OPT_INV_TC): split-BF16 products keep X U = I to ~1e-5 (about 16
+    mantissa bits per operand); one BF16 product to ~1e-2.  The LU itself is
+    unchanged and the zero triangles stay exactly zero."""
+    torch = torch_cuda
+    A, _, _, _ = orc.matgen(n, 3)
+    dA = from_np_colmajor(torch, A)
+    XU = torch.full((n * n,), float("nan"), dtype=torch.float32, device="cuda")
+    XL = torch.full((n * n,), float("nan"), dtype=torch.float32, device="cuda")
+    ws = mxp.Workspace(n, n, 0, trsm_single=single)
+    ws.set_option(mxp.OPT_INV_TC, start)
+    mxp.getrf_nopiv_inv(dA, n, n, XU, XL, n, ws)
+    LU = to_np_colmajor(dA, n, n, n).astype(np.float64)
+    U = np.triu(LU)
+    L = np.tril(LU, -1) + np.eye(n)
+    xu = to_np_colmajor(XU, n, n, n).astype(np.float64)
+    xl = to_np_colmajor(XL, n, n, n).astype(np.float64)
+    assert np.array_equal(np.tril(xu, -1), np.zeros((n, n)))
+    assert np.array_equal(np.triu(xl, 1), np.zeros((n, n)))
+    tol = 1e-2 if single else 1e-4
+    assert np.abs(xu @ U - np.eye(n)).max() < tol
+    assert np.abs(xl @ L - np.eye(n)).max() < tol
+    ref = A.copy(order="F")
+    assert orc.lib().orc_getrf_nopiv(n, n, ref.ctypes.data, n) == 0
+    assert rel_fro(LU, ref) < 1e-6
+
+
+def test_inv_tc_option_bounds(mxp, torch_cuda):
+    ws = mxp.Workspace(512, 128, 0)
+    for bad in (-1, 64, 300):
+        with pytest.raises(mxp.MxpError):
+            ws.set_option(mxp.OPT_INV_TC, bad)
+    ws.set_option(mxp.OPT_INV_TC, 0)
