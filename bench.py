@@ -258,6 +258,8 @@ def _solve_arm(args, form_name, p, dev, dist, local, e2e_on, trsm=None):
         ws.set_option(mxp.OPT_OVERLAP_DIAG, args.overlap_diag)
     if args.overlap_min is not None:
         ws.set_option(mxp.OPT_OVERLAP_MIN, args.overlap_min)
+    if args.trsv_inv is not None:
+        ws.set_option(mxp.OPT_TRSV_INV, args.trsv_inv)
     method = mxp.IR_GMRES if args.ir == "gmres" else mxp.IR_CLASSIC
     x = torch.empty(n, dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream()
@@ -691,6 +693,9 @@ def parse(argv=None):
     ap.add_argument("--inv-tc", type=int, default=None,
                     help="triangular-inverse doubling levels from this block size on the tensor cores "
                          "(library default 1024; 0: all SIMT FP32)")
+    ap.add_argument("--trsv-inv", type=int, default=None,
+                    help="1 (library default): refinement solves with the stored inverses of the "
+                         "diagonal blocks; 0: the chain of 64-row blocks")
     ap.add_argument("--overlap-diag", type=int, default=None,
                     help="SMs for the diagonal factorisation run beside the trailing pass (0: off)")
     ap.add_argument("--overlap-min", type=int, default=None,

@@ -129,10 +129,18 @@ typedef enum {
                                    updates the column and row blocks of the group's later panels,
                                    then one pass with K = depth * b applies the whole group
                                    (MXP_OPT_MERGE_PANELS 0 / 1 = depth 1 / 3) */
-    MXP_OPT_INV_TC = 13         /* triangular inverses of the diagonal block: doubling levels that
+    MXP_OPT_INV_TC = 13,        /* triangular inverses of the diagonal block: doubling levels that
                                    join blocks of this size and larger run as tensor-core products
                                    in the TRSM's precision (default 1024; 0: all in the cooperative
                                    kernel, SIMT FP32) */
+    MXP_OPT_TRSV_INV = 14       /* 1 (default): mxp_panel_lu keeps the FP32 inverses of every
+                                   diagonal block (2 * n * b floats of the workspace) and the
+                                   refinement's triangular solves of that factor run as nb steps
+                                   of bandwidth-bound products with them (each diagonal block:
+                                   product with its inverse, then one refinement step against
+                                   the factor block, in FP64); 0: the chain of 64-row blocks,
+                                   each inverting its diagonal block in FP64.  Setting the
+                                   option forgets the stored inverses. */
 } mxp_option;
 mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int value);
 mxp_status mxp_workspace_destroy(mxp_workspace *ws);
@@ -247,9 +255,16 @@ mxp_status mxp_otf_gemv_noalloc(int n, uint64_t seed, const double *d_d, double 
                                 const double *d_x, double beta, double *d_y, void *stream);
 
 /* trsvL_h + trsvU_h (panel_trsv.hpp:308-597): x <- U^{-1} L^{-1} x with
- * the FP32 factors of mxp_panel_lu, vectors in FP64, exact block
- * substitution.  Blocking: reads the workspace status word (MXP_TIMEOUT when a
- * bounded wait between row blocks gave up). */
+ * the FP32 factors of mxp_panel_lu, vectors in FP64, block substitution.
+ * When d_LU, n and lda are those of the last successful mxp_panel_lu on this
+ * workspace (and MXP_OPT_TRSV_INV is on), the diagonal blocks are solved
+ * with the inverses that LU kept (a product, then one refinement step against
+ * the factor block); a factor written into that buffer by other means must be
+ * solved after MXP_OPT_TRSV_INV is set again (setting it, to either value,
+ * forgets the stored inverses) or from another buffer.  Otherwise 64-row
+ * blocks substitute exactly in FP64 along a chain.  Blocking: reads the
+ * workspace status word (MXP_TIMEOUT when a bounded wait between row blocks
+ * gave up). */
 mxp_status mxp_lu_solve(int n, const float *d_LU, int64_t lda, double *d_x, mxp_workspace *ws,
                         void *stream);
 

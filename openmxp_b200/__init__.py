@@ -163,6 +163,7 @@ OPT_OVERLAP_MIN = 10
 OPT_TRSM_SINGLE = 11
 OPT_MERGE_DEPTH = 12
 OPT_INV_TC = 13
+OPT_TRSV_INV = 14
 
 
 class Workspace:

@@ -112,6 +112,15 @@ struct mxp_workspace {
     int inv_tc = 1024;       // inverse doubling levels from this block size on the tensor cores (0: none)
     int64_t ldk3 = 0;
     float *tinv_u = nullptr, *tinv_l = nullptr, *tinv_tmp = nullptr;
+    // inverses of every diagonal block kept for the refinement's triangular
+    // solves: block k's inv(U_kk) at inv_store + 2k*b*b, inv(L_kk) after it
+    int trsv_inv = 1;
+    int inv_blocks = 0;
+    float *inv_store = nullptr;
+    double *trsv_t = nullptr;             // 3 b doubles
+    const float *inv_lu = nullptr;        // factor the stored inverses belong to (nullptr: none)
+    int inv_n = 0;
+    int64_t inv_lda = 0;
     // cooperative diagonal-block factorisation (LU + inverses in one launch)
     int coop = 1;
     float *coop_tmp = nullptr;          // 2 x diag_factor_tmp_floats(b)
@@ -139,6 +148,9 @@ static size_t trsm_bytes(int n, int b) {
            (size_t)(rows + 2 * (int64_t)b) * ldk3 * 2 + 4096 + 2 * diag_factor_tmp_floats(b) * 4 + 256;
 }
 
+// Stored inverses of the diagonal blocks: 2 x (n / b) blocks of b x b floats.
+static size_t inv_store_bytes(int n, int b) { return 2 * (size_t)(n / b) * b * b * 4 + 256; }
+
 static size_t ws_layout(int n, int b, int form, size_t *panel_bytes, size_t *scale_bytes,
                         size_t *vec_doubles, size_t *flag_ints) {
     const int64_t ldk = panel_ldk(b, form);
@@ -150,7 +162,7 @@ static size_t ws_layout(int n, int b, int form, size_t *panel_bytes, size_t *sca
     *flag_ints = lu_solve_flag_ints(n) + 64;
     *vec_doubles += (size_t)31 * n + 64 * 32 + 2 * 31 * 64 + 31 * (size_t)(2 * 148 + 2) + 1024;
     return 2 * *panel_bytes + 2 * *scale_bytes + *vec_doubles * 8 + *flag_ints * 4 + 256 +
-           trsm_bytes(n, b);
+           trsm_bytes(n, b) + inv_store_bytes(n, b) + (size_t)3 * b * 8 + 256;
 }
 
 extern "C" size_t mxp_workspace_bytes(int n, int b, int form) {
@@ -219,6 +231,9 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
         ok = ok && (ws->split_big = alloc((size_t)rows * ws->ldk3 * 2 + 1024));
         ok = ok && (ws->split_u = alloc((size_t)b * ws->ldk3 * 2 + 1024));
         ok = ok && (ws->split_l = alloc((size_t)b * ws->ldk3 * 2 + 1024));
+        ws->inv_blocks = n / b;
+        ok = ok && (ws->inv_store = (float *)alloc(inv_store_bytes(n, b)));
+        ok = ok && (ws->trsv_t = (double *)alloc((size_t)3 * b * 8 + 256));
     }
     if (ok) ok = cudaMallocHost(&ws->h_scal, 64 * sizeof(double)) == cudaSuccess;
     if (ok) {
@@ -289,6 +304,10 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
             if (value != 0 && (value < 128 || (value & (value - 1)) != 0))
                 return fail(MXP_INVALID_ARG, "set_option: inverse level must be 0 or a power of two >= 128");
             ws->inv_tc = value;
+            return MXP_OK;
+        case MXP_OPT_TRSV_INV:
+            ws->trsv_inv = value ? 1 : 0;
+            ws->inv_lu = nullptr;  // setting it forgets the stored inverses
             return MXP_OK;
         case MXP_OPT_OVERLAP_MIN:
             if (value < 2) return fail(MXP_INVALID_ARG, "set_option: overlap minimum must be >= 2 blocks");
@@ -516,6 +535,16 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
     // panels per trailing pass; merging needs FP8 scale tiles aligned to the block size
     const int depth = (!fp8 || b % 128 == 0) ? ws->merge : 1;
     const int64_t sct = cdiv(b, 128);  // scale tiles per panel slot (FP8)
+    // The inverses of every diagonal block (the last one too) are kept for
+    // the refinement's triangular solves when the cooperative kernel makes them.
+    ws->inv_lu = nullptr;
+    const bool keep_inv = ws->trsv_inv && ws->coop && ws->trsm_tc && nb <= ws->inv_blocks;
+    auto inv_u = [&](int64_t kk) -> float * {
+        return keep_inv ? ws->inv_store + 2 * (kk / b) * (int64_t)b * b : ws->tinv_u;
+    };
+    auto inv_l = [&](int64_t kk) -> float * {
+        return keep_inv ? ws->inv_store + (2 * (kk / b) + 1) * (int64_t)b * b : ws->tinv_l;
+    };
     // C -= L R^T over panel slots slot0 .. slot0+kfac-1 (K = kfac * b), L rows
     // from buffer row lrow, R rows from buffer row rrow.
     auto schur = [&](int64_t mrows, int64_t ncols, int kfac, int64_t lrow, int64_t rrow, float *C,
@@ -534,18 +563,18 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
     auto factor_diag = [&](int64_t kk, cudaStream_t on, int max_grid) -> mxp_status {
         float *Akk = d_A + kk + kk * lda;
         const int m = n - (int)kk - b;
-        const bool coop_inv = ws->coop && ws->trsm_tc && m > 0;
+        const bool coop_inv = ws->coop && ws->trsm_tc && (m > 0 || keep_inv);
         float *tmpU = ws->coop_tmp, *tmpL = ws->coop_tmp + diag_factor_tmp_floats(b);
+        float *XU = inv_u(kk), *XL = inv_l(kk);
         if (!ws->coop) return launch_getrf_blocked(b, Akk, lda, ws->status, (int)kk, on);
         // the large doubling levels of the inverses on the tensor cores (same
         // stream; not beside a trailing pass, whose SMs they would share)
         const int tc = coop_inv && max_grid == 0 ? inv_tc_start(ws, b) : 0;
-        mxp_status q = launch_diag_factor(b, Akk, lda, coop_inv ? ws->tinv_u : nullptr,
-                                          coop_inv ? ws->tinv_l : nullptr, b, tmpU, tmpL, ws->coop_sync,
-                                          ws->status, (int)kk, on, max_grid, tc);
+        mxp_status q = launch_diag_factor(b, Akk, lda, coop_inv ? XU : nullptr, coop_inv ? XL : nullptr, b,
+                                          tmpU, tmpL, ws->coop_sync, ws->status, (int)kk, on, max_grid, tc);
         if (q == MXP_OK && tc > 0)
-            q = finish_inverses_tc(b, Akk, lda, ws->tinv_u, ws->tinv_l, b, tc,
-                                   ws->trsm_single ? kFormBf16 : MXP_FORM_BF16X2, tmpU, ws, on);
+            q = finish_inverses_tc(b, Akk, lda, XU, XL, b, tc, ws->trsm_single ? kFormBf16 : MXP_FORM_BF16X2,
+                                   tmpU, ws, on);
         return q;
     };
     // Factor the diagonal block of step kk (unless diag_done: it was factored
@@ -577,13 +606,13 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
             }
             pt.mark(PH_CAST);
             if (q == MXP_OK) q = launch_cast_left(bf, m, b, Lcol, lda, ws->split_big, ws->ldk3, nullptr, st);
-            if (q == MXP_OK) q = launch_cast_right(bf, b, b, ws->tinv_u, b, ws->split_u, ws->ldk3, nullptr, st);
+            if (q == MXP_OK) q = launch_cast_right(bf, b, b, inv_u(kk), b, ws->split_u, ws->ldk3, nullptr, st);
             pt.mark(PH_TGEMM);
             if (q == MXP_OK)
                 q = launch_schur(bf, m, b, b, ws->split_big, ws->ldk3, nullptr, ws->split_u, ws->ldk3,
                                  nullptr, Lcol, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/1, ws->trsm_pair);
             pt.mark(PH_CAST);
-            if (q == MXP_OK) q = launch_cast_left(bf, b, b, ws->tinv_l, b, ws->split_l, ws->ldk3, nullptr, st);
+            if (q == MXP_OK) q = launch_cast_left(bf, b, b, inv_l(kk), b, ws->split_l, ws->ldk3, nullptr, st);
             if (q == MXP_OK) q = launch_cast_right(bf, m, b, Urow, lda, ws->split_big, ws->ldk3, nullptr, st);
             pt.mark(PH_TGEMM);
             if (q == MXP_OK)
@@ -681,6 +710,11 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
     }
     DevStatus h;
     mxp_status rs = read_status(ws, st, &h);
+    if (rs == MXP_OK && keep_inv) {
+        ws->inv_lu = d_A;
+        ws->inv_n = n;
+        ws->inv_lda = lda;
+    }
     if (stats) {
         double ms[6];
         pt.collect(ms, 6);
@@ -702,6 +736,19 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
 // ---------------------------------------------------------------------------
 // refinement
 // ---------------------------------------------------------------------------
+// x <- U^{-1} L^{-1} x with the factor LU: by the stored inverses of the
+// diagonal blocks when they belong to this factor (the last mxp_panel_lu on
+// the workspace), else by the chain of 64-row blocks.
+static mxp_status lu_solve_ws(mxp_workspace *ws, int n, const float *LU, int64_t lda, double *x,
+                              cudaStream_t st, int withhold = -1) {
+    if (withhold < 0 && ws->trsv_inv && ws->inv_lu && LU == ws->inv_lu && n == ws->inv_n &&
+        lda == ws->inv_lda && lu_solve_inv_supported(n, ws->b, LU, lda)) {
+        const int64_t bb = (int64_t)ws->b * ws->b;
+        return launch_lu_solve_inv(n, ws->b, LU, lda, ws->inv_store, ws->inv_store + bb, 2 * bb, x, ws->trsv_t, st);
+    }
+    return launch_lu_solve(n, LU, lda, x, ws->flags, ws->status, st, withhold);
+}
+
 extern "C" mxp_status mxp_otf_gemv(int n, uint64_t seed, const double *d_d, double alpha,
                                    const double *d_x, double beta, double *d_y, mxp_workspace *ws,
                                    void *stream) {
@@ -718,7 +765,7 @@ extern "C" mxp_status mxp_lu_solve(int n, const float *d_LU, int64_t lda, double
     cudaStream_t st = as_stream(stream);
     const int withhold = ws->withhold;
     ws->withhold = -1;  // one call only
-    mxp_status s = launch_lu_solve(n, d_LU, lda, d_x, ws->flags, ws->status, st, withhold);
+    mxp_status s = lu_solve_ws(ws, n, d_LU, lda, d_x, st, withhold);
     if (s != MXP_OK) return s;
     return read_status(ws, st);  // bounded-wait timeouts surface here
 }
@@ -770,7 +817,7 @@ static mxp_status gmres_correction(int n, uint64_t seed, const float *LU, int64_
     };
     // z = M^{-1} r -> V_0 after normalisation
     s = launch_copy(n, r, V, st);
-    if (s == MXP_OK) s = timed(ms_trsv, [&] { return launch_lu_solve(n, LU, lda, V, ws->flags, ws->status, st); });
+    if (s == MXP_OK) s = timed(ms_trsv, [&] { return lu_solve_ws(ws, n, LU, lda, V, st); });
     if (s == MXP_OK) s = launch_mdot(n, 1, V, n, V, ws->gpart, sc + 0, 0, st);
     if (s == MXP_OK) s = launch_sqrt(sc + 0, sc + 1, st);
     if (s == MXP_OK) s = launch_vdiv(n, V, sc + 1, V, st);
@@ -788,7 +835,7 @@ static mxp_status gmres_correction(int n, uint64_t seed, const float *LU, int64_
         for (int j = 0; j < m; ++j) {
             double *vj = V + (int64_t)j * n;
             s = timed(ms_gemv, [&] { return launch_otf_gemv(n, seed, dd, 1.0, vj, 0.0, w, ws->partials, ws->max_splits, st); });
-            if (s == MXP_OK) s = timed(ms_trsv, [&] { return launch_lu_solve(n, LU, lda, w, ws->flags, ws->status, st); });
+            if (s == MXP_OK) s = timed(ms_trsv, [&] { return lu_solve_ws(ws, n, LU, lda, w, st); });
             // classical Gram-Schmidt, twice
             if (s == MXP_OK) s = launch_mdot(n, j + 1, V, n, w, ws->gpart, hcol, 0, st);
             if (s == MXP_OK) s = launch_vsub(n, j + 1, V, n, hcol, w, st);
@@ -908,7 +955,7 @@ extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float
             if (s != MXP_OK) return done(s);
         } else {
             cudaEventRecord(t0, st);
-            s = launch_lu_solve(n, d_LU, lda, r, ws->flags, ws->status, st);
+            s = lu_solve_ws(ws, n, d_LU, lda, r, st);
             cudaEventRecord(t1, st);
             if (s == MXP_OK) s = launch_axpy(n, 1.0, r, d_x, st);
             if (s != MXP_OK) return done(s);

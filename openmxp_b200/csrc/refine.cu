@@ -5,9 +5,10 @@
 //    The reference launches one <<<b,256>>> kernel per b x b block pair and
 //    synchronises after each; here one launch covers the matrix: each thread
 //    owns two rows (two independent LCG chains) over a column range and
-//    steps the state with J_n = INC1^n per column.  The state -> double
-//    conversion uses the exact split-integer route (no 64-bit converter),
-//    and the 2^-64 scale of RandStat::operator double is folded into x.
+//    steps the state with J_n = INC1^n per column.  Each state enters as
+//    its two exact 32-bit halves (no 64-bit converter, no rounding of the
+//    integer), and the 2^-64 scale of RandStat::operator double is folded
+//    into x.
 //    Column splits write partial sums to the workspace and a second kernel
 //    reduces them in a fixed order, so the result is deterministic.
 //  * lu_solve: x <- U^{-1} L^{-1} x with the FP32 factors (trsvL_h /
@@ -17,7 +18,12 @@
 //    (waiting, bounded, on per-block completion flags), then solves its 64 x
 //    64 diagonal triangle in FP64 and publishes.  Claim order guarantees every
 //    awaited block is owned by a CTA that is already running.
+//  * lu_solve_inv: the same solve in nb steps of bandwidth-bound products
+//    with the stored inverses of the b x b diagonal blocks (used after
+//    mxp_panel_lu, which keeps them); no chain of 64-row links.
 //  * infnorm / vector ops (panel_norm.hpp:11-58, panel.hpp:525-623).
+#include <algorithm>
+
 #include "mxp_internal.cuh"
 
 namespace mxp {
@@ -33,43 +39,75 @@ constexpr int kGemvRows = kGemvThreads * kGemvRowsPerThread;  // 256 rows per CT
 constexpr int kGemvXChunk = 1024;
 constexpr double kLcgScale = 0x1.fffffffffffffP-65;
 
+// Per element the state s = hi * 2^32 + lo (hi signed, lo unsigned) enters
+// as two exact doubles, both made by placing the integer in the mantissa of
+// a biased constant: hi * 2^32 = (2^84 + (hi ^ 2^31) * 2^32) - (2^84 + 2^63),
+// and 2^52 + lo, whose bias 2^52 is not removed per element: the CTA sums
+// 2^52 * xs over its columns once and subtracts it from every row at the
+// end (the bias terms are 2^-12 |x| each against |a_ij x| ~ |x|/4, so the
+// extra rounding stays far below the FP64 rounding of the sum itself).  The
+// diagonal column is accumulated like the others and its LCG value taken
+// out afterwards (no compare per element), then d_i x_i is added.
 __global__ void __launch_bounds__(kGemvThreads)
 otf_gemv_kernel(int n, uint64_t s00, Aff jn, const double *__restrict__ d,
                 const double *__restrict__ x, int64_t cols_per_split, double alpha, double beta,
                 double *__restrict__ y, double *__restrict__ partials) {
     __shared__ double xs[kGemvXChunk];
+    __shared__ double bias_red[kGemvThreads];
     const int64_t r0 = (int64_t)blockIdx.x * kGemvRows + threadIdx.x;
     const int64_t r1 = r0 + kGemvThreads;
     const int64_t j_begin = (int64_t)blockIdx.y * cols_per_split;
     const int64_t j_end = imin64(n, j_begin + cols_per_split);
+    constexpr double kHiBias = 0x1p84 + 0x1p63;
+    constexpr double kLoBias = 0x1p52;
 
     const Aff inc1 = lcg_inc1();
     // states of (r0, j_begin) and (r1, j_begin)
     uint64_t s0 = aff_apply(aff_pow(inc1, (uint64_t)r0 + (uint64_t)n * (uint64_t)j_begin), s00);
     uint64_t s1 = aff_apply(aff_pow(inc1, (uint64_t)kGemvThreads), s0);
-    double acc0 = 0.0, acc1 = 0.0;
+    double acc0 = 0.0, acc1 = 0.0, bias = 0.0;
     for (int64_t jc = j_begin; jc < j_end; jc += kGemvXChunk) {
         const int len = (int)imin64(kGemvXChunk, j_end - jc);
         __syncthreads();
-        for (int q = threadIdx.x; q < len; q += kGemvThreads) xs[q] = x[jc + q] * kLcgScale;
+        for (int q = threadIdx.x; q < len; q += kGemvThreads) {
+            const double v = x[jc + q] * kLcgScale;
+            xs[q] = v;
+            bias = __fma_rn(kLoBias, v, bias);
+        }
         __syncthreads();
 #pragma unroll 4
         for (int q = 0; q < len; ++q) {
-            const int64_t j = jc + q;
             const double xq = xs[q];
-            double v0 = i64_to_double_rn(s0);
-            double v1 = i64_to_double_rn(s1);
-            v0 = (j == r0) ? 0.0 : v0;
-            v1 = (j == r1) ? 0.0 : v1;
-            acc0 = __fma_rn(v0, xq, acc0);
-            acc1 = __fma_rn(v1, xq, acc1);
+            const double h0 = __hiloint2double(0x45300000, (int)((uint32_t)(s0 >> 32) ^ 0x80000000u)) - kHiBias;
+            const double h1 = __hiloint2double(0x45300000, (int)((uint32_t)(s1 >> 32) ^ 0x80000000u)) - kHiBias;
+            acc0 = __fma_rn(h0, xq, acc0);
+            acc1 = __fma_rn(h1, xq, acc1);
+            acc0 = __fma_rn(__hiloint2double(0x43300000, (int)(uint32_t)s0), xq, acc0);
+            acc1 = __fma_rn(__hiloint2double(0x43300000, (int)(uint32_t)s1), xq, acc1);
             s0 = aff_apply(jn, s0);
             s1 = aff_apply(jn, s1);
         }
     }
-    // diagonal entries come from d (otf_gemv_diag_d, panel_gemv.hpp:26)
-    if (r0 < n && r0 >= j_begin && r0 < j_end) acc0 += d[r0] * x[r0];
-    if (r1 < n && r1 >= j_begin && r1 < j_end) acc1 += d[r1] * x[r1];
+    // the CTA's bias sum, in a fixed order
+    bias_red[threadIdx.x] = bias;
+    __syncthreads();
+    for (int w = kGemvThreads / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) bias_red[threadIdx.x] += bias_red[threadIdx.x + w];
+        __syncthreads();
+    }
+    bias = bias_red[0];
+    acc0 -= bias;
+    acc1 -= bias;
+    // diagonal entries come from d (otf_gemv_diag_d, panel_gemv.hpp:26): the
+    // LCG value accumulated at (r, r) is taken out, d_r x_r added
+    if (r0 < n && r0 >= j_begin && r0 < j_end) {
+        const uint64_t sd = aff_apply(aff_pow(inc1, (uint64_t)r0 + (uint64_t)n * (uint64_t)r0), s00);
+        acc0 = __fma_rn(-i64_to_double_rn(sd), x[r0] * kLcgScale, acc0) + d[r0] * x[r0];
+    }
+    if (r1 < n && r1 >= j_begin && r1 < j_end) {
+        const uint64_t sd = aff_apply(aff_pow(inc1, (uint64_t)r1 + (uint64_t)n * (uint64_t)r1), s00);
+        acc1 = __fma_rn(-i64_to_double_rn(sd), x[r1] * kLcgScale, acc1) + d[r1] * x[r1];
+    }
     if (partials) {
         double *p = partials + (int64_t)blockIdx.y * n;
         if (r0 < n) p[r0] = acc0;
@@ -326,6 +364,118 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
 }
 
 // ---------------------------------------------------------------------------
+// block triangular solves with the stored inverses of the diagonal blocks
+// ---------------------------------------------------------------------------
+// The LU keeps inv(L_kk) and inv(U_kk) of every b x b diagonal block (the
+// TRSM-by-inverse computes them anyway).  A triangle is then solved in nb
+// steps of bandwidth-bound products instead of a chain of 64-row links:
+//   lower, k = 0 .. nb-1:  x_k <- L_kk^{-1} x_k;  x_i -= L(i, k) x_k (rows below)
+//   upper, k = nb-1 .. 0:  x_k <- U_kk^{-1} x_k;  x_i -= U(i, k) x_k (rows above)
+// Block substitution as trsvL_h / trsvU_h (panel_trsv.hpp:308-597).  The
+// diagonal-block solve is a product with the stored inverse X followed by
+// one step of refinement against the factor block T, all in FP64:
+//   t1 = X v,  s = v - T t1,  t = t1 + X s,
+// so the result carries the square of the inverse's relative error (the
+// inverse's tensor-core levels are near FP32, not FP32).  The unit diagonal
+// of inv(L) and the diagonal 1/u_ii of inv(U) are applied exactly.  Every
+// row is summed by one CTA in a fixed order: results are deterministic.
+constexpr int kIvThreads = 256;
+
+// One CTA: ROWS rows (ROWS/4 quads of four rows, one float4 per column) x
+// 256 / (ROWS/4) column groups.  M: column-major FP32, ldm % 4 == 0, 16-byte
+// aligned.  v: cols doubles, staged in shared memory.  With sum_i over the
+// mode's entries of row i:
+//   MODE 0: out[i] = base[i] - sum_j M(i,j) v_j                 (all columns)
+//   MODE 1: out[i] = [base[i] +] v_i + sum_{j<i} M(i,j) v_j      (unit lower inverse)
+//   MODE 2: out[i] = [base[i] +] v_i / T(i,i) + sum_{j>i} M(i,j) v_j  (upper inverse)
+//   MODE 3: out[i] = base[i] - v_i - sum_{j<i} M(i,j) v_j        (v - T v, T unit lower)
+//   MODE 4: out[i] = base[i] - sum_{j>=i} M(i,j) v_j             (v - T v, T upper)
+// T(i,i) is read from tdiag (ld ldt).  CTA 0 also writes copy_dst[0..cols) = v.
+template <int MODE, int ROWS>
+__global__ void __launch_bounds__(kIvThreads)
+trsv_inv_kernel(int rows, int cols, const float *__restrict__ M, int64_t ldm, const double *v,
+                const float *__restrict__ tdiag, int64_t ldt, const double *base, double *out,
+                double *copy_dst) {
+    constexpr int QUADS = ROWS / 4;
+    constexpr int GROUPS = kIvThreads / QUADS;
+    extern __shared__ __align__(16) unsigned char iv_smem[];
+    double *vs = reinterpret_cast<double *>(iv_smem);
+    double(*red)[ROWS + 1] = reinterpret_cast<double(*)[ROWS + 1]>(vs + cols);
+    const int tid = threadIdx.x;
+    for (int j = tid; j < cols; j += kIvThreads) vs[j] = v[j];
+    __syncthreads();
+    if (copy_dst && blockIdx.x == 0)
+        for (int j = tid; j < cols; j += kIvThreads) copy_dst[j] = vs[j];
+    const int r0 = blockIdx.x * ROWS;
+    if (r0 >= rows) return;  // a CTA launched only for the copy
+    const int q = tid % QUADS, g = tid / QUADS;
+    const int ri = r0 + 4 * q;  // first of this thread's four rows
+    constexpr bool kLow = MODE == 1 || MODE == 3;   // strictly lower entries
+    constexpr bool kUpS = MODE == 2;                // strictly upper
+    constexpr bool kUpD = MODE == 4;                // upper with the diagonal
+    // column range the CTA's rows need
+    int jb = 0, je = cols;
+    if (kLow) je = min(cols, r0 + ROWS - 1);
+    if (kUpS) jb = r0 + 1;
+    if (kUpD) jb = r0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    const float *mp = M + ri;
+    auto fma4 = [&](float4 m, int j) {
+        const double vj = vs[j];
+        if (MODE == 0) {
+            a0 = __fma_rn((double)m.x, vj, a0);
+            a1 = __fma_rn((double)m.y, vj, a1);
+            a2 = __fma_rn((double)m.z, vj, a2);
+            a3 = __fma_rn((double)m.w, vj, a3);
+        } else {
+            const bool k0 = kLow ? j < ri : (kUpS ? j > ri : j >= ri);
+            const bool k1 = kLow ? j < ri + 1 : (kUpS ? j > ri + 1 : j >= ri + 1);
+            const bool k2 = kLow ? j < ri + 2 : (kUpS ? j > ri + 2 : j >= ri + 2);
+            const bool k3 = kLow ? j < ri + 3 : (kUpS ? j > ri + 3 : j >= ri + 3);
+            a0 = __fma_rn(k0 ? (double)m.x : 0.0, vj, a0);
+            a1 = __fma_rn(k1 ? (double)m.y : 0.0, vj, a1);
+            a2 = __fma_rn(k2 ? (double)m.z : 0.0, vj, a2);
+            a3 = __fma_rn(k3 ? (double)m.w : 0.0, vj, a3);
+        }
+    };
+    int j = jb + g;
+    // eight 16-byte loads in flight per thread
+    for (; j + 7 * GROUPS < je; j += 8 * GROUPS) {
+        float4 m[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            m[u] = __ldcs(reinterpret_cast<const float4 *>(mp + (int64_t)(j + GROUPS * u) * ldm));
+#pragma unroll
+        for (int u = 0; u < 8; ++u) fma4(m[u], j + GROUPS * u);
+    }
+    for (; j < je; j += GROUPS) fma4(__ldcs(reinterpret_cast<const float4 *>(mp + (int64_t)j * ldm)), j);
+    red[g][4 * q + 0] = a0;
+    red[g][4 * q + 1] = a1;
+    red[g][4 * q + 2] = a2;
+    red[g][4 * q + 3] = a3;
+    __syncthreads();
+    if (tid < ROWS) {
+        double s = 0.0;
+#pragma unroll 8
+        for (int c = 0; c < GROUPS; ++c) s += red[c][tid];
+        const int i = r0 + tid;
+        double y;
+        if (MODE == 0) y = base[i] - s;
+        else if (MODE == 1) y = vs[i] + s;
+        else if (MODE == 2) y = vs[i] / (double)tdiag[(int64_t)i * (ldt + 1)] + s;
+        else if (MODE == 3) y = base[i] - vs[i] - s;
+        else y = base[i] - s;
+        if ((MODE == 1 || MODE == 2) && base) y += base[i];
+        out[i] = y;
+    }
+}
+
+constexpr int kIvRowsUpd = 32;   // rows per CTA of the trailing products
+constexpr int kIvRowsDiag = 16;  // rows per CTA of the diagonal-block products (b / 16 CTAs)
+
+size_t trsv_inv_smem(int b) { return (size_t)b * sizeof(double) + sizeof(double) * 64 * (kIvRowsUpd + 1); }
+
+// ---------------------------------------------------------------------------
 // norms and vector ops
 // ---------------------------------------------------------------------------
 __global__ void infnorm_kernel(int n, const double *__restrict__ x, unsigned long long *out) {
@@ -420,6 +570,64 @@ mxp_status launch_lu_solve(int n, const float *LU, int64_t lda, double *x, int *
     MXP_LAUNCHED();
     trsv_kernel<false><<<nrb, kTrsvThreads, kTrsvSmem, st>>>(n, LU, lda, x, flags + nrb + 1, dst, -1);
     MXP_LAUNCHED();
+    return MXP_OK;
+}
+
+bool lu_solve_inv_supported(int n, int b, const float *LU, int64_t lda) {
+    return n > 0 && b > 0 && n % b == 0 && b % kIvRowsUpd == 0 && lda % 4 == 0 &&
+           (reinterpret_cast<uintptr_t>(LU) & 15u) == 0 && trsv_inv_smem(b) <= 200 * 1024;
+}
+
+mxp_status launch_lu_solve_inv(int n, int b, const float *LU, int64_t lda, const float *XU,
+                               const float *XL, int64_t xstride, double *x, double *t, cudaStream_t st) {
+    if (n <= 0) return MXP_OK;
+    if (!lu_solve_inv_supported(n, b, LU, lda) || xstride % 4 != 0 ||
+        ((reinterpret_cast<uintptr_t>(XU) | reinterpret_cast<uintptr_t>(XL)) & 15u))
+        return fail(MXP_INVALID_ARG, "lu_solve_inv: shape or alignment not supported");
+    const int nb = n / b;
+    const size_t smem = trsv_inv_smem(b);
+    if (smem > 48 * 1024) {
+        MXP_CUDA(cudaFuncSetAttribute(trsv_inv_kernel<0, kIvRowsUpd>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        MXP_CUDA(cudaFuncSetAttribute(trsv_inv_kernel<1, kIvRowsDiag>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        MXP_CUDA(cudaFuncSetAttribute(trsv_inv_kernel<2, kIvRowsDiag>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        MXP_CUDA(cudaFuncSetAttribute(trsv_inv_kernel<3, kIvRowsDiag>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        MXP_CUDA(cudaFuncSetAttribute(trsv_inv_kernel<4, kIvRowsDiag>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    double *t1 = t, *sv = t + b, *t2 = t + 2 * (int64_t)b;  // 3 b doubles
+    const unsigned dg = (unsigned)(b / kIvRowsDiag);
+    auto upd_grid = [](int rows) { return (unsigned)std::max(1, rows / kIvRowsUpd); };
+    // forward: unit lower L
+    for (int k = 0; k < nb; ++k) {
+        const int64_t kk = (int64_t)k * b;
+        const float *X = XL + k * xstride, *T = LU + kk + kk * lda;
+        double *xk = x + kk;
+        trsv_inv_kernel<1, kIvRowsDiag><<<dg, kIvThreads, smem, st>>>(b, b, X, b, xk, nullptr, 0, nullptr, t1, nullptr);
+        MXP_LAUNCHED();
+        trsv_inv_kernel<3, kIvRowsDiag><<<dg, kIvThreads, smem, st>>>(b, b, T, lda, t1, nullptr, 0, xk, sv, nullptr);
+        MXP_LAUNCHED();
+        trsv_inv_kernel<1, kIvRowsDiag><<<dg, kIvThreads, smem, st>>>(b, b, X, b, sv, nullptr, 0, t1, t2, nullptr);
+        MXP_LAUNCHED();
+        const int rows = (int)(n - kk - b);
+        trsv_inv_kernel<0, kIvRowsUpd><<<upd_grid(rows), kIvThreads, smem, st>>>(
+            rows, b, LU + (kk + b) + kk * lda, lda, t2, nullptr, 0, x + kk + b, x + kk + b, xk);
+        MXP_LAUNCHED();
+    }
+    // backward: upper U
+    for (int k = nb - 1; k >= 0; --k) {
+        const int64_t kk = (int64_t)k * b;
+        const float *X = XU + k * xstride, *T = LU + kk + kk * lda;
+        double *xk = x + kk;
+        trsv_inv_kernel<2, kIvRowsDiag><<<dg, kIvThreads, smem, st>>>(b, b, X, b, xk, T, lda, nullptr, t1, nullptr);
+        MXP_LAUNCHED();
+        trsv_inv_kernel<4, kIvRowsDiag><<<dg, kIvThreads, smem, st>>>(b, b, T, lda, t1, nullptr, 0, xk, sv, nullptr);
+        MXP_LAUNCHED();
+        trsv_inv_kernel<2, kIvRowsDiag><<<dg, kIvThreads, smem, st>>>(b, b, X, b, sv, T, lda, t1, t2, nullptr);
+        MXP_LAUNCHED();
+        const int rows = (int)kk;
+        trsv_inv_kernel<0, kIvRowsUpd><<<upd_grid(rows), kIvThreads, smem, st>>>(
+            rows, b, LU + kk * lda, lda, t2, nullptr, 0, x, x, xk);
+        MXP_LAUNCHED();
+    }
     return MXP_OK;
 }
 

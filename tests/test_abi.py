@@ -30,9 +30,10 @@ def test_library_exports_every_declared_symbol(mxp):
 
 def test_version_and_sizes(mxp):
     assert b"sm_100a" in mxp.lib().mxp_version()
-    # C3: FP16 panels 4 x (N-B) x B x 2 bytes plus vectors; well under 8 GB
+    # C3: FP16 panels 4 x (N-B) x B x 2 bytes, vectors, and the inverses of
+    # the 48 diagonal blocks kept for the refinement (2 x N x B x 4 bytes)
     nbytes = mxp.Workspace.bytes(122880, 2560, mxp.FORM_FP16)
-    assert 2.4e9 < nbytes < 8e9
+    assert 2.4e9 + 2 * 122880 * 2560 * 4 < nbytes < 10e9
     assert mxp.Workspace.bytes(122880, 2560, mxp.FORM_BF16X2) > 2.9 * 2.4e9
 
 
