@@ -593,40 +593,57 @@ def run_batched(args):
     import torch
 
     import openmxp_b200 as mxp
-    torch.cuda.set_device(0)
-    sizes = mxp.batch_sizes(args.batch_count, args.batch_size_seed)
-    seeds = [1000 + i for i in range(len(sizes))]
-    bt = mxp.Batch(sizes, seeds)
+    world, rank, local = dist_env()
+    dist = init_dist("nccl") if world > 1 else None
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    all_sizes = mxp.batch_sizes(args.batch_count, args.batch_size_seed)
+    all_seeds = [1000 + i for i in range(len(all_sizes))]
+    # independent systems: each rank solves its part (balanced by n^3), no
+    # exchange between GPUs; the job time is the slowest rank's
+    part = mxp.batch_partition(all_sizes, world) if world > 1 else [0] * len(all_sizes)
+    mine = [i for i in range(len(all_sizes)) if part[i] == rank]
+    sizes = [all_sizes[i] for i in mine]
+    seeds = [all_seeds[i] for i in mine]
+    bt = mxp.Batch(sizes, seeds, device=local)
     bt.matgen()
     tune = bt.autotune() if not args.batch_config else None
     if args.batch_config:
         b, tn, stg = (int(v) for v in args.batch_config.split(","))
         bt.set_config(b, tn, stg)
-    flops = batch_flops(sizes)
+    flops = batch_flops(all_sizes)
     for _ in range(args.warmup):
         bt.matgen()
         bt.solve()
     ms = []
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(local)
     clocks.start()
     mxp.reset_kernel_launches()
     for _ in range(args.steps):
         bt.matgen()
         torch.cuda.synchronize()
-        ms.append(bt.solve()["ms_total"])
-    launches = mxp.kernel_launches()
+        barrier(dist)
+        ms.append(max_over_ranks(bt.solve()["ms_total"], dist, dev))
+    launches = int(sum_over_ranks(mxp.kernel_launches(), dist, dev))
     clk = clocks.stop()
     res = bt.results()
     t = sum(ms) / len(ms) / 1e3
-    out = {"metric": "batched solve: systems/s and credited TFLOP/s", "value": len(sizes) / t,
-           "unit": "systems/s", "tflops": flops / t / 1e12, "ms_per_step": 1e3 * t,
-           "steps": args.steps, "warmup": args.warmup, "systems": len(sizes),
-           "orders": {"min": min(sizes), "max": max(sizes), "sum_n3": float(sum(n ** 3 for n in sizes))},
+    converged = int(sum_over_ranks(sum(r["converged"] for r in res), dist, dev))
+    max_it = int(max_over_ranks(max(r["iterations"] for r in res), dist, dev))
+    max_hpl = max_over_ranks(max(r["hpl_harness"] for r in res), dist, dev)
+    out = {"metric": "batched solve: systems/s and credited TFLOP/s", "value": len(all_sizes) / t,
+           "unit": "systems/s", "tflops": flops / t / 1e12, "ms_per_step": 1e3 * t, "n_gpus": world,
+           "scaling": "strong", "steps": args.steps, "warmup": args.warmup, "systems": len(all_sizes),
+           "orders": {"min": min(all_sizes), "max": max(all_sizes),
+                      "sum_n3": float(sum(n ** 3 for n in all_sizes))},
            "config": tune if tune else {"b": b, "tile_n": tn, "stages": stg},
-           "converged": sum(r["converged"] for r in res), "max_iterations": max(r["iterations"] for r in res),
-           "max_hpl_harness": max(r["hpl_harness"] for r in res), "gpu_launches": launches, "clocks": clk}
+           "converged": converged, "max_iterations": max_it, "max_hpl_harness": max_hpl,
+           "gpu_launches": launches, "clocks": clk}
+    if world > 1:
+        out["partition"] = "systems split by n^3 (mxp_batch_partition); rank 0 share of n^3: %.3f" % (
+            sum(n ** 3 for n in sizes) / sum(n ** 3 for n in all_sizes))
     # per-system loop of the plain single-system path on a sample of the systems
-    if args.batch_loop_sample > 0:
+    if args.batch_loop_sample > 0 and world == 1:
         stride = max(1, len(sizes) // args.batch_loop_sample)
         idx = list(range(0, len(sizes), stride))[: args.batch_loop_sample]
         loop_s, loop_flops = 0.0, 0.0
@@ -653,7 +670,11 @@ def run_batched(args):
                                   "what": "mxp_solve (FP16 Schur, B=256 or 128, classic IR) one system at a time"}
         out["speedup_vs_loop"] = out["value"] / out["per_system_loop"]["systems_per_s"]
     bt.close()
-    print(json.dumps(out), flush=True)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    barrier(dist)
+    if dist is not None:
+        dist.destroy_process_group()
     return 0
 
 

@@ -340,6 +340,13 @@ typedef struct {
 /* Orders of a batch drawn from the generator stream of size_seed: value i,
  * v in [-0.5, 0.5], gives n = 128 * (2 + floor((v + 0.5) * 31)). */
 mxp_status mxp_batch_sizes(int count, uint64_t size_seed, int *h_n);
+/* Split a batch over nparts GPUs (no reference counterpart: the reference
+ * solves one system per job).  Systems are independent, so each part is
+ * solved by its own mxp_batch with no exchange between GPUs; the parts are
+ * balanced by the LU work n^3: largest first, each to the part with the least
+ * work so far (ties to the lower part).  Deterministic, so every rank computes
+ * the same split.  h_part[i] in [0, nparts). */
+mxp_status mxp_batch_partition(int count, const int *h_n, int nparts, int *h_part);
 mxp_status mxp_batch_create(int count, const int *h_n, const uint64_t *h_seed, int device, mxp_batch **out);
 mxp_status mxp_batch_destroy(mxp_batch *bt);
 mxp_status mxp_batch_layout(const mxp_batch *bt, int64_t *matrix_floats, int64_t *vector_doubles,

@@ -103,6 +103,7 @@ _SIGS = {
                               _vp, C.POINTER(LuStats), C.POINTER(IrStats)]),
     "mxp_infnorm": (_i32, [_i32, _vp, C.POINTER(_dbl), _vp, _vp]),
     "mxp_batch_sizes": (_i32, [_i32, _u64, C.POINTER(C.c_int)]),
+    "mxp_batch_partition": (_i32, [_i32, C.POINTER(C.c_int), _i32, C.POINTER(C.c_int)]),
     "mxp_batch_create": (_i32, [_i32, C.POINTER(C.c_int), C.POINTER(C.c_uint64), _i32, C.POINTER(_vp)]),
     "mxp_batch_destroy": (_i32, [_vp]),
     "mxp_batch_layout": (_i32, [_vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
@@ -387,6 +388,15 @@ def hpl_flops(n: int) -> float:
 # ---------------------------------------------------------------------------
 # batched form: many systems of uneven orders in one persistent launch
 # ---------------------------------------------------------------------------
+def batch_partition(sizes, nparts: int) -> list:
+    """Part (0 .. nparts-1) of each system: largest first, each to the part with
+    the least n^3 work so far (mxp_batch_partition)."""
+    n = len(sizes)
+    out = (C.c_int * n)()
+    check(lib().mxp_batch_partition(n, (C.c_int * n)(*sizes), nparts, out))
+    return list(out)
+
+
 def batch_sizes(count: int, size_seed: int = 3) -> list:
     """Orders 128 * (2 + floor((v + 0.5) * 31)) from the generator stream of size_seed."""
     out = (C.c_int * count)()

@@ -793,6 +793,27 @@ extern "C" mxp_status mxp_batch_sizes(int count, uint64_t size_seed, int *h_n) {
     return MXP_OK;
 }
 
+extern "C" mxp_status mxp_batch_partition(int count, const int *h_n, int nparts, int *h_part) {
+    if (count <= 0 || !h_n || !h_part || nparts <= 0) return fail(MXP_INVALID_ARG, "batch_partition: bad arguments");
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) {
+        if (h_n[i] <= 0) return fail(MXP_INVALID_ARG, "batch_partition: every n must be positive");
+        order[i] = i;
+    }
+    // largest first (stable: equal orders keep their index order)
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h_n[a] > h_n[b]; });
+    std::vector<double> load(nparts, 0.0);
+    for (int i : order) {
+        int best = 0;
+        for (int p = 1; p < nparts; ++p)
+            if (load[p] < load[best]) best = p;
+        const double n = h_n[i];
+        load[best] += n * n * n;
+        h_part[i] = best;
+    }
+    return MXP_OK;
+}
+
 extern "C" mxp_status mxp_batch_create(int count, const int *h_n, const uint64_t *h_seed, int device,
                                        mxp_batch **out) {
     if (!out || count <= 0 || !h_n || !h_seed) return fail(MXP_INVALID_ARG, "batch_create: bad arguments");

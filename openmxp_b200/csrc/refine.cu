@@ -379,10 +379,14 @@ trsv_kernel(int n, const float *__restrict__ LU, int64_t lda, double *x, int *fl
 // inverse's tensor-core levels are near FP32, not FP32).  The unit diagonal
 // of inv(L) and the diagonal 1/u_ii of inv(U) are applied exactly.  Every
 // row is summed by one CTA in a fixed order: results are deterministic.
+// The diagonal-block products are load-latency bound (a 13 MB triangle at
+// b = 2560): small row tiles give many CTAs, each staging only the part of v
+// its rows use; the trailing products stream the factor at HBM bandwidth.
 constexpr int kIvThreads = 256;
 
 // One CTA: ROWS rows (ROWS/4 quads of four rows, one float4 per column) x
-// 256 / (ROWS/4) column groups.  M: column-major FP32, ldm % 4 == 0, 16-byte
+// 256 / (ROWS/4) column groups (ROWS >= 8: a warp reads whole 32-byte
+// sectors).  M: column-major FP32, ldm % 4 == 0, 16-byte
 // aligned.  v: cols doubles, staged in shared memory.  With sum_i over the
 // mode's entries of row i:
 //   MODE 0: out[i] = base[i] - sum_j M(i,j) v_j                 (all columns)
@@ -402,17 +406,23 @@ trsv_inv_kernel(int rows, int cols, const float *__restrict__ M, int64_t ldm, co
     double *vs = reinterpret_cast<double *>(iv_smem);
     double(*red)[ROWS + 1] = reinterpret_cast<double(*)[ROWS + 1]>(vs + cols);
     const int tid = threadIdx.x;
-    for (int j = tid; j < cols; j += kIvThreads) vs[j] = v[j];
-    __syncthreads();
-    if (copy_dst && blockIdx.x == 0)
-        for (int j = tid; j < cols; j += kIvThreads) copy_dst[j] = vs[j];
     const int r0 = blockIdx.x * ROWS;
-    if (r0 >= rows) return;  // a CTA launched only for the copy
-    const int q = tid % QUADS, g = tid / QUADS;
-    const int ri = r0 + 4 * q;  // first of this thread's four rows
     constexpr bool kLow = MODE == 1 || MODE == 3;   // strictly lower entries
     constexpr bool kUpS = MODE == 2;                // strictly upper
     constexpr bool kUpD = MODE == 4;                // upper with the diagonal
+    // the part of v this CTA reads: its rows and the columns they need
+    int s0 = 0, s1 = cols;
+    if (MODE != 0 && r0 < rows) {
+        if (kLow) s1 = min(cols, r0 + ROWS);
+        else s0 = r0;
+    }
+    for (int j = s0 + tid; j < s1; j += kIvThreads) vs[j] = v[j];
+    __syncthreads();
+    if (copy_dst && blockIdx.x == 0)
+        for (int j = tid; j < cols; j += kIvThreads) copy_dst[j] = vs[j];
+    if (r0 >= rows) return;  // a CTA launched only for the copy
+    const int q = tid % QUADS, g = tid / QUADS;
+    const int ri = r0 + 4 * q;  // first of this thread's four rows
     // column range the CTA's rows need
     int jb = 0, je = cols;
     if (kLow) je = min(cols, r0 + ROWS - 1);
@@ -471,7 +481,7 @@ trsv_inv_kernel(int rows, int cols, const float *__restrict__ M, int64_t ldm, co
 }
 
 constexpr int kIvRowsUpd = 32;   // rows per CTA of the trailing products
-constexpr int kIvRowsDiag = 16;  // rows per CTA of the diagonal-block products (b / 16 CTAs)
+constexpr int kIvRowsDiag = 8;   // rows per CTA of the diagonal-block products (b / 8 CTAs)
 
 size_t trsv_inv_smem(int b) { return (size_t)b * sizeof(double) + sizeof(double) * 64 * (kIvRowsUpd + 1); }
 

@@ -20,3 +20,26 @@ def test_batch_sizes_follow_the_generator(mxp, orc):
 def test_batch_sizes_reject_bad_count(mxp):
     with pytest.raises(mxp.MxpError):
         mxp.batch_sizes(0, 3)
+
+
+@pytest.mark.parametrize("nparts", [1, 2, 3, 8])
+def test_batch_partition_balances_lu_work(mxp, nparts):
+    """mxp_batch_partition: largest system first, each to the part with the least
+    n^3 so far (ties to the lower part), restated here in Python."""
+    sizes = mxp.batch_sizes(2048, 3)
+    got = mxp.batch_partition(sizes, nparts)
+    load = [0.0] * nparts
+    want = [0] * len(sizes)
+    for i in sorted(range(len(sizes)), key=lambda i: (-sizes[i], i)):
+        p = min(range(nparts), key=lambda k: (load[k], k))
+        load[p] += float(sizes[i]) ** 3
+        want[i] = p
+    assert got == want
+    assert max(load) / (sum(load) / nparts) < 1.01
+
+
+def test_batch_partition_rejects_bad_arguments(mxp):
+    with pytest.raises(mxp.MxpError):
+        mxp.batch_partition([256, 512], 0)
+    with pytest.raises(mxp.MxpError):
+        mxp.batch_partition([256, -1], 2)
