@@ -117,7 +117,8 @@ struct mxp_workspace {
     int trsv_inv = 1;
     int inv_blocks = 0;
     float *inv_store = nullptr;
-    double *trsv_t = nullptr;             // 3 b doubles
+    double *trsv_t = nullptr;             // 4 b doubles
+    cudaEvent_t ev_trsv[4] = {nullptr, nullptr, nullptr, nullptr};  // two-stream refinement solves
     const float *inv_lu = nullptr;        // factor the stored inverses belong to (nullptr: none)
     int inv_n = 0;
     int64_t inv_lda = 0;
@@ -162,7 +163,7 @@ static size_t ws_layout(int n, int b, int form, size_t *panel_bytes, size_t *sca
     *flag_ints = lu_solve_flag_ints(n) + 64;
     *vec_doubles += (size_t)31 * n + 64 * 32 + 2 * 31 * 64 + 31 * (size_t)(2 * 148 + 2) + 1024;
     return 2 * *panel_bytes + 2 * *scale_bytes + *vec_doubles * 8 + *flag_ints * 4 + 256 +
-           trsm_bytes(n, b) + inv_store_bytes(n, b) + (size_t)3 * b * 8 + 256;
+           trsm_bytes(n, b) + inv_store_bytes(n, b) + (size_t)4 * b * 8 + 256;
 }
 
 extern "C" size_t mxp_workspace_bytes(int n, int b, int form) {
@@ -181,6 +182,8 @@ extern "C" mxp_status mxp_workspace_destroy(mxp_workspace *ws) {
     if (ws->h_scal) cudaFreeHost(ws->h_scal);
     if (ws->ev_fork) cudaEventDestroy(ws->ev_fork);
     if (ws->ev_join) cudaEventDestroy(ws->ev_join);
+    for (cudaEvent_t e : ws->ev_trsv)
+        if (e) cudaEventDestroy(e);
     if (ws->side) cudaStreamDestroy(ws->side);
     cudaSetDevice(cur);
     delete ws;
@@ -233,7 +236,7 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
         ok = ok && (ws->split_l = alloc((size_t)b * ws->ldk3 * 2 + 1024));
         ws->inv_blocks = n / b;
         ok = ok && (ws->inv_store = (float *)alloc(inv_store_bytes(n, b)));
-        ok = ok && (ws->trsv_t = (double *)alloc((size_t)3 * b * 8 + 256));
+        ok = ok && (ws->trsv_t = (double *)alloc((size_t)4 * b * 8 + 256));
     }
     if (ok) ok = cudaMallocHost(&ws->h_scal, 64 * sizeof(double)) == cudaSuccess;
     if (ok) {
@@ -242,6 +245,8 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
              cudaStreamCreateWithPriority(&ws->side, cudaStreamNonBlocking, greatest) == cudaSuccess &&
              cudaEventCreateWithFlags(&ws->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&ws->ev_join, cudaEventDisableTiming) == cudaSuccess;
+        for (int e = 0; e < 4 && ok; ++e)
+            ok = cudaEventCreateWithFlags(&ws->ev_trsv[e], cudaEventDisableTiming) == cudaSuccess;
     }
     if (!ok) {
         cudaGetLastError();
@@ -744,7 +749,8 @@ static mxp_status lu_solve_ws(mxp_workspace *ws, int n, const float *LU, int64_t
     if (withhold < 0 && ws->trsv_inv && ws->inv_lu && LU == ws->inv_lu && n == ws->inv_n &&
         lda == ws->inv_lda && lu_solve_inv_supported(n, ws->b, LU, lda)) {
         const int64_t bb = (int64_t)ws->b * ws->b;
-        return launch_lu_solve_inv(n, ws->b, LU, lda, ws->inv_store, ws->inv_store + bb, 2 * bb, x, ws->trsv_t, st);
+        return launch_lu_solve_inv(n, ws->b, LU, lda, ws->inv_store, ws->inv_store + bb, 2 * bb, x, ws->trsv_t, st,
+                                   ws->side, ws->ev_trsv);
     }
     return launch_lu_solve(n, LU, lda, x, ws->flags, ws->status, st, withhold);
 }

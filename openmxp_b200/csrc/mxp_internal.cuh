@@ -194,11 +194,15 @@ mxp_status launch_lu_solve(int n, const float *LU, int64_t lda, double *x, int *
 size_t lu_solve_flag_ints(int n);
 // Block triangular solves with the stored FP32 inverses of the b x b diagonal
 // blocks (XU: inv(U_kk), XL: inv(L_kk), block k at offset k*xstride, ld b):
-// x <- U^{-1} L^{-1} x.  t: 3 b doubles of scratch.  Needs n % b == 0,
+// x <- U^{-1} L^{-1} x.  t: 4 b doubles of scratch.  The chain of
+// diagonal-block products runs on `side`, the bulk of the trailing updates on
+// st, overlapped (side is forked from and joined back to st); ev: 4 events.
+// Needs n % b == 0,
 // b % 32 == 0, lda % 4 == 0 and 16-byte aligned LU / XU / XL.
 bool lu_solve_inv_supported(int n, int b, const float *LU, int64_t lda);
 mxp_status launch_lu_solve_inv(int n, int b, const float *LU, int64_t lda, const float *XU,
-                               const float *XL, int64_t xstride, double *x, double *t, cudaStream_t st);
+                               const float *XL, int64_t xstride, double *x, double *t, cudaStream_t st,
+                               cudaStream_t side, cudaEvent_t *ev);
 
 mxp_status launch_infnorm(int n, const double *x, double *out, cudaStream_t st);
 mxp_status launch_ir_init(int n, const double *rhs, const double *d, double *x, cudaStream_t st);

@@ -589,7 +589,8 @@ bool lu_solve_inv_supported(int n, int b, const float *LU, int64_t lda) {
 }
 
 mxp_status launch_lu_solve_inv(int n, int b, const float *LU, int64_t lda, const float *XU,
-                               const float *XL, int64_t xstride, double *x, double *t, cudaStream_t st) {
+                               const float *XL, int64_t xstride, double *x, double *t, cudaStream_t st,
+                               cudaStream_t side, cudaEvent_t *ev) {
     if (n <= 0) return MXP_OK;
     if (!lu_solve_inv_supported(n, b, LU, lda) || xstride % 4 != 0 ||
         ((reinterpret_cast<uintptr_t>(XU) | reinterpret_cast<uintptr_t>(XL)) & 15u))
@@ -603,40 +604,72 @@ mxp_status launch_lu_solve_inv(int n, int b, const float *LU, int64_t lda, const
         MXP_CUDA(cudaFuncSetAttribute(trsv_inv_kernel<3, kIvRowsDiag>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         MXP_CUDA(cudaFuncSetAttribute(trsv_inv_kernel<4, kIvRowsDiag>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
-    double *t1 = t, *sv = t + b, *t2 = t + 2 * (int64_t)b;  // 3 b doubles
+    double *t1 = t, *sv = t + b, *t2 = t + 2 * (int64_t)b;  // 4 b doubles (t2 double-buffered)
     const unsigned dg = (unsigned)(b / kIvRowsDiag);
     auto upd_grid = [](int rows) { return (unsigned)std::max(1, rows / kIvRowsUpd); };
-    // forward: unit lower L
-    for (int k = 0; k < nb; ++k) {
-        const int64_t kk = (int64_t)k * b;
-        const float *X = XL + k * xstride, *T = LU + kk + kk * lda;
-        double *xk = x + kk;
-        trsv_inv_kernel<1, kIvRowsDiag><<<dg, kIvThreads, smem, st>>>(b, b, X, b, xk, nullptr, 0, nullptr, t1, nullptr);
-        MXP_LAUNCHED();
-        trsv_inv_kernel<3, kIvRowsDiag><<<dg, kIvThreads, smem, st>>>(b, b, T, lda, t1, nullptr, 0, xk, sv, nullptr);
-        MXP_LAUNCHED();
-        trsv_inv_kernel<1, kIvRowsDiag><<<dg, kIvThreads, smem, st>>>(b, b, X, b, sv, nullptr, 0, t1, t2, nullptr);
-        MXP_LAUNCHED();
-        const int rows = (int)(n - kk - b);
-        trsv_inv_kernel<0, kIvRowsUpd><<<upd_grid(rows), kIvThreads, smem, st>>>(
-            rows, b, LU + (kk + b) + kk * lda, lda, t2, nullptr, 0, x + kk + b, x + kk + b, xk);
-        MXP_LAUNCHED();
-    }
-    // backward: upper U
-    for (int k = nb - 1; k >= 0; --k) {
-        const int64_t kk = (int64_t)k * b;
-        const float *X = XU + k * xstride, *T = LU + kk + kk * lda;
-        double *xk = x + kk;
-        trsv_inv_kernel<2, kIvRowsDiag><<<dg, kIvThreads, smem, st>>>(b, b, X, b, xk, T, lda, nullptr, t1, nullptr);
-        MXP_LAUNCHED();
-        trsv_inv_kernel<4, kIvRowsDiag><<<dg, kIvThreads, smem, st>>>(b, b, T, lda, t1, nullptr, 0, xk, sv, nullptr);
-        MXP_LAUNCHED();
-        trsv_inv_kernel<2, kIvRowsDiag><<<dg, kIvThreads, smem, st>>>(b, b, X, b, sv, T, lda, t1, t2, nullptr);
-        MXP_LAUNCHED();
-        const int rows = (int)kk;
-        trsv_inv_kernel<0, kIvRowsUpd><<<upd_grid(rows), kIvThreads, smem, st>>>(
-            rows, b, LU + kk * lda, lda, t2, nullptr, 0, x, x, xk);
-        MXP_LAUNCHED();
+    if (!side || !ev) return fail(MXP_INVALID_ARG, "lu_solve_inv: needs a second stream and four events");
+    {
+        // Two streams.  The chain that bounds the solve -- the three
+        // diagonal-block products of step s and the update of the next
+        // block's rows -- runs on `side` (high priority); the update of all
+        // rows beyond the next block, which only step s+2 needs, runs on `st`
+        // and overlaps the chain of step s+1.  Every row still receives its
+        // updates in step order (the next-block update of step s waits for
+        // the bulk update of step s-1, which covered that block), so the
+        // result is the same, bit for bit, as with every launch on one stream.
+        // ev[0]: fork / join, ev[1]: t2 of the step ready, ev[2 + s % 2]: bulk update of step s done.
+        for (int tri = 0; tri < 2; ++tri) {
+            const bool lower = tri == 0;
+            MXP_CUDA(cudaEventRecord(ev[0], st));
+            MXP_CUDA(cudaStreamWaitEvent(side, ev[0], 0));
+            int bulk_step[2] = {-1, -1};
+            for (int s = 0; s < nb; ++s) {
+                const int k = lower ? s : nb - 1 - s;
+                const int64_t kk = (int64_t)k * b;
+                const float *X = (lower ? XL : XU) + k * xstride, *T = LU + kk + kk * lda;
+                double *xk = x + kk;
+                double *t2s = t2 + (int64_t)(s & 1) * b;
+                if (s >= 2 && bulk_step[s & 1] == s - 2) MXP_CUDA(cudaStreamWaitEvent(side, ev[2 + (s & 1)], 0));
+                if (lower) {
+                    trsv_inv_kernel<1, kIvRowsDiag><<<dg, kIvThreads, smem, side>>>(b, b, X, b, xk, nullptr, 0, nullptr, t1, nullptr);
+                    MXP_LAUNCHED();
+                    trsv_inv_kernel<3, kIvRowsDiag><<<dg, kIvThreads, smem, side>>>(b, b, T, lda, t1, nullptr, 0, xk, sv, nullptr);
+                    MXP_LAUNCHED();
+                    trsv_inv_kernel<1, kIvRowsDiag><<<dg, kIvThreads, smem, side>>>(b, b, X, b, sv, nullptr, 0, t1, t2s, nullptr);
+                    MXP_LAUNCHED();
+                } else {
+                    trsv_inv_kernel<2, kIvRowsDiag><<<dg, kIvThreads, smem, side>>>(b, b, X, b, xk, T, lda, nullptr, t1, nullptr);
+                    MXP_LAUNCHED();
+                    trsv_inv_kernel<4, kIvRowsDiag><<<dg, kIvThreads, smem, side>>>(b, b, T, lda, t1, nullptr, 0, xk, sv, nullptr);
+                    MXP_LAUNCHED();
+                    trsv_inv_kernel<2, kIvRowsDiag><<<dg, kIvThreads, smem, side>>>(b, b, X, b, sv, T, lda, t1, t2s, nullptr);
+                    MXP_LAUNCHED();
+                }
+                MXP_CUDA(cudaEventRecord(ev[1], side));
+                // rows of the next block (and x_k = t2) on the chain, after the bulk update of step s-1
+                if (s >= 1 && bulk_step[(s - 1) & 1] == s - 1)
+                    MXP_CUDA(cudaStreamWaitEvent(side, ev[2 + ((s - 1) & 1)], 0));
+                const bool has_next = s + 1 < nb;
+                const int64_t nx = lower ? kk + b : kk - b;  // first row of the next block
+                trsv_inv_kernel<0, kIvRowsUpd><<<upd_grid(has_next ? b : 0), kIvThreads, smem, side>>>(
+                    has_next ? b : 0, b, LU + (has_next ? nx : 0) + kk * lda, lda, t2s, nullptr, 0,
+                    x + (has_next ? nx : 0), x + (has_next ? nx : 0), xk);
+                MXP_LAUNCHED();
+                // rows beyond the next block
+                const int64_t r0 = lower ? kk + 2 * (int64_t)b : 0;
+                const int rows = (int)(lower ? n - kk - 2 * (int64_t)b : kk - b);
+                if (rows > 0) {
+                    MXP_CUDA(cudaStreamWaitEvent(st, ev[1], 0));
+                    trsv_inv_kernel<0, kIvRowsUpd><<<upd_grid(rows), kIvThreads, smem, st>>>(
+                        rows, b, LU + r0 + kk * lda, lda, t2s, nullptr, 0, x + r0, x + r0, nullptr);
+                    MXP_LAUNCHED();
+                    MXP_CUDA(cudaEventRecord(ev[2 + (s & 1)], st));
+                    bulk_step[s & 1] = s;
+                }
+            }
+            MXP_CUDA(cudaEventRecord(ev[0], side));
+            MXP_CUDA(cudaStreamWaitEvent(st, ev[0], 0));
+        }
     }
     return MXP_OK;
 }
