@@ -603,6 +603,7 @@ mxp_status launch_lu_solve_inv(int n, int b, const float *LU, int64_t lda, const
         MXP_CUDA(cudaFuncSetAttribute(trsv_inv_kernel<2, kIvRowsDiag>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         MXP_CUDA(cudaFuncSetAttribute(trsv_inv_kernel<3, kIvRowsDiag>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         MXP_CUDA(cudaFuncSetAttribute(trsv_inv_kernel<4, kIvRowsDiag>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        MXP_CUDA(cudaFuncSetAttribute(trsv_inv_kernel<0, kIvRowsDiag>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
     double *t1 = t, *sv = t + b, *t2 = t + 2 * (int64_t)b;  // 4 b doubles (t2 double-buffered)
     const unsigned dg = (unsigned)(b / kIvRowsDiag);
@@ -651,7 +652,8 @@ mxp_status launch_lu_solve_inv(int n, int b, const float *LU, int64_t lda, const
                     MXP_CUDA(cudaStreamWaitEvent(side, ev[2 + ((s - 1) & 1)], 0));
                 const bool has_next = s + 1 < nb;
                 const int64_t nx = lower ? kk + b : kk - b;  // first row of the next block
-                trsv_inv_kernel<0, kIvRowsUpd><<<upd_grid(has_next ? b : 0), kIvThreads, smem, side>>>(
+                // (on the chain: small row tiles, many CTAs)
+                trsv_inv_kernel<0, kIvRowsDiag><<<has_next ? dg : 1, kIvThreads, smem, side>>>(
                     has_next ? b : 0, b, LU + (has_next ? nx : 0) + kk * lda, lda, t2s, nullptr, 0,
                     x + (has_next ? nx : 0), x + (has_next ? nx : 0), xk);
                 MXP_LAUNCHED();
