@@ -228,7 +228,7 @@ def workload_config(args):
             "compare": args.compare,
             "diag_rule": "rowsum" if args.diag_rule == 0 else "0.55*rowsum+1",
             "ir": args.ir, "trsm": args.trsm, "compare_trsm": args.compare_trsm,
-            "merge_depth": args.merge_depth if args.merge_depth is not None else 3,
+            "merge_depth": args.merge_depth if args.merge_depth is not None else 4,
             "parallelism": "replicas (one independent system per GPU)",
             "l2": f"inputs larger than L2 (A = {args.n * args.n * 4 / 1e9:.1f} GB per GPU)"}
 
@@ -339,7 +339,7 @@ def _solve_arm(args, form_name, p, dev, dist, local, e2e_on, trsm=None):
 SCHUR_TRAFFIC_RATIO = {"schur_tc_f16_kernel": 2.853 / 2.315, "schur_tc_fp8_kernel": 2.857 / 2.315}
 
 
-def _schur_launch_bytes(n, b, es, kmul, depth=3):
+def _schur_launch_bytes(n, b, es, kmul, depth=4):
     """Average algorithmic bytes of one trailing Schur launch of the merged
     schedule (groups of `depth` panels, K = depth * b)."""
     tot, cnt = 0.0, 0
@@ -372,7 +372,7 @@ def _roofline(args, arm):
         peak, src = bf16, f"{peak_kind} bf16 dense sustained (MEASURED_PEAKS.json)"
         kern = "schur_tc_f16_kernel"
     achieved = sflops / (schur_ms / 1e3) / 1e12 if schur_ms > 0 else None
-    depth = args.merge_depth if args.merge_depth is not None else 3
+    depth = args.merge_depth if args.merge_depth is not None else 4
     alg = _schur_launch_bytes(args.n, args.b, es, kmul, depth)
     return {"bound": "tensor", "kernel": kern, "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
@@ -710,7 +710,7 @@ def parse(argv=None):
                     help="micro: run the launch this long before timing (sustained clocks)")
     ap.add_argument("--trsm-pair", action="store_true", help="TRSM-by-inverse products on the 2-SM kernel")
     ap.add_argument("--merge-depth", type=int, default=None,
-                    help="panels per trailing Schur pass, 1..3 (library default 3)")
+                    help="panels per trailing Schur pass, 1..4 (library default 4)")
     ap.add_argument("--inv-tc", type=int, default=None,
                     help="triangular-inverse doubling levels from this block size on the tensor cores "
                          "(library default 1024; 0: all SIMT FP32)")

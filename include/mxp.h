@@ -104,7 +104,7 @@ typedef enum {
     MXP_OPT_GMRES_RESTART = 2,  /* Arnoldi steps per GMRES correction, 1..30 (default 30) */
     MXP_OPT_GMRES_TOL_EXP = 3,  /* inner tolerance 10^-value on the preconditioned residual (default 10) */
     MXP_OPT_MERGE_PANELS = 4,   /* 1 (default): merged look-ahead, MXP_OPT_MERGE_DEPTH panels per
-                                   trailing pass (3); 0: one panel per step, as the reference */
+                                   trailing pass (4); 0: one panel per step, as the reference */
     MXP_OPT_SCHUR_PAIR = 5,     /* 1: tensor-core products on pairs of SMs (2-SM MMA, 256 x 256
                                    tiles); 0 (default): one SM per 128 x 256 tile */
     MXP_OPT_DIAG_COOP = 6,      /* 1 (default): diagonal-block LU (and the triangular inverses of
@@ -125,10 +125,10 @@ typedef enum {
                                    (hi*hi + hi*lo + lo*hi, near FP32); 1: one BF16 product, K = b
                                    (relative error ~2^-9, the reference's Alt-TRSM idea with BF16's
                                    range in place of FP16's) */
-    MXP_OPT_MERGE_DEPTH = 12,   /* panels per trailing pass, 1..3 (default 3): each panel of a group
+    MXP_OPT_MERGE_DEPTH = 12,   /* panels per trailing pass, 1..4 (default 4): each panel of a group
                                    updates the column and row blocks of the group's later panels,
                                    then one pass with K = depth * b applies the whole group
-                                   (MXP_OPT_MERGE_PANELS 0 / 1 = depth 1 / 3) */
+                                   (MXP_OPT_MERGE_PANELS 0 / 1 = depth 1 / 4) */
     MXP_OPT_INV_TC = 13,        /* triangular inverses of the diagonal block: doubling levels that
                                    join blocks of this size and larger run as tensor-core products
                                    in the TRSM's precision (default 1024; 0: all in the cooperative

@@ -78,7 +78,7 @@ mxp_status launch_sqrt(const double *in, double *out, cudaStream_t st);
 // ---------------------------------------------------------------------------
 // Panel slots of the workspace buffers: at most this many panels per trailing
 // pass (K = kMaxMerge * b).
-constexpr int kMaxMerge = 3;
+constexpr int kMaxMerge = 4;
 
 struct mxp_workspace {
     int n = 0, b = 0, form = 0, device = 0;
@@ -282,7 +282,7 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
             ws->merge = value ? kMaxMerge : 1;
             return MXP_OK;
         case MXP_OPT_MERGE_DEPTH:
-            if (value < 1 || value > kMaxMerge) return fail(MXP_INVALID_ARG, "set_option: merge depth must be 1..3");
+            if (value < 1 || value > kMaxMerge) return fail(MXP_INVALID_ARG, "set_option: merge depth must be 1..4");
             ws->merge = value;
             return MXP_OK;
         case MXP_OPT_SCHUR_PAIR:

@@ -1,6 +1,6 @@
-"""Merged schedule with three panels per trailing pass (MXP_OPT_MERGE_DEPTH = 3):
-each panel of a group updates the column and row blocks of the group's later
-panels, then one pass with K = 3b applies the group.  The factors must match
+"""Merged schedule with D panels per trailing pass (MXP_OPT_MERGE_DEPTH = D, 3
+or 4): each panel of a group updates the column and row blocks of the group's
+later panels, then one pass with K = D b applies the group.  The factors must match
 the oracle's restatement of the reference's one-panel-per-step LU to the same
 bar as the default schedule."""
 import numpy as np
@@ -11,12 +11,13 @@ from tests.gpu_util import to_np_colmajor, rel_fro
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("depth", [3, 4])
 @pytest.mark.parametrize("form", [0, 1, 2])
 @pytest.mark.parametrize("n,b,seed", [(1024, 128, 7), (2048, 256, 11), (1792, 256, 3), (1280, 256, 5),
                                       (2560, 512, 42)])
-def test_depth3_factors(mxp, orc, torch_cuda, form, n, b, seed):
+def test_depth_factors(mxp, orc, torch_cuda, depth, form, n, b, seed):
     p = mxp.panel_matgen(n, seed)
-    ws = mxp.Workspace(n, b, form, merge_depth=3)
+    ws = mxp.Workspace(n, b, form, merge_depth=depth)
     st = mxp.panel_lu(p, b, ws)
     got = to_np_colmajor(p.A, n, n, n)
     A, _, _, _ = orc.matgen(n, seed, 0)
@@ -24,15 +25,15 @@ def test_depth3_factors(mxp, orc, torch_cuda, form, n, b, seed):
     assert rel_fro(got, A) <= 1e-3
     low = np.tril(np.ones((n, n), bool), -1)
     assert rel_fro(got[low], A[low]) <= 1e-3
-    # groups of three: 2 + 2 updates inside and one trailing pass (5 launches);
-    # a last full group has no trailing matrix and no row blocks (2); a tail
-    # of two panels updates one column block (1); a tail of one, nothing
-    q, t = divmod(n // b, 3)
-    want = 5 * q + {0: -3, 1: 0, 2: 1}[t]
+    # groups of D: 2 (D - 1) updates inside and one trailing pass; a last
+    # full group has no trailing matrix and no row blocks (D - 1 launches); a
+    # tail of t < D panels updates t - 1 column blocks
+    q, t = divmod(n // b, depth)
+    want = (2 * depth - 1) * q + (-depth if t == 0 else t - 1)
     assert st["schur_launches"] == want
 
 
-@pytest.mark.parametrize("depth", [1, 2, 3])
+@pytest.mark.parametrize("depth", [1, 2, 3, 4])
 def test_depth_solve_converges(mxp, torch_cuda, depth):
     n, b = 3072, 256
     p = mxp.panel_matgen(n, 13)
@@ -43,6 +44,6 @@ def test_depth_solve_converges(mxp, torch_cuda, depth):
 
 def test_depth_option_bounds(mxp, torch_cuda):
     ws = mxp.Workspace(512, 128, 0)
-    for bad in (0, 4):
+    for bad in (0, 5):
         with pytest.raises(mxp.MxpError):
             ws.set_option(mxp.OPT_MERGE_DEPTH, bad)
