@@ -260,6 +260,8 @@ def _solve_arm(args, form_name, p, dev, dist, local, e2e_on, trsm=None):
         ws.set_option(mxp.OPT_OVERLAP_MIN, args.overlap_min)
     if args.trsv_inv is not None:
         ws.set_option(mxp.OPT_TRSV_INV, args.trsv_inv)
+    if args.fp8_fused_cast is not None:
+        ws.set_option(mxp.OPT_FP8_FUSED_CAST, args.fp8_fused_cast)
     method = mxp.IR_GMRES if args.ir == "gmres" else mxp.IR_CLASSIC
     x = torch.empty(n, dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream()
@@ -714,6 +716,9 @@ def parse(argv=None):
     ap.add_argument("--inv-tc", type=int, default=None,
                     help="triangular-inverse doubling levels from this block size on the tensor cores "
                          "(library default 1024; 0: all SIMT FP32)")
+    ap.add_argument("--fp8-fused-cast", type=int, default=None,
+                    help="1 (library default): the FP8 form's L panels are quantized in the TRSM product's "
+                         "epilogue; 0: by a separate cast launch")
     ap.add_argument("--trsv-inv", type=int, default=None,
                     help="1 (library default): refinement solves with the stored inverses of the "
                          "diagonal blocks; 0: the chain of 64-row blocks")

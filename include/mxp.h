@@ -133,7 +133,7 @@ typedef enum {
                                    join blocks of this size and larger run as tensor-core products
                                    in the TRSM's precision (default 1024; 0: all in the cooperative
                                    kernel, SIMT FP32) */
-    MXP_OPT_TRSV_INV = 14       /* 1 (default): mxp_panel_lu keeps the FP32 inverses of every
+    MXP_OPT_TRSV_INV = 14,      /* 1 (default): mxp_panel_lu keeps the FP32 inverses of every
                                    diagonal block (2 * n * b floats of the workspace) and the
                                    refinement's triangular solves of that factor run as nb steps
                                    of bandwidth-bound products with them (each diagonal block:
@@ -141,6 +141,11 @@ typedef enum {
                                    the factor block, in FP64); 0: the chain of 64-row blocks,
                                    each inverting its diagonal block in FP64.  Setting the
                                    option forgets the stored inverses. */
+    MXP_OPT_FP8_FUSED_CAST = 15, /* FP8 form, tensor-core TRSM, b % 256 == 0: 1 (default) the
+                                   TRSM product that forms the L panel also writes its E4M3 copy
+                                   and per-tile scales (the same bytes as the FP8 panel cast of
+                                   the stored FP32 panel, without reading it back); 0: a separate
+                                   cast launch */
 } mxp_option;
 mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int value);
 mxp_status mxp_workspace_destroy(mxp_workspace *ws);

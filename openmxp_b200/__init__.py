@@ -165,6 +165,7 @@ OPT_TRSM_SINGLE = 11
 OPT_MERGE_DEPTH = 12
 OPT_INV_TC = 13
 OPT_TRSV_INV = 14
+OPT_FP8_FUSED_CAST = 15
 
 
 class Workspace:

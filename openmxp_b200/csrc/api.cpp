@@ -109,6 +109,7 @@ struct mxp_workspace {
     // tensor-core panel TRSM: FP32 triangular inverses and split-BF16 operands
     int trsm_tc = 1;
     int trsm_single = 0;     // one BF16 product instead of three split products
+    int fp8_fused = 1;       // FP8 form: the L panel's E4M3 copy written by the TRSM product's epilogue
     int inv_tc = 1024;       // inverse doubling levels from this block size on the tensor cores (0: none)
     int64_t ldk3 = 0;
     float *tinv_u = nullptr, *tinv_l = nullptr, *tinv_tmp = nullptr;
@@ -309,6 +310,9 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
             if (value != 0 && (value < 128 || (value & (value - 1)) != 0))
                 return fail(MXP_INVALID_ARG, "set_option: inverse level must be 0 or a power of two >= 128");
             ws->inv_tc = value;
+            return MXP_OK;
+        case MXP_OPT_FP8_FUSED_CAST:
+            ws->fp8_fused = value ? 1 : 0;
             return MXP_OK;
         case MXP_OPT_TRSV_INV:
             ws->trsv_inv = value ? 1 : 0;
@@ -589,6 +593,7 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
         float *Akk = d_A + kk + kk * lda;
         const int m = n - (int)kk - b;
         const bool coop_inv = ws->coop && ws->trsm_tc && m > 0;
+        const bool fuse_l = fp8 && ws->trsm_tc && ws->fp8_fused && !ws->trsm_pair && b % 256 == 0 && m > 0;
         mxp_status q = MXP_OK;
         if (!diag_done) {
             pt.mark(PH_DIAG);
@@ -613,9 +618,16 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
             if (q == MXP_OK) q = launch_cast_left(bf, m, b, Lcol, lda, ws->split_big, ws->ldk3, nullptr, st);
             if (q == MXP_OK) q = launch_cast_right(bf, b, b, inv_u(kk), b, ws->split_u, ws->ldk3, nullptr, st);
             pt.mark(PH_TGEMM);
+            // FP8 form: the product's epilogue also writes the E4M3 L panel and
+            // its scales into the panel slot (the separate cast below is skipped)
+            F8Out f8{nullptr, 0, nullptr, 0};
+            if (fuse_l)
+                f8 = F8Out{Lb + (row0 * ldk + slot * kp) * es, ldk,
+                           Ls + (row0 / 128) * scl + slot * (int64_t)cdiv(b, 128), scl};
             if (q == MXP_OK)
                 q = launch_schur(bf, m, b, b, ws->split_big, ws->ldk3, nullptr, ws->split_u, ws->ldk3,
-                                 nullptr, Lcol, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/1, ws->trsm_pair);
+                                 nullptr, Lcol, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/1, ws->trsm_pair,
+                                 nullptr, fuse_l ? &f8 : nullptr);
             pt.mark(PH_CAST);
             if (q == MXP_OK) q = launch_cast_left(bf, b, b, inv_l(kk), b, ws->split_l, ws->ldk3, nullptr, st);
             if (q == MXP_OK) q = launch_cast_right(bf, m, b, Urow, lda, ws->split_big, ws->ldk3, nullptr, st);
@@ -631,8 +643,9 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
         pt.mark(PH_CAST);
         const int64_t koff = slot * kp;
         const int64_t soff = slot * (int64_t)cdiv(b, 128);
-        q = launch_cast_left(form, m, b, Lcol, lda, Lb + (row0 * ldk + koff) * es, ldk,
-                             fp8 ? Ls + (row0 / 128) * scl + soff : nullptr, st, scl);
+        if (!fuse_l)
+            q = launch_cast_left(form, m, b, Lcol, lda, Lb + (row0 * ldk + koff) * es, ldk,
+                                 fp8 ? Ls + (row0 / 128) * scl + soff : nullptr, st, scl);
         if (q == MXP_OK)
             q = launch_cast_right(form, m, b, Urow, lda, Rb + (row0 * ldk + koff) * es, ldk,
                                   fp8 ? Rs + (row0 / 128) * scl + soff : nullptr, st, scl);

@@ -24,6 +24,8 @@
 #include <cuda_fp16.h>
 #include <cuda_fp8.h>
 
+#include "fp8_quant.cuh"
+
 #include "mxp_internal.cuh"
 
 namespace mxp {
@@ -171,21 +173,7 @@ cast_right_kernel(int m, int b, const float *__restrict__ A, int64_t lda, void *
 
 // ---- FP8 E4M3 with per-128x128-tile power-of-two scales -----------------
 
-// Largest e with amax * 2^e <= 448, clamped to [-126, 126]; 0 for a zero or
-// non-finite amax.  Mirrors orc_e4m3_scale_exp of the oracle bit for bit.
-__device__ __forceinline__ int e4m3_scale_exp(float amax) {
-    if (!(amax > 0.0f) || !(amax < 3.0e38f)) return 0;
-    int ea = (int)((__float_as_uint(amax) >> 23) & 0xffu) - 127;
-    if (ea < -126) ea = -126;
-    int e = 8 - ea;
-    if ((double)amax * exp2((double)e) > 448.0) e -= 1;
-    e = max(-126, min(126, e));
-    return e;
-}
-
-__device__ __forceinline__ uint8_t to_e4m3(float x) {
-    return (uint8_t)__nv_cvt_float_to_fp8(x, __NV_SATFINITE, __NV_E4M3);
-}
+// e4m3_scale_exp, e4m3_scale_up and to_e4m3: fp8_quant.cuh
 
 __device__ __forceinline__ float block_max_256(float v, float *red) {
 #pragma unroll
@@ -220,7 +208,7 @@ cast_left_fp8_kernel(int m, int b, const float *__restrict__ A, int64_t lda, uin
     }
     amax = block_max_256(amax, red);
     const int e = e4m3_scale_exp(amax);
-    const float up = __int_as_float((e + 127) << 23);
+    const float up = e4m3_scale_up(e);
 #pragma unroll
     for (int q = 0; q < 64; q += 4) {
         uint32_t w = 0;
@@ -288,7 +276,7 @@ cast_right_fp8_kernel(int m, int b, const float *__restrict__ A, int64_t lda, ui
     }
     amax = block_max_256(amax, red);
     const int e = e4m3_scale_exp(amax);
-    const float up = __int_as_float((e + 127) << 23);
+    const float up = e4m3_scale_up(e);
     if (threadIdx.x == 0) scales[(int64_t)blockIdx.x * sc_ld + blockIdx.y] = (uint8_t)(127 - e);
 #pragma unroll
     for (int c = 0; c < 16; ++c) {

@@ -178,11 +178,22 @@ struct SchurSched {
     int skip_rows = 0, skip_cols = 0;
 };
 
+// Optional FP8 copy of a store-mode product (FP16/BF16 operands, single-SM
+// kernel, n % 256 == 0): out[i * ldk + j] = E4M3(C(i, j) * 2^e) with one
+// scale per 128 x 128 block of C, byte 127 - e at sc[(i / 128) * sc_ld + j / 128],
+// exactly as the FP8 panel cast of C would write them.
+struct F8Out {
+    uint8_t *out;
+    int64_t ldk;
+    uint8_t *sc;
+    int sc_ld;
+};
+
 mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ldl,
                         const uint8_t *lsc, const void *R, int64_t ldr, const uint8_t *rsc,
                         float *C, int64_t ldc, DevStatus *dst, cudaStream_t st, int store = 0,
                         int lsc_ld = 0, int rsc_ld = 0, int tri_mode = 0, int pair = 0,
-                        const SchurSched *sched = nullptr);
+                        const SchurSched *sched = nullptr, const F8Out *f8out = nullptr);
 
 mxp_status launch_otf_gemv(int n, uint64_t seed, const double *d, double alpha, const double *x,
                            double beta, double *y, double *partials, int max_splits,

@@ -29,6 +29,7 @@
 
 #include <mutex>
 
+#include "fp8_quant.cuh"
 #include "mxp_internal.cuh"
 #include "tc_ptx.cuh"
 
@@ -151,10 +152,11 @@ __device__ __forceinline__ void ring_init(const TileRing &r) {
     }
 }
 
+template <bool F8>
 __global__ void __launch_bounds__(kThreads, 1)
 schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                     int M, int N, int K, float *__restrict__ C, int64_t ldc, uint32_t idesc,
-                    TileMap tiles, TileSrc src, int store, int tri_mode, int seg, DevStatus *dst) {
+                    TileMap tiles, TileSrc src, int store, int tri_mode, int seg, F8Out f8, DevStatus *dst) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                 ~uintptr_t(1023));
@@ -169,6 +171,11 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                         reinterpret_cast<volatile int *>(bars + 2 * kStages + 4 + 2 * kRing)};
     uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(bars + 2 * kStages + 4 + 2 * kRing) + kRing;
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_holder + 1);
+    // FP8 copy of the output (store mode): per column half, the four epilogue
+    // warps meet at amax_bar (count 4) to combine their 32-row amax partials
+    // (double-buffered by tile parity)
+    uint64_t *amax_bar = bars + 40;                                    // [2]
+    float *amax_part = reinterpret_cast<float *>(bars + 42);           // [2 parity][2 half][4 quarter]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total_tiles = tiles.tiles_m * tiles.tiles_n;
@@ -192,6 +199,8 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             mbar_init(smem_u32(&tempty[a]), kEpiWarps);
         }
         ring_init(ring);
+        mbar_init(smem_u32(&amax_bar[0]), 4);
+        mbar_init(smem_u32(&amax_bar[1]), 4);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -328,6 +337,8 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             tc_fence_after();
             const int64_t row = (int64_t)tm * kBM + quarter * 32 + lane;
             const bool row_ok = row < M;
+            const float sg = store == 2 ? -1.0f : 1.0f;
+            float rmax = 0.0f;  // |C| over this thread's 128 columns (FP8 copy)
 #pragma unroll 1
             for (int c0 = col_half * 128; c0 < col_half * 128 + 128; c0 += 32) {
                 uint32_t r[32];
@@ -338,10 +349,13 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                     float cv[32];
                     const int ncol = (int)imin64(32, (int64_t)N - col0);
                     if (store) {  // C = acc (panel solves), or C = -acc (store == 2)
-                        const float sg = store == 2 ? -1.0f : 1.0f;
 #pragma unroll
                         for (int j = 0; j < 32; ++j)
                             if (j < ncol) __stcs(cp + j * ldc, sg * __uint_as_float(r[j]));
+                        if (F8) {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) rmax = fmaxf(rmax, fabsf(sg * __uint_as_float(r[j])));
+                        }
                     } else if (ncol >= 32) {
 #pragma unroll
                         for (int j = 0; j < 32; ++j) cv[j] = __ldcs(cp + j * ldc);
@@ -353,6 +367,48 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                             if (j < ncol) cp[j * ldc] = cp[j * ldc] - __uint_as_float(r[j]);
                     }
                 }
+            }
+            if (F8) {
+                // E4M3 copy of this 128 x 128 block of C with one power-of-two
+                // scale from its amax, as cast_left_fp8_kernel makes from C in
+                // memory (same values, same rounding, same bytes)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+                const uint32_t par = it & 1u;
+                float *part = amax_part + (par * 2 + col_half) * 4;
+                if (lane == 0) {
+                    part[quarter] = rmax;
+                    mbar_arrive(smem_u32(&amax_bar[col_half]));
+                }
+                const bool met = mbar_wait(smem_u32(&amax_bar[col_half]), par, abort_flag);
+                if (!__all_sync(0xffffffffu, met)) {
+                    ok = false;
+                    break;
+                }
+                const float amax = fmaxf(fmaxf(part[0], part[1]), fmaxf(part[2], part[3]));
+                const int e = e4m3_scale_exp(amax);
+                const float up = e4m3_scale_up(e);
+#pragma unroll 1
+                for (int c0 = col_half * 128; c0 < col_half * 128 + 128; c0 += 32) {
+                    uint32_t r[32];
+                    tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quarter * 32) << 16) + acc * kBN + c0, r);
+                    if (row_ok) {
+                        uint32_t w[8];
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            uint32_t v = 0u;
+#pragma unroll
+                            for (int b4 = 0; b4 < 4; ++b4)
+                                v |= (uint32_t)to_e4m3(__fmul_rn(sg * __uint_as_float(r[4 * q + b4]), up)) << (8 * b4);
+                            w[q] = v;
+                        }
+                        uint4 *dp = reinterpret_cast<uint4 *>(f8.out + row * f8.ldk + (int64_t)tn * kBN + c0);
+                        dp[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                        dp[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                    }
+                }
+                if (lane == 0 && quarter == 0)
+                    f8.sc[(int64_t)tm * f8.sc_ld + 2 * tn + col_half] = (uint8_t)(127 - e);
             }
             tc_fence_before();
             __syncwarp();
@@ -770,8 +826,10 @@ mxp_status launch_schur2(int form, int m, int n, int k, const void *L, int64_t l
 mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ldl,
                         const uint8_t *lsc, const void *R, int64_t ldr, const uint8_t *rsc,
                         float *C, int64_t ldc, DevStatus *dst, cudaStream_t st, int store,
-                        int lsc_ld, int rsc_ld, int tri_mode, int pair, const SchurSched *sched) {
+                        int lsc_ld, int rsc_ld, int tri_mode, int pair, const SchurSched *sched,
+                        const F8Out *f8out) {
     if (pair) {
+        if (f8out && f8out->out) return fail(MXP_UNSUPPORTED, "schur: the FP8 copy is single-SM only");
         if (sched) return fail(MXP_UNSUPPORTED, "schur: tile schedules are single-SM only");
         return launch_schur2(form, m, n, k, L, ldl, lsc, R, ldr, rsc, C, ldc, dst, st, store, lsc_ld,
                              rsc_ld, tri_mode);
@@ -832,15 +890,28 @@ mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ld
     if (s != MXP_OK) return s;
     static bool attr_done = false;
     if (!attr_done) {
-        MXP_CUDA(cudaFuncSetAttribute(schur_tc_f16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        MXP_CUDA(cudaFuncSetAttribute(schur_tc_f16_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      kSmemBytes));
+        MXP_CUDA(cudaFuncSetAttribute(schur_tc_f16_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       kSmemBytes));
         attr_done = true;
     }
     const uint32_t idesc = idesc_f16(form == MXP_FORM_FP16 ? 0u : 1u);
     // the triangular skip needs whole stages inside one K segment
     if (tri_mode != 0 && (k % 64 != 0)) tri_mode = 0;
-    schur_tc_f16_kernel<<<grid, kThreads, kSmemBytes, st>>>(mapA, mapB, m, n, (int)K, C, ldc, idesc,
-                                                            tiles, src, store, tri_mode, k, dst);
+    F8Out f8{nullptr, 0, nullptr, 0};
+    if (f8out && f8out->out) {
+        if (!store || n % kBN != 0 || f8out->ldk % 16 != 0 || !f8out->sc ||
+            (reinterpret_cast<uintptr_t>(f8out->out) & 15u))
+            return fail(MXP_INVALID_ARG, "schur: FP8 copy needs store mode, n % 256 == 0 and 16-byte rows");
+        f8 = *f8out;
+    }
+    if (f8.out)
+        schur_tc_f16_kernel<true><<<grid, kThreads, kSmemBytes, st>>>(mapA, mapB, m, n, (int)K, C, ldc, idesc,
+                                                                      tiles, src, store, tri_mode, k, f8, dst);
+    else
+        schur_tc_f16_kernel<false><<<grid, kThreads, kSmemBytes, st>>>(mapA, mapB, m, n, (int)K, C, ldc, idesc,
+                                                                       tiles, src, store, tri_mode, k, f8, dst);
     MXP_LAUNCHED();
     return MXP_OK;
 }
