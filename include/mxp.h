@@ -142,10 +142,10 @@ typedef enum {
                                    each inverting its diagonal block in FP64.  Setting the
                                    option forgets the stored inverses. */
     MXP_OPT_FP8_FUSED_CAST = 15, /* FP8 form, tensor-core TRSM, b % 256 == 0: 1 (default) the
-                                   TRSM product that forms the L panel also writes its E4M3 copy
-                                   and per-tile scales (the same bytes as the FP8 panel cast of
-                                   the stored FP32 panel, without reading it back); 0: a separate
-                                   cast launch */
+                                   TRSM products that form the L and U panels also write their
+                                   E4M3 copies and per-tile scales (the same bytes as the FP8 panel
+                                   casts of the stored FP32 panels, without reading them back);
+                                   0: separate cast launches */
 } mxp_option;
 mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int value);
 mxp_status mxp_workspace_destroy(mxp_workspace *ws);

@@ -593,7 +593,7 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
         float *Akk = d_A + kk + kk * lda;
         const int m = n - (int)kk - b;
         const bool coop_inv = ws->coop && ws->trsm_tc && m > 0;
-        const bool fuse_l = fp8 && ws->trsm_tc && ws->fp8_fused && !ws->trsm_pair && b % 256 == 0 && m > 0;
+        const bool fuse_f8 = fp8 && ws->trsm_tc && ws->fp8_fused && !ws->trsm_pair && b % 256 == 0 && m > 0;
         mxp_status q = MXP_OK;
         if (!diag_done) {
             pt.mark(PH_DIAG);
@@ -619,22 +619,28 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
             if (q == MXP_OK) q = launch_cast_right(bf, b, b, inv_u(kk), b, ws->split_u, ws->ldk3, nullptr, st);
             pt.mark(PH_TGEMM);
             // FP8 form: the product's epilogue also writes the E4M3 L panel and
-            // its scales into the panel slot (the separate cast below is skipped)
-            F8Out f8{nullptr, 0, nullptr, 0};
-            if (fuse_l)
+            // its scales into the panel slot (the separate casts below are skipped)
+            F8Out f8{nullptr, 0, nullptr, 0, 0};
+            if (fuse_f8)
                 f8 = F8Out{Lb + (row0 * ldk + slot * kp) * es, ldk,
-                           Ls + (row0 / 128) * scl + slot * (int64_t)cdiv(b, 128), scl};
+                           Ls + (row0 / 128) * scl + slot * (int64_t)cdiv(b, 128), scl, 0};
             if (q == MXP_OK)
                 q = launch_schur(bf, m, b, b, ws->split_big, ws->ldk3, nullptr, ws->split_u, ws->ldk3,
                                  nullptr, Lcol, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/1, ws->trsm_pair,
-                                 nullptr, fuse_l ? &f8 : nullptr);
+                                 nullptr, fuse_f8 ? &f8 : nullptr);
             pt.mark(PH_CAST);
             if (q == MXP_OK) q = launch_cast_left(bf, b, b, inv_l(kk), b, ws->split_l, ws->ldk3, nullptr, st);
             if (q == MXP_OK) q = launch_cast_right(bf, m, b, Urow, lda, ws->split_big, ws->ldk3, nullptr, st);
             pt.mark(PH_TGEMM);
+            // ... and the one that forms U12 the E4M3 R panel (transposed layout)
+            F8Out f8u{nullptr, 0, nullptr, 0, 0};
+            if (fuse_f8)
+                f8u = F8Out{Rb + (row0 * ldk + slot * kp) * es, ldk,
+                            Rs + (row0 / 128) * scl + slot * (int64_t)cdiv(b, 128), scl, 1};
             if (q == MXP_OK)
                 q = launch_schur(bf, b, m, b, ws->split_l, ws->ldk3, nullptr, ws->split_big, ws->ldk3,
-                                 nullptr, Urow, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/2, ws->trsm_pair);
+                                 nullptr, Urow, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/2, ws->trsm_pair,
+                                 nullptr, fuse_f8 ? &f8u : nullptr);
         } else {
             q = launch_trsm_runn(m, b, Akk, lda, Lcol, lda, st);
             if (q == MXP_OK) q = launch_trsm_llnu(b, m, Akk, lda, Urow, lda, st);
@@ -643,10 +649,10 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
         pt.mark(PH_CAST);
         const int64_t koff = slot * kp;
         const int64_t soff = slot * (int64_t)cdiv(b, 128);
-        if (!fuse_l)
+        if (!fuse_f8)
             q = launch_cast_left(form, m, b, Lcol, lda, Lb + (row0 * ldk + koff) * es, ldk,
                                  fp8 ? Ls + (row0 / 128) * scl + soff : nullptr, st, scl);
-        if (q == MXP_OK)
+        if (q == MXP_OK && !fuse_f8)
             q = launch_cast_right(form, m, b, Urow, lda, Rb + (row0 * ldk + koff) * es, ldk,
                                   fp8 ? Rs + (row0 / 128) * scl + soff : nullptr, st, scl);
         return q;

@@ -179,14 +179,17 @@ struct SchurSched {
 };
 
 // Optional FP8 copy of a store-mode product (FP16/BF16 operands, single-SM
-// kernel, n % 256 == 0): out[i * ldk + j] = E4M3(C(i, j) * 2^e) with one
-// scale per 128 x 128 block of C, byte 127 - e at sc[(i / 128) * sc_ld + j / 128],
-// exactly as the FP8 panel cast of C would write them.
+// kernel, n % 256 == 0), with one power-of-two scale per 128 x 128 block of C,
+// exactly as the FP8 panel casts of C would write them.  trans == 0 (L panel
+// layout): out[i * ldk + j] = E4M3(C(i, j) * 2^e), byte 127 - e at
+// sc[(i / 128) * sc_ld + j / 128]; trans == 1 (R panel layout, C holds U
+// columns): out[j * ldk + i], scale at sc[(j / 128) * sc_ld + i / 128].
 struct F8Out {
     uint8_t *out;
     int64_t ldk;
     uint8_t *sc;
     int sc_ld;
+    int trans;
 };
 
 mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ldl,

@@ -392,7 +392,15 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                 for (int c0 = col_half * 128; c0 < col_half * 128 + 128; c0 += 32) {
                     uint32_t r[32];
                     tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quarter * 32) << 16) + acc * kBN + c0, r);
-                    if (row_ok) {
+                    if (row_ok && f8.trans) {
+                        // R layout: row j of the panel holds its k contiguously, so for
+                        // each column j the 32 lanes (32 consecutive k) store one
+                        // 32-byte run
+                        uint8_t *dp = f8.out + ((int64_t)tn * kBN + c0) * f8.ldk + row;
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            dp[j * f8.ldk] = to_e4m3(__fmul_rn(sg * __uint_as_float(r[j]), up));
+                    } else if (row_ok) {
                         uint32_t w[8];
 #pragma unroll
                         for (int q = 0; q < 8; ++q) {
@@ -407,8 +415,10 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                         dp[1] = make_uint4(w[4], w[5], w[6], w[7]);
                     }
                 }
-                if (lane == 0 && quarter == 0)
-                    f8.sc[(int64_t)tm * f8.sc_ld + 2 * tn + col_half] = (uint8_t)(127 - e);
+                if (lane == 0 && quarter == 0) {
+                    if (f8.trans) f8.sc[(int64_t)(2 * tn + col_half) * f8.sc_ld + tm] = (uint8_t)(127 - e);
+                    else f8.sc[(int64_t)tm * f8.sc_ld + 2 * tn + col_half] = (uint8_t)(127 - e);
+                }
             }
             tc_fence_before();
             __syncwarp();
@@ -899,10 +909,10 @@ mxp_status launch_schur(int form, int m, int n, int k, const void *L, int64_t ld
     const uint32_t idesc = idesc_f16(form == MXP_FORM_FP16 ? 0u : 1u);
     // the triangular skip needs whole stages inside one K segment
     if (tri_mode != 0 && (k % 64 != 0)) tri_mode = 0;
-    F8Out f8{nullptr, 0, nullptr, 0};
+    F8Out f8{nullptr, 0, nullptr, 0, 0};
     if (f8out && f8out->out) {
-        if (!store || n % kBN != 0 || f8out->ldk % 16 != 0 || !f8out->sc ||
-            (reinterpret_cast<uintptr_t>(f8out->out) & 15u))
+        if (!store || n % kBN != 0 || !f8out->sc ||
+            (!f8out->trans && (f8out->ldk % 16 != 0 || (reinterpret_cast<uintptr_t>(f8out->out) & 15u))))
             return fail(MXP_INVALID_ARG, "schur: FP8 copy needs store mode, n % 256 == 0 and 16-byte rows");
         f8 = *f8out;
     }

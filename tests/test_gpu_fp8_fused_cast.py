@@ -1,7 +1,7 @@
-"""FP8 form: the TRSM-by-inverse product that forms each L panel also writes
-its E4M3 copy and per-tile scales (MXP_OPT_FP8_FUSED_CAST).  Those bytes must
-be the ones the FP8 panel cast makes from the stored FP32 panel, so the whole
-factorisation is bit-identical with the option on and off."""
+"""FP8 form: the TRSM-by-inverse products that form each L and U panel also
+write their E4M3 copies and per-tile scales (MXP_OPT_FP8_FUSED_CAST).  Those
+bytes must be the ones the FP8 panel casts make from the stored FP32 panels,
+so the whole factorisation is bit-identical with the option on and off."""
 import pytest
 import torch
 
