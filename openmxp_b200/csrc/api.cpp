@@ -95,6 +95,7 @@ struct mxp_workspace {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int *tile_ctr = nullptr;  // shared tile counter of the split trailing pass
+    int *trsm_ctr = nullptr;  // tile counter of the TRSM-by-inverse products (claimed dynamically)
     size_t esize = 2;        // panel element size
     void *lpanel[2] = {nullptr, nullptr};
     void *rpanel[2] = {nullptr, nullptr};
@@ -232,6 +233,7 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
         ok = ok && (ws->coop_tmp = (float *)alloc(2 * diag_factor_tmp_floats(b) * 4));
         ok = ok && (ws->coop_sync = (unsigned int *)alloc(256));
         if (ok) ws->tile_ctr = reinterpret_cast<int *>(ws->coop_sync + 32);
+        if (ok) ws->trsm_ctr = reinterpret_cast<int *>(ws->coop_sync + 33);
         ok = ok && (ws->split_big = alloc((size_t)rows * ws->ldk3 * 2 + 1024));
         ok = ok && (ws->split_u = alloc((size_t)b * ws->ldk3 * 2 + 1024));
         ok = ok && (ws->split_l = alloc((size_t)b * ws->ldk3 * 2 + 1024));
@@ -624,10 +626,19 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
             if (fuse_f8)
                 f8 = F8Out{Lb + (row0 * ldk + slot * kp) * es, ldk,
                            Ls + (row0 / 128) * scl + slot * (int64_t)cdiv(b, 128), scl, 0};
+            // The triangular K-skip makes the tiles' work uneven (1 to b/256 K blocks):
+            // CTAs claim tiles from a counter instead of a static round robin.
+            SchurSched tsched;
+            tsched.counter = ws->trsm_ctr;
+            const SchurSched *ts = ws->trsm_pair ? nullptr : &tsched;
+            if (q == MXP_OK && ts) {
+                cudaError_t e = cudaMemsetAsync(ws->trsm_ctr, 0, sizeof(int), st);
+                if (e != cudaSuccess) q = cuda_fail(e, "panel_lu: TRSM tile counter");
+            }
             if (q == MXP_OK)
                 q = launch_schur(bf, m, b, b, ws->split_big, ws->ldk3, nullptr, ws->split_u, ws->ldk3,
                                  nullptr, Lcol, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/1, ws->trsm_pair,
-                                 nullptr, fuse_f8 ? &f8 : nullptr);
+                                 ts, fuse_f8 ? &f8 : nullptr);
             pt.mark(PH_CAST);
             if (q == MXP_OK) q = launch_cast_left(bf, b, b, inv_l(kk), b, ws->split_l, ws->ldk3, nullptr, st);
             if (q == MXP_OK) q = launch_cast_right(bf, m, b, Urow, lda, ws->split_big, ws->ldk3, nullptr, st);
@@ -637,10 +648,14 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
             if (fuse_f8)
                 f8u = F8Out{Rb + (row0 * ldk + slot * kp) * es, ldk,
                             Rs + (row0 / 128) * scl + slot * (int64_t)cdiv(b, 128), scl, 1};
+            if (q == MXP_OK && ts) {
+                cudaError_t e = cudaMemsetAsync(ws->trsm_ctr, 0, sizeof(int), st);
+                if (e != cudaSuccess) q = cuda_fail(e, "panel_lu: TRSM tile counter");
+            }
             if (q == MXP_OK)
                 q = launch_schur(bf, b, m, b, ws->split_l, ws->ldk3, nullptr, ws->split_big, ws->ldk3,
                                  nullptr, Urow, lda, ws->status, st, /*store=*/1, 0, 0, /*tri=*/2, ws->trsm_pair,
-                                 nullptr, fuse_f8 ? &f8u : nullptr);
+                                 ts, fuse_f8 ? &f8u : nullptr);
         } else {
             q = launch_trsm_runn(m, b, Akk, lda, Lcol, lda, st);
             if (q == MXP_OK) q = launch_trsm_llnu(b, m, Akk, lda, Urow, lda, st);
