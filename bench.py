@@ -163,24 +163,31 @@ class ClockSampler:
 CPU_SAMPLE = {"n": 8192, "b": 256, "seed": 42}
 
 
+def cpu_kind():
+    """"reference" when the reference's CPU kernels were compiled (oracle/_ref),
+    else "port" (the oracle's restatement alone)."""
+    from oracle import oracle as O
+    return "reference" if O.ref_available() else "port"
+
+
 def cpu_solve_once(form_id: int = 0):
     from oracle import oracle as O
     n, b, seed = CPU_SAMPLE["n"], CPU_SAMPLE["b"], CPU_SAMPLE["seed"]
-    rc, x, st = O.solve(n, b, seed, 0, form_id, 50)
+    rc, x, st = O.solve(n, b, seed, 0, form_id, 50, ref_kernels=cpu_kind() == "reference")
     t = st["t_lu"] + st["t_ir"]
     return hpl_flops(n) / t / 1e12, t, st, O.lib().orc_num_threads()
 
 
-def cpu_baseline(samples: int = 1):
-    vals = []
+def cpu_baseline(samples: int = 2):
+    """One untimed solve (threads and pages warm), then the mean rate of
+    `samples` timed solves."""
+    cpu_solve_once()
+    tot_t, cores = 0.0, 1
     for _ in range(samples):
         v, t, st, cores = cpu_solve_once()
-        vals.append(v)
-    return {"value": max(vals), "unit": "TFLOP/s", "cores": cores, "kind": "port",
-            "sample": (f"whole solve (LU + classic IR, generation excluded) at N={CPU_SAMPLE['n']}, "
-                       f"B={CPU_SAMPLE['b']}, seed {CPU_SAMPLE['seed']}, FP16-emulated Schur, on "
-                       f"{cores} OpenMP threads of the oracle (oracle/mxp_oracle.c); the "
-                       f"N=122880 solve would take hours on the host")}
+        tot_t += t
+    return {"value": hpl_flops(CPU_SAMPLE["n"]) * samples / tot_t / 1e12, "unit": "TFLOP/s", "cores": cores,
+            "kind": cpu_kind(), "sample": cpu_baseline_sample_text(cores)}
 
 
 def run_reference(args):
@@ -203,8 +210,8 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f16", "data": "synthetic (HPL-MxP LCG generator)",
-        "config": workload_config(args),
-        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": cores, "kind": "port",
+        "config": cpu_sample_config(),
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": cores, "kind": cpu_kind(),
                          "sample": cpu_baseline_sample_text(cores)},
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -214,9 +221,22 @@ def run_reference(args):
 
 
 def cpu_baseline_sample_text(cores):
-    return (f"CPU restatement of the reference's path (oracle/mxp_oracle.c) solving "
-            f"N={CPU_SAMPLE['n']}, B={CPU_SAMPLE['b']}, seed {CPU_SAMPLE['seed']} per step on "
-            f"{cores} host threads; a bounded stand-in for the N=122880 workload")
+    what = ("the reference's compiled CPU kernels (sgetrf_nopiv_omp<6> for the diagonal blocks, "
+            "otf_gemv_kernel for the residual) with the oracle's restated panel TRSM, FP16-emulated "
+            "Schur update and triangular solves" if cpu_kind() == "reference" else
+            "the oracle's CPU restatement of the reference's path (oracle/mxp_oracle.c)")
+    return (f"whole solve (LU + classic IR, generation excluded) at N={CPU_SAMPLE['n']}, B={CPU_SAMPLE['b']}, "
+            f"seed {CPU_SAMPLE['seed']} per step on {cores} OpenMP threads: {what}; a bounded sample "
+            f"(the N=122880 solve would take hours on the host)")
+
+
+def cpu_sample_config():
+    n, b, seed = CPU_SAMPLE["n"], CPU_SAMPLE["b"], CPU_SAMPLE["seed"]
+    return {"workload": (f"HPL-MxP solve N={n} B={b} seed={seed} on the host cores: FP16-emulated Schur, "
+                         "FP32 panels, FP64 classic IR to scaled residual<16 (the CPU configuration; a "
+                         "bounded sample beside the N=122880 GPU workload)"),
+            "n": n, "b": b, "seed": seed, "form": "fp16", "diag_rule": "rowsum", "ir": "classic",
+            "trsm": "fp32 substitution", "parallelism": "OpenMP threads of one host"}
 
 
 def workload_config(args):
@@ -236,6 +256,9 @@ def workload_config(args):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+TRSM_TEXT = {"tensor": "TRSM by inverse, three split-BF16 products (near FP32)",
+             "single": "TRSM by inverse, one BF16 product",
+             "simt": "FP32 SIMT substitution"}
 def _solve_arm(args, form_name, p, dev, dist, local, e2e_on, trsm=None):
     """Warm up, then time args.steps solves of form `form_name` on problem p."""
     import torch
@@ -335,8 +358,8 @@ def _solve_arm(args, form_name, p, dev, dist, local, e2e_on, trsm=None):
 
 
 # DRAM bytes (read + write) per Schur launch over the algorithmic bytes (C read +
-# write, L and R panels once), from one ncu capture of each kernel at m = n = 16384
-# (profiles/schur_tc_*.md).  The traffic of a launch of the solve is this ratio
+# write, L and R panels once), from one ncu capture of each kernel at
+# m = n = 16384.  The traffic of a launch of the solve is this ratio
 # times its algorithmic bytes: the C read-modify-write dominates both.
 SCHUR_TRAFFIC_RATIO = {"schur_tc_f16_kernel": 2.853 / 2.315, "schur_tc_fp8_kernel": 2.857 / 2.315}
 
@@ -405,6 +428,10 @@ def run_gpu(args):
     plain = None
     if args.compare not in ("none", args.form):
         plain = _solve_arm(args, args.compare, p, dev, dist, local, False, trsm=args.compare_trsm)
+    # the headline form again with the plain form's TRSM: a like-for-like ratio
+    same = None
+    if plain is not None and not args.no_same_trsm and args.trsm != args.compare_trsm:
+        same = _solve_arm(args, args.form, p, dev, dist, local, False, trsm=args.compare_trsm)
     rhs = p.rhs.clone()
     del p
     torch.cuda.empty_cache()
@@ -416,6 +443,8 @@ def run_gpu(args):
         fwd = {arm["form"]: fe.forward_error(arm["x"], x_ref)}
         if plain is not None:
             fwd[plain["form"]] = fe.forward_error(plain["x"], x_ref)
+        if same is not None:
+            fwd[same["form"] + "_" + args.compare_trsm + "_trsm"] = fe.forward_error(same["x"], x_ref)
         del x_ref
         torch.cuda.empty_cache()
 
@@ -443,6 +472,16 @@ def run_gpu(args):
                                                    "ir_ms", "clocks", "gpu_launches", "overlapped_diag")}
             line["plain"]["roofline"] = _roofline(args, plain)
             line["ratio_vs_plain"] = arm["value"] / plain["value"]
+            line["trsm_forms"] = {
+                args.form: TRSM_TEXT[args.trsm], args.compare: TRSM_TEXT[args.compare_trsm],
+                "why": ("the headline form's panels are rounded to E4M3 (2^-4) right after the TRSM, so one "
+                        "BF16 product (2^-9) does not limit its factors; the reference's own production "
+                        "runs use a single low-precision product too (Alt-TRSM, panel_trf_gdirect.hpp:73-107). "
+                        "The plain form keeps FP32-accurate panels as config C3 states")}
+        if same is not None:
+            line["same_trsm"] = {k: same[k] for k in ("form", "value", "ms_per_step", "ir", "phases_ms", "ir_ms")}
+            line["same_trsm"]["trsm"] = TRSM_TEXT[args.compare_trsm]
+            line["ratio_vs_plain_same_trsm"] = same["value"] / plain["value"]
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -703,6 +742,8 @@ def parse(argv=None):
                          "(its panels are E4M3 next), tensor otherwise")
     ap.add_argument("--compare-trsm", choices=["tensor", "single", "simt"], default="tensor",
                     help="panel TRSM of the --compare arm (the plain method: FP32-accurate)")
+    ap.add_argument("--no-same-trsm", action="store_true",
+                    help="skip the third arm: --form again with --compare-trsm (the like-for-like ratio)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -146,10 +146,40 @@ typedef enum {
                                    E4M3 copies and per-tile scales (the same bytes as the FP8 panel
                                    casts of the stored FP32 panels, without reading them back);
                                    0: separate cast launches */
+    MXP_OPT_TRSM_COUNTER = 16,  /* 1-SM TRSM-by-inverse products: 1 (default) CTAs claim output
+                                   tiles from a device counter (the triangular K-skip makes tile
+                                   work uneven); 0: static round robin.  Each tile is computed the
+                                   same way either way, so the factors are bit-identical. */
 } mxp_option;
 mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int value);
 mxp_status mxp_workspace_destroy(mxp_workspace *ws);
 size_t mxp_workspace_bytes(int n, int b, int form);
+
+/* Where the workspace keeps the low-precision L or R panels the Schur update
+ * reads (the device side of LRPanels::operator()(i, 'd') / get_lda(),
+ * panel.hpp:321-359).  The buffer holds MXP_OPT_MERGE_DEPTH panel slots
+ * side by side along K; after mxp_panel_lu the slots hold the last group's
+ * panels: slot s holds panel k0 + s (k0 = first panel of the last group),
+ * its row t (a row of L, or a column of U for R) at buffer row s * b + t,
+ * K-major: element (row r, k) of slot s at
+ *   data + (r * ld + s * slot_k + k) * esize
+ * (BF16X2: three K segments, hi|hi|lo for L and hi|lo|hi for R).  FP8: the
+ * UE8M0 scale of row tile r / 128 and K tile k / 128 of slot s is
+ *   scales[(r / 128) * sc_ld + s * sc_slot + k / 128]
+ * (the scale is 2^-(127 - byte)); other forms: scales == NULL.  Read-only
+ * for callers; valid until the workspace is destroyed. */
+typedef struct {
+    void *data;
+    int64_t ld;       /* row stride, elements */
+    int64_t slot_k;   /* K offset of one slot, elements */
+    int esize;        /* bytes per element: 2 (FP16, BF16X2) or 1 (FP8) */
+    int slots;        /* slots in the buffer */
+    int64_t rows;     /* rows in the buffer */
+    uint8_t *scales;
+    int sc_ld, sc_slot;
+} mxp_panel_view;
+mxp_status mxp_workspace_panel_view(const mxp_workspace *ws, int side /* 0: L, 1: R */,
+                                    mxp_panel_view *out);
 
 /* ---- generation ------------------------------------------------------- */
 

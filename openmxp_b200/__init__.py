@@ -56,6 +56,12 @@ class IrStats(C.Structure):
         return d
 
 
+class PanelView(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("ld", C.c_int64), ("slot_k", C.c_int64), ("esize", C.c_int),
+                ("slots", C.c_int), ("rows", C.c_int64), ("scales", C.c_void_p), ("sc_ld", C.c_int),
+                ("sc_slot", C.c_int)]
+
+
 class BatchResult(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("info", C.c_int), ("pad", C.c_int),
                 ("hpl_harness", C.c_double), ("residual", C.c_double)]
@@ -80,6 +86,7 @@ _SIGS = {
     "mxp_workspace_destroy": (_i32, [_vp]),
     "mxp_workspace_bytes": (C.c_size_t, [_i32, _i32, _i32]),
     "mxp_workspace_set_option": (_i32, [_vp, _i32, _i32]),
+    "mxp_workspace_panel_view": (_i32, [_vp, _i32, C.POINTER(PanelView)]),
     "mxp_matgen": (_i32, [_i32, _u64, _i32, _vp, _i64, _vp, _vp, _vp, _vp]),
     "mxp_matgen_f64": (_i32, [_i32, _u64, _i32, _vp, _i64, _vp]),
     "mxp_getrf_nopiv": (_i32, [_i32, _vp, _i64, _vp, _vp]),
@@ -166,6 +173,7 @@ OPT_MERGE_DEPTH = 12
 OPT_INV_TC = 13
 OPT_TRSV_INV = 14
 OPT_FP8_FUSED_CAST = 15
+OPT_TRSM_COUNTER = 16
 
 
 class Workspace:
@@ -195,6 +203,13 @@ class Workspace:
 
     def set_option(self, key: int, value: int) -> None:
         check(lib().mxp_workspace_set_option(self.handle, key, value))
+
+    def panel_view(self, side: int) -> dict:
+        """Device location of the low-precision L (side 0) or R (side 1) panel
+        slots (mxp_workspace_panel_view)."""
+        v = PanelView()
+        check(lib().mxp_workspace_panel_view(self.handle, side, C.byref(v)))
+        return {k: getattr(v, k) for k, _ in PanelView._fields_}
 
     def close(self):
         if self.handle:

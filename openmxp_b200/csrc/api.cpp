@@ -96,6 +96,7 @@ struct mxp_workspace {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int *tile_ctr = nullptr;  // shared tile counter of the split trailing pass
     int *trsm_ctr = nullptr;  // tile counter of the TRSM-by-inverse products (claimed dynamically)
+    int trsm_counter = 1;     // TRSM products take tiles from trsm_ctr (0: static round robin)
     size_t esize = 2;        // panel element size
     void *lpanel[2] = {nullptr, nullptr};
     void *rpanel[2] = {nullptr, nullptr};
@@ -134,8 +135,22 @@ struct mxp_workspace {
     double gm_tol = 1e-10;
     double *gV = nullptr, *gH = nullptr, *gsmall = nullptr, *gpart = nullptr;
     double *h_scal = nullptr;  // pinned host scalars
+    // timing events, created once: the refinement's six, and a pool the LU
+    // phase marks and the GMRES regions draw from (grown on first use only)
+    cudaEvent_t ev_ir[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    std::vector<cudaEvent_t> ev_pool;
     std::vector<void *> allocs;
 };
+
+// Event i of the workspace's pool (created the first time it is asked for).
+static cudaEvent_t pool_event(mxp_workspace *ws, size_t i) {
+    while (ws->ev_pool.size() <= i) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        ws->ev_pool.push_back(e);
+    }
+    return ws->ev_pool[i];
+}
 
 static int64_t panel_ldk(int b, int form) {
     const int64_t K = form == MXP_FORM_BF16X2 ? 3 * (int64_t)b : b;
@@ -185,6 +200,10 @@ extern "C" mxp_status mxp_workspace_destroy(mxp_workspace *ws) {
     if (ws->ev_fork) cudaEventDestroy(ws->ev_fork);
     if (ws->ev_join) cudaEventDestroy(ws->ev_join);
     for (cudaEvent_t e : ws->ev_trsv)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ws->ev_ir)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ws->ev_pool)
         if (e) cudaEventDestroy(e);
     if (ws->side) cudaStreamDestroy(ws->side);
     cudaSetDevice(cur);
@@ -250,6 +269,7 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
              cudaEventCreateWithFlags(&ws->ev_join, cudaEventDisableTiming) == cudaSuccess;
         for (int e = 0; e < 4 && ok; ++e)
             ok = cudaEventCreateWithFlags(&ws->ev_trsv[e], cudaEventDisableTiming) == cudaSuccess;
+        for (int e = 0; e < 6 && ok; ++e) ok = cudaEventCreate(&ws->ev_ir[e]) == cudaSuccess;
     }
     if (!ok) {
         cudaGetLastError();
@@ -316,6 +336,9 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
         case MXP_OPT_FP8_FUSED_CAST:
             ws->fp8_fused = value ? 1 : 0;
             return MXP_OK;
+        case MXP_OPT_TRSM_COUNTER:
+            ws->trsm_counter = value ? 1 : 0;
+            return MXP_OK;
         case MXP_OPT_TRSV_INV:
             ws->trsv_inv = value ? 1 : 0;
             ws->inv_lu = nullptr;  // setting it forgets the stored inverses
@@ -335,6 +358,22 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
         default:
             return fail(MXP_INVALID_ARG, "set_option: unknown key");
     }
+}
+
+extern "C" mxp_status mxp_workspace_panel_view(const mxp_workspace *ws, int side, mxp_panel_view *out) {
+    if (!ws || !out) return fail(MXP_INVALID_ARG, "panel_view: NULL argument");
+    if (side != 0 && side != 1) return fail(MXP_INVALID_ARG, "panel_view: side must be 0 (L) or 1 (R)");
+    const bool fp8 = ws->form == MXP_FORM_FP8;
+    out->data = side ? ws->rpanel[0] : ws->lpanel[0];
+    out->ld = ws->ldk;
+    out->slot_k = ws->kp;
+    out->esize = (int)ws->esize;
+    out->slots = kMaxMerge;
+    out->rows = ws->n > ws->b ? ws->n - ws->b : 1;
+    out->scales = fp8 ? (side ? ws->rscale[0] : ws->lscale[0]) : nullptr;
+    out->sc_ld = fp8 ? ws->sc_ld : 0;
+    out->sc_slot = fp8 ? (int)cdiv(ws->b, 128) : 0;
+    return MXP_OK;
 }
 
 // Read and clear the device status word; synchronises the stream.
@@ -495,14 +534,18 @@ extern "C" mxp_status mxp_schur_update(int form, int m, int n, int k, const void
 // LU
 // ---------------------------------------------------------------------------
 namespace {
+// Phase marks on the solve stream, from the workspace's event pool (no event
+// is created once the pool has grown to a solve's number of marks); read
+// after the LU's final synchronisation.
 struct PhaseTimer {
     bool on = false;
     cudaStream_t st = 0;
+    mxp_workspace *ws = nullptr;
     std::vector<std::pair<cudaEvent_t, int>> marks;  // event, phase id after it
     void mark(int phase) {
         if (!on) return;
-        cudaEvent_t e;
-        cudaEventCreate(&e);
+        cudaEvent_t e = pool_event(ws, marks.size());
+        if (!e) return;
         cudaEventRecord(e, st);
         marks.push_back({e, phase});
     }
@@ -515,7 +558,6 @@ struct PhaseTimer {
             const int ph = marks[i].second;
             if (ph >= 0 && ph < nphase) ms[ph] += t;
         }
-        for (auto &m : marks) cudaEventDestroy(m.first);
         marks.clear();
     }
 };
@@ -535,6 +577,7 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
     PhaseTimer pt;
     pt.on = stats != nullptr;
     pt.st = st;
+    pt.ws = ws;
     int schur_launches = 0;
     mxp_status s = MXP_OK;
     const int64_t ldk = ws->ldk, kp = ws->kp;
@@ -630,7 +673,7 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
             // CTAs claim tiles from a counter instead of a static round robin.
             SchurSched tsched;
             tsched.counter = ws->trsm_ctr;
-            const SchurSched *ts = ws->trsm_pair ? nullptr : &tsched;
+            const SchurSched *ts = ws->trsm_pair || !ws->trsm_counter ? nullptr : &tsched;
             if (q == MXP_OK && ts) {
                 cudaError_t e = cudaMemsetAsync(ws->trsm_ctr, 0, sizeof(int), st);
                 if (e != cudaSuccess) q = cuda_fail(e, "panel_lu: TRSM tile counter");
@@ -842,18 +885,29 @@ static mxp_status gmres_correction(int n, uint64_t seed, const float *LU, int64_
     double *w = ws->w;
     double *h = ws->h_scal + 8;
     mxp_status s;
-    cudaEvent_t a, b;
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
+    // Timed regions bracket pool events; their times are read at the stream
+    // synchronisations the Arnoldi loop makes anyway (no wait of their own).
+    std::vector<std::pair<size_t, double *>> pending;
+    size_t next_ev = 0;
     auto timed = [&](double *acc, auto &&fn) -> mxp_status {
-        cudaEventRecord(a, st);
+        cudaEvent_t a = pool_event(ws, next_ev), b = pool_event(ws, next_ev + 1);
+        if (a && b) cudaEventRecord(a, st);
         mxp_status q = fn();
-        cudaEventRecord(b, st);
-        cudaEventSynchronize(b);
-        float t = 0.f;
-        cudaEventElapsedTime(&t, a, b);
-        *acc += t;
+        if (a && b) {
+            cudaEventRecord(b, st);
+            pending.push_back({next_ev, acc});
+            next_ev += 2;
+        }
         return q;
+    };
+    auto settle = [&]() {  // after a synchronisation of st
+        for (auto &pr : pending) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ws->ev_pool[pr.first], ws->ev_pool[pr.first + 1]);
+            *pr.second += t;
+        }
+        pending.clear();
+        next_ev = 0;
     };
     // z = M^{-1} r -> V_0 after normalisation
     s = launch_copy(n, r, V, st);
@@ -866,6 +920,7 @@ static mxp_status gmres_correction(int n, uint64_t seed, const float *LU, int64_
     {
         MXP_CUDA(cudaMemcpyAsync(h, sc + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
         MXP_CUDA(cudaStreamSynchronize(st));
+        settle();
         const double beta = h[0];
         int k = 0;
         if (!(beta > 0.0) || !std::isfinite(beta)) {
@@ -889,6 +944,7 @@ static mxp_status gmres_correction(int n, uint64_t seed, const float *LU, int64_
             if (s != MXP_OK) goto out;
             MXP_CUDA(cudaMemcpyAsync(h + 1, sc + 3, sizeof(double), cudaMemcpyDeviceToHost, st));
             MXP_CUDA(cudaStreamSynchronize(st));
+            settle();
             k = j + 1;
             if (!(h[1] > ws->gm_tol * beta)) break;
         }
@@ -901,8 +957,6 @@ static mxp_status gmres_correction(int n, uint64_t seed, const float *LU, int64_
         if (s == MXP_OK) s = launch_vadd(n, k, V, n, y, r, st);
     }
 out:
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
     return s;
 }
 
@@ -919,38 +973,25 @@ extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float
     double *r = ws->r;
     double *sc = ws->scal;  // [0] normx [1] normr [2] norma [3] normb
     double *h = ws->h_scal;
-    cudaEvent_t e0, e1, g0, g1, t0, t1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventCreate(&g0);
-    cudaEventCreate(&g1);
-    cudaEventCreate(&t0);
-    cudaEventCreate(&t1);
+    cudaEvent_t e0 = ws->ev_ir[0], e1 = ws->ev_ir[1], g0 = ws->ev_ir[2], g1 = ws->ev_ir[3], t0 = ws->ev_ir[4],
+                t1 = ws->ev_ir[5];
     double ms_gemv = 0.0, ms_trsv = 0.0;
+    bool trsv_pending = false;  // t0..t1 recorded, read at the next synchronisation
     mxp_status s = MXP_OK;
-    auto done = [&](mxp_status res) {
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        cudaEventDestroy(g0);
-        cudaEventDestroy(g1);
-        cudaEventDestroy(t0);
-        cudaEventDestroy(t1);
-        return res;
-    };
     cudaEventRecord(e0, st);
     MXP_CUDA(cudaMemsetAsync(ws->status, 0, sizeof(DevStatus), st));
     if (norma <= 0.0) {
         s = launch_norma(n, d_d, d_rowsum, sc + 2, st);
-        if (s != MXP_OK) return done(s);
+        if (s != MXP_OK) return s;
     }
     s = launch_infnorm(n, d_rhs, sc + 3, st);
-    if (s != MXP_OK) return done(s);
+    if (s != MXP_OK) return s;
     MXP_CUDA(cudaMemcpyAsync(h + 2, sc + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
     MXP_CUDA(cudaStreamSynchronize(st));
     if (norma <= 0.0) norma = h[2];
     const double normb = h[3];
     s = launch_ir_init(n, d_rhs, d_d, d_x, st);
-    if (s != MXP_OK) return done(s);
+    if (s != MXP_OK) return s;
     const double eps = 0x1p-53;  // DBL_EPSILON / 2
     int it = 0;
     bool converged = false;
@@ -963,11 +1004,13 @@ extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float
         if (s == MXP_OK) s = launch_otf_gemv(n, seed, d_d, -1.0, d_x, 1.0, r, ws->partials, ws->max_splits, st);
         cudaEventRecord(g1, st);
         if (s == MXP_OK) s = launch_infnorm(n, r, sc + 1, st);
-        if (s != MXP_OK) return done(s);
+        if (s != MXP_OK) return s;
         ++gemv_calls;
         MXP_CUDA(cudaMemcpyAsync(h, sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
         MXP_CUDA(cudaStreamSynchronize(st));
         ms_gemv += elapsed(g0, g1);
+        if (trsv_pending) ms_trsv += elapsed(t0, t1);
+        trsv_pending = false;
         normx = h[0];
         normr = h[1];
         hpl = normr / (norma * normx + normb) * 1.0 / ((double)n * eps);
@@ -992,20 +1035,20 @@ extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float
             gemv_calls += inner - before;
             trsv_calls += inner - before + 1;
             if (s == MXP_OK) s = launch_axpy(n, 1.0, r, d_x, st);
-            if (s != MXP_OK) return done(s);
+            if (s != MXP_OK) return s;
         } else {
             cudaEventRecord(t0, st);
             s = lu_solve_ws(ws, n, d_LU, lda, r, st);
             cudaEventRecord(t1, st);
             if (s == MXP_OK) s = launch_axpy(n, 1.0, r, d_x, st);
-            if (s != MXP_OK) return done(s);
+            if (s != MXP_OK) return s;
             ++trsv_calls;
-            MXP_CUDA(cudaStreamSynchronize(st));
-            ms_trsv += elapsed(t0, t1);
+            trsv_pending = true;
         }
     }
     cudaEventRecord(e1, st);
     mxp_status rs = read_status(ws, st);
+    if (trsv_pending) ms_trsv += elapsed(t0, t1);
     if (stats) {
         stats->iterations = it;
         stats->converged = converged ? 1 : 0;
@@ -1021,10 +1064,10 @@ extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float
         stats->trsv_calls = trsv_calls;
         stats->inner_iterations = inner;
     }
-    if (s != MXP_OK) return done(s);
-    if (rs != MXP_OK) return done(rs);
-    if (!converged) return done(fail(MXP_NOT_CONVERGED, "IR: maxit reached without convergence"));
-    return done(MXP_OK);
+    if (s != MXP_OK) return s;
+    if (rs != MXP_OK) return rs;
+    if (!converged) return fail(MXP_NOT_CONVERGED, "IR: maxit reached without convergence");
+    return MXP_OK;
 }
 
 extern "C" mxp_status mxp_solve(int n, int b, uint64_t seed, float *d_A, int64_t lda,

@@ -6,8 +6,8 @@
  * baseline leg load it.  The product path never calls into it.
  *
  * Parity pinning: the generator functions below are checked bit-for-bit
- * against the reference's own hpl_rand.hpp compiled in place
- * (oracle/build_ref.sh -> oracle/_ref/libmxpref.so) and against the committed
+ * against the reference's own hpl_rand.hpp compiled in place (the Makefile's
+ * `ref` target -> oracle/_ref/libmxpref.so) and against the committed
  * fixtures in tests/golden/.  The LU/Schur/TRSM/IR restatements follow the
  * reference's algorithm; the reference's numbers at that boundary come from
  * rocBLAS/rocSOLVER, which are not part of the reference tree, so factor
@@ -415,8 +415,141 @@ static void schur_f32(int m, int n, int K, const float *Lf, int64_t ldl, const f
     }
 }
 
+/* ------------------------------------------------------------------------ */
+/* Blocked diagonal-block LU and triangular inverses                         */
+/* ------------------------------------------------------------------------ */
+
+/* Right-looking no-pivot LU of an n x n FP32 block in 64-column steps: the
+ * 64 x 64 diagonal block by sgetrf_nopiv_naive's order (reciprocal pivot,
+ * scale, rank-1 update; sgetrf_nopiv.cpp:27-61), the L strip below it by
+ * STRSM(R,U,N,N), the U strip right of it by STRSM(L,L,N,U), then the
+ * rank-64 FP32 update of the trailing block.  The reference factors the
+ * diagonal block with rocSOLVER sgetrf_npvt (panel_trf.hpp:678-681), whose
+ * blocking is not part of the reference tree; this is the same no-pivot LU,
+ * blocked the way the product's diagonal kernel is, so both round alike.
+ * Returns 0 or 1 + the index of the first zero / non-finite pivot. */
+ORC_EXPORT int orc_getrf_nopiv_blocked(int n, float *a, int64_t lda) {
+    const int NB = 64;
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        int nb = n - j0 < NB ? n - j0 : NB;
+        float *D = a + j0 + lda * j0;
+        int info = orc_getrf_nopiv(nb, nb, D, lda);
+        if (info) return j0 + info;
+        int m = n - j0 - nb;
+        if (m <= 0) break;
+        orc_trsm_runn(m, nb, D, lda, D + nb, lda);
+        orc_trsm_llnu(nb, m, D, lda, D + lda * nb, lda);
+        const float *L = D + nb;
+        const float *U = D + lda * nb;
+        float *T = D + nb + lda * nb;
+#pragma omp parallel for schedule(static)
+        for (int j = 0; j < m; ++j) {
+            float *tj = T + lda * j;
+            const float *uj = U + lda * j;
+            for (int k = 0; k < nb; ++k) {
+                float ukj = uj[k];
+                const float *lk = L + lda * k;
+                for (int i = 0; i < m; ++i) tj[i] -= lk[i] * ukj;
+            }
+        }
+    }
+    return 0;
+}
+
+/* C (m x n) = alpha * A (m x K) B (K x n), FP32, with the k range of every
+ * output column limited to [kb(j), ke(j)) or of every row to [kb(i), ke(i))
+ * by the triangular operand (tri: 1 A upper, 2 A lower, 3 B upper, 4 B
+ * lower; 0 none).  The zeros skipped contribute exact zeros. */
+static void gemm_f32_tri(int m, int n, int K, float alpha, const float *A, int64_t lda, const float *B,
+                         int64_t ldb, float *C, int64_t ldc, int tri) {
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int j = 0; j < n; ++j) {
+        float *cj = C + ldc * j;
+        for (int i = 0; i < m; ++i) cj[i] = 0.0f;
+        int kb = 0, ke = K;
+        if (tri == 3) ke = j + 1 < K ? j + 1 : K;
+        if (tri == 4) kb = j;
+        for (int k = kb; k < ke; ++k) {
+            float bkj = B[k + ldb * j];
+            const float *ak = A + lda * k;
+            int ib = 0, ie = m;
+            if (tri == 1) ie = k + 1 < m ? k + 1 : m; /* A upper: rows <= k */
+            if (tri == 2) ib = k;                     /* A lower: rows >= k */
+            for (int i = ib; i < ie; ++i) cj[i] += ak[i] * bkj;
+        }
+        for (int i = 0; i < m; ++i) cj[i] *= alpha;
+    }
+}
+
+/* inv(U) -> XU and inv(L) -> XL (L unit lower) of a factored n x n block by
+ * recursive doubling.  The reference forms the same inverses for its
+ * TRSM-by-inverse path by a triangular solve against the identity
+ * (gen_identity_mat + STRSM, panel_trf_gdirect.hpp:86-92,124-129); the
+ * product computes them by doubling, and this is that computation:
+ *   1. every 64 x 64 diagonal block by substitution: row i of the inverse
+ *      solves x T = e_i (x_j = (delta_ij - sum_{q<j} x_q U(q,j)) / U(j,j)
+ *      for U; x_j = delta_ij - sum_{q>j} x_q L(q,j) for L);
+ *   2. for S = 64, 128, ... while S < s_stop (or S < n when s_stop <= 0):
+ *      adjacent S-blocks (the last pair may be ragged, second block c < S)
+ *      give the off-diagonal blocks X12 = -inv(U11) (U12 inv(U22)) and
+ *      X21 = -inv(L22) (L21 inv(L11)), FP32 products.
+ * Levels from s_stop on are left to the caller (they run as low-precision
+ * tensor-core products in the product path).  Everything outside the
+ * block triangles written is set to zero. */
+ORC_EXPORT void orc_tri_inverses(int n, const float *A, int64_t lda, float *XU, float *XL, int64_t ldx,
+                                 int s_stop) {
+    const int NB = 64;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            XU[i + ldx * j] = 0.0f;
+            XL[i + ldx * j] = 0.0f;
+        }
+    int nblk = (n + NB - 1) / NB;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int it = 0; it < 2 * nblk; ++it) {
+        int upper = it < nblk;
+        int r0 = (it % nblk) * NB;
+        int nb = n - r0 < NB ? n - r0 : NB;
+        float *X = upper ? XU : XL;
+        float x[64];
+        for (int i = 0; i < nb; ++i) {
+            if (upper) {
+                for (int jj = 0; jj < nb; ++jj) {
+                    float v = (jj == i) ? 1.0f : 0.0f;
+                    for (int q = 0; q < jj; ++q) v = fmaf(-x[q], A[r0 + q + lda * (r0 + jj)], v);
+                    x[jj] = jj >= i ? v / A[r0 + jj + lda * (r0 + jj)] : 0.0f;
+                }
+            } else {
+                for (int jj = nb - 1; jj >= 0; --jj) {
+                    float v = (jj == i) ? 1.0f : 0.0f;
+                    for (int q = jj + 1; q < nb; ++q) v = fmaf(-x[q], A[r0 + q + lda * (r0 + jj)], v);
+                    x[jj] = jj <= i ? v : 0.0f;
+                }
+            }
+            for (int jj = 0; jj < nb; ++jj) X[r0 + i + ldx * (r0 + jj)] = x[jj];
+        }
+    }
+    float *T = (float *)malloc(sizeof(float) * (size_t)n * n);
+    for (int S = NB; S < n && (s_stop <= 0 || S < s_stop); S *= 2) {
+        int np = n / (2 * S);
+        int c = n - np * 2 * S - S;
+        for (int p = 0; p <= np; ++p) {
+            int s2 = p < np ? S : c;
+            if (s2 <= 0) break;
+            int64_t r0 = (int64_t)p * 2 * S, r1 = r0 + S;
+            /* U: T = U12 inv(U22) (S x s2), X12 = -inv(U11) T */
+            gemm_f32_tri(S, s2, s2, 1.0f, A + r0 + lda * r1, lda, XU + r1 + ldx * r1, ldx, T, S, 3);
+            gemm_f32_tri(S, s2, S, -1.0f, XU + r0 + ldx * r0, ldx, T, S, XU + r0 + ldx * r1, ldx, 1);
+            /* L: T = L21 inv(L11) (s2 x S), X21 = -inv(L22) T */
+            gemm_f32_tri(s2, S, S, 1.0f, A + r1 + lda * r0, lda, XL + r0 + ldx * r0, ldx, T, s2, 4);
+            gemm_f32_tri(s2, S, s2, -1.0f, XL + r1 + ldx * r1, ldx, T, s2, XL + r1 + ldx * r0, ldx, 2);
+        }
+    }
+    free(T);
+}
+
 /* Precision forms of the Schur update. */
-enum { ORC_FORM_FP16 = 0, ORC_FORM_BF16X2 = 1, ORC_FORM_FP8 = 2, ORC_FORM_FP32 = 3 };
+enum { ORC_FORM_FP16 = 0, ORC_FORM_BF16X2 = 1, ORC_FORM_FP8 = 2, ORC_FORM_FP32 = 3, ORC_FORM_BF16 = 4 };
 
 /* Quantise an m x K FP32 block (column-major, ld) to the dequantised FP32
  * values the tensor cores see.  out is m x Kout column-major (ld = m).
@@ -424,6 +557,27 @@ enum { ORC_FORM_FP16 = 0, ORC_FORM_BF16X2 = 1, ORC_FORM_FP8 = 2, ORC_FORM_FP32 =
  * as three K segments (hi|hi|lo for the left panel, hi|lo|hi for the right),
  * so one K'=3K product gives hi*hi + hi*lo + lo*hi.  FP8: E4M3 with a
  * power-of-two scale per 128 x 128 tile. */
+static void quantise_panel(int form, int is_right, int m, int K, const float *src, int64_t ld,
+                           float *out);
+
+/* Exported quantiser: the dequantised tensor-core operand of an m x K panel
+ * (rows = output rows, columns = K; element (i, k) at src[i + ld k], or at
+ * src[k + ld i] when src_rowmajor) into out, m x K*kmul column-major with
+ * ld = m (BF16X2: hi|hi|lo segments, or hi|lo|hi when is_right). */
+ORC_EXPORT void orc_quantise(int form, int is_right, int m, int K, const float *src, int64_t ld, int src_rowmajor,
+                             float *out) {
+    if (!src_rowmajor) {
+        quantise_panel(form, is_right, m, K, src, ld, out);
+        return;
+    }
+    float *t = (float *)malloc(sizeof(float) * (size_t)m * K);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < K; ++k)
+        for (int i = 0; i < m; ++i) t[(int64_t)k * m + i] = src[k + ld * (int64_t)i];
+    quantise_panel(form, is_right, m, K, t, m, out);
+    free(t);
+}
+
 static void quantise_panel(int form, int is_right, int m, int K, const float *src, int64_t ld,
                            float *out) {
     if (form == ORC_FORM_FP32) {
@@ -433,6 +587,10 @@ static void quantise_panel(int form, int is_right, int m, int K, const float *sr
 #pragma omp parallel for schedule(static)
         for (int k = 0; k < K; ++k)
             for (int i = 0; i < m; ++i) out[(int64_t)k * m + i] = orc_h2f(orc_f2h(src[i + ld * k]));
+    } else if (form == ORC_FORM_BF16) {
+#pragma omp parallel for schedule(static)
+        for (int k = 0; k < K; ++k)
+            for (int i = 0; i < m; ++i) out[(int64_t)k * m + i] = orc_bf2f(orc_f2bf(src[i + ld * k]));
     } else if (form == ORC_FORM_BF16X2) {
 #pragma omp parallel for schedule(static)
         for (int k = 0; k < K; ++k)
@@ -468,6 +626,7 @@ static void quantise_panel(int form, int is_right, int m, int K, const float *sr
 
 static int form_kmul(int form) { return form == ORC_FORM_BF16X2 ? 3 : 1; }
 
+
 /* Exported single Schur update on FP32 sources (quantise both panels then
  * C -= L * R^T): L is m x K (column-major, ldl), U is K x n (the U row
  * panel, column-major, ldu), C is m x n.  This is the oracle of
@@ -496,14 +655,30 @@ ORC_EXPORT void orc_schur_update(int form, int m, int n, int K, const float *L, 
  * the L column (:723, body :188-207) and the U row (:747, body :225-246),
  * casts (:724,:748), Schur update (:825-837).  Returns 0, or 1 + the global
  * index of the first zero / non-finite pivot. */
+/* Factor of a diagonal block (returns 0 or 1 + the first bad pivot) and the
+ * residual GEMV y = beta y + alpha A x: the oracle's own by default; the
+ * CPU baseline passes the reference's compiled CPU kernels instead
+ * (oracle/ref_wrap.cpp). */
+typedef int (*orc_getrf_fn)(int n, float *a, int64_t lda);
+typedef void (*orc_gemv_fn)(int n, int b, uint64_t seed, const double *d, double alpha, const double *x,
+                            double beta, double *y);
+
+static int getrf_default(int n, float *a, int64_t lda) { return orc_getrf_nopiv(n, n, a, lda); }
+
+static int panel_lu_impl(int n, int b, float *A, int64_t lda, int form, orc_getrf_fn getrf);
+
 ORC_EXPORT int orc_panel_lu(int n, int b, float *A, int64_t lda, int form) {
+    return panel_lu_impl(n, b, A, lda, form, getrf_default);
+}
+
+static int panel_lu_impl(int n, int b, float *A, int64_t lda, int form, orc_getrf_fn getrf) {
     int nb = n / b;
     int kmul = form_kmul(form);
     float *Lf = NULL, *Rf = NULL, *Ut = NULL;
     for (int k = 0; k < nb; ++k) {
         int64_t kk = (int64_t)k * b;
         float *Akk = A + kk + lda * kk;
-        int info = orc_getrf_nopiv(b, b, Akk, lda);
+        int info = getrf(b, Akk, lda);
         if (info) {
             free(Lf);
             free(Rf);
@@ -646,10 +821,27 @@ ORC_EXPORT double orc_infnorm(int n, const double *x) {
  * before the residual test passed (the reference's "step"), or -1 when maxit
  * evaluations did not converge (iterative_refinement.hpp:173).  hist (may be
  * NULL) receives the scaled residual of every evaluation. */
+static void gemv_default(int n, int b, uint64_t seed, const double *d, double alpha, const double *x,
+                         double beta, double *y) {
+    (void)b;
+    orc_otf_gemv(n, seed, d, alpha, x, beta, y);
+}
+
+static int ir_classic_impl(int n, int b, uint64_t seed, const float *LU, int64_t lda, const double *d,
+                           const double *rowsum, const double *rhs, double *x, int maxit, int ref1x1,
+                           double *out_resid, double *out_hpl, double *hist, orc_gemv_fn gemv);
+
 ORC_EXPORT int orc_ir_classic(int n, int b, uint64_t seed, const float *LU, int64_t lda,
                               const double *d, const double *rowsum, const double *rhs,
                               double *x, int maxit, int ref1x1, double *out_resid,
                               double *out_hpl, double *hist) {
+    return ir_classic_impl(n, b, seed, LU, lda, d, rowsum, rhs, x, maxit, ref1x1, out_resid, out_hpl, hist,
+                           gemv_default);
+}
+
+static int ir_classic_impl(int n, int b, uint64_t seed, const float *LU, int64_t lda, const double *d,
+                           const double *rowsum, const double *rhs, double *x, int maxit, int ref1x1,
+                           double *out_resid, double *out_hpl, double *hist, orc_gemv_fn gemv) {
     double *r = (double *)malloc(sizeof(double) * (size_t)n);
     double norma = 0.0;
     for (int i = 0; i < n; ++i) {
@@ -663,7 +855,7 @@ ORC_EXPORT int orc_ir_classic(int n, int b, uint64_t seed, const float *LU, int6
     for (int it = 0; it < maxit; ++it) {
         memcpy(r, rhs, sizeof(double) * (size_t)n);
         double normx = orc_infnorm(n, x);
-        orc_otf_gemv(n, seed, d, -1.0, x, 1.0, r);
+        gemv(n, b, seed, d, -1.0, x, 1.0, r);
         double normr = orc_infnorm(n, r);
         double hpl = normr / (norma * normx + normb) * 1.0 / ((double)n * eps);
         if (hist) hist[it] = hpl;
@@ -693,21 +885,33 @@ static double wall(void) {
     return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
 }
 
+ORC_EXPORT int orc_solve_ex(int n, int b, uint64_t seed, int diag_rule, int form, int maxit, double *x,
+                            double *out_stats, orc_getrf_fn getrf, orc_gemv_fn gemv);
+
 ORC_EXPORT int orc_solve(int n, int b, uint64_t seed, int diag_rule, int form, int maxit,
                          double *x, double *out_stats /* [t_lu, t_ir, resid, hpl, iters] */) {
+    return orc_solve_ex(n, b, seed, diag_rule, form, maxit, x, out_stats, NULL, NULL);
+}
+
+/* orc_solve with the diagonal-block factor and the residual GEMV supplied by
+ * the caller (NULL: the oracle's own). */
+ORC_EXPORT int orc_solve_ex(int n, int b, uint64_t seed, int diag_rule, int form, int maxit, double *x,
+                            double *out_stats, orc_getrf_fn getrf, orc_gemv_fn gemv) {
+    if (!getrf) getrf = getrf_default;
+    if (!gemv) gemv = gemv_default;
     float *A = (float *)malloc(sizeof(float) * (size_t)n * n);
     double *d = (double *)malloc(sizeof(double) * (size_t)n);
     double *rs = (double *)malloc(sizeof(double) * (size_t)n);
     double *rhs = (double *)malloc(sizeof(double) * (size_t)n);
     orc_matgen(n, seed, diag_rule, A, n, d, rs, rhs);
     double t0 = wall();
-    int info = orc_panel_lu(n, b, A, n, form);
+    int info = panel_lu_impl(n, b, A, n, form, getrf);
     double t1 = wall();
     int ret = -1;
     double resid = -1.0, hpl = -1.0;
     if (info == 0)
-        ret = orc_ir_classic(n, b, seed, A, n, d, diag_rule ? rs : NULL, rhs, x, maxit, 0, &resid,
-                             &hpl, NULL);
+        ret = ir_classic_impl(n, b, seed, A, n, d, diag_rule ? rs : NULL, rhs, x, maxit, 0, &resid, &hpl, NULL,
+                              gemv);
     double t2 = wall();
     if (out_stats) {
         out_stats[0] = t1 - t0;

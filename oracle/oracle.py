@@ -29,8 +29,8 @@ _vp = C.c_void_p
 
 
 def build() -> None:
-    """Compile the oracle (and oracle/_ref when the reference tree exists)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    """Compile the oracle (oracle/_ref is built by __graft_entry__.build)."""
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
 
 
 def lib() -> C.CDLL:
@@ -67,6 +67,10 @@ def lib() -> C.CDLL:
         L.orc_getrf_nopiv.restype = i32
         L.orc_trsm_runn.argtypes = [i32, i32, _vp, i64, _vp, i64]
         L.orc_trsm_llnu.argtypes = [i32, i32, _vp, i64, _vp, i64]
+        L.orc_getrf_nopiv_blocked.argtypes = [i32, _vp, i64]
+        L.orc_getrf_nopiv_blocked.restype = i32
+        L.orc_tri_inverses.argtypes = [i32, _vp, i64, _vp, _vp, i64, i32]
+        L.orc_quantise.argtypes = [i32, i32, i32, i32, _vp, i64, i32, _vp]
         L.orc_schur_update.argtypes = [i32, i32, i32, i32, _vp, i64, _vp, i64, _vp, i64]
         L.orc_panel_lu.argtypes = [i32, i32, _vp, i64, i32]
         L.orc_panel_lu.restype = i32
@@ -80,6 +84,8 @@ def lib() -> C.CDLL:
         L.orc_ir_classic.restype = i32
         L.orc_solve.argtypes = [i32, i32, u64, i32, i32, i32, _vp, _vp]
         L.orc_solve.restype = i32
+        L.orc_solve_ex.argtypes = [i32, i32, u64, i32, i32, i32, _vp, _vp, _vp, _vp]
+        L.orc_solve_ex.restype = i32
         L.orc_num_threads.restype = i32
         _lib = L
     return _lib
@@ -108,6 +114,9 @@ def ref() -> C.CDLL:
         R.ref_fp16_bits.argtypes = [C.c_float]
         R.ref_fp16_bits.restype = C.c_uint16
         R.otf_gemv_kernel.argtypes = [C.c_int64, i32, i32, dbl, _vp, _vp, u64]
+        R.ref_getrf_diag.argtypes = [i32, _vp, C.c_int64]
+        R.ref_getrf_diag.restype = i32
+        R.ref_otf_gemv.argtypes = [i32, i32, u64, _vp, dbl, _vp, dbl, _vp]
         _ref = R
     return _ref
 
@@ -165,10 +174,19 @@ def ir_classic(n, b, seed, LU, d, rowsum, rhs, maxit=50, ref1x1=False):
     return it, x, float(resid[0]), float(hpl[0]), hist
 
 
-def solve(n, b, seed, diag_rule=DIAG_ROWSUM, form=FORM_FP16, maxit=50):
+def solve(n, b, seed, diag_rule=DIAG_ROWSUM, form=FORM_FP16, maxit=50, ref_kernels=False):
+    """Whole CPU solve (generation excluded from t_lu / t_ir).  ref_kernels:
+    the diagonal blocks by the reference's compiled sgetrf_nopiv_omp<6> and the
+    residual by its compiled otf_gemv_kernel (oracle/_ref), the rest by the
+    oracle's restatement."""
     x = np.empty(n, np.float64)
     st = np.zeros(5)
-    rc = lib().orc_solve(n, b, seed, diag_rule, form, maxit, _p(x), _p(st))
+    if ref_kernels:
+        R = ref()
+        rc = lib().orc_solve_ex(n, b, seed, diag_rule, form, maxit, _p(x), _p(st),
+                                C.cast(R.ref_getrf_diag, C.c_void_p), C.cast(R.ref_otf_gemv, C.c_void_p))
+    else:
+        rc = lib().orc_solve(n, b, seed, diag_rule, form, maxit, _p(x), _p(st))
     return rc, x, {"t_lu": st[0], "t_ir": st[1], "resid": st[2], "hpl": st[3], "iters": int(st[4])}
 
 

@@ -85,3 +85,38 @@ def test_ir_1x1_reference_behaviour(orc):
     it_exact, *_ = orc.ir_classic(n, b, 42, A, d, None, rhs)
     it_ref, *_ = orc.ir_classic(n, b, 42, A, d, None, rhs, ref1x1=True)
     assert 0 <= it_exact < it_ref
+
+
+@pytest.mark.parametrize("n,b,seed", [(512, 128, 42), (1024, 256, 7), (640, 320, 11)])
+def test_reference_otf_gemv_driver(orc, n, b, seed):
+    """ref_otf_gemv (the reference's otf_gemv_kernel driven block by block as
+    panel_gemv.hpp:310-338 does) against the oracle's residual GEMV: the same
+    FP64 products summed in another order."""
+    R = orc.ref()
+    _, d, _, rhs = orc.matgen(n, seed, with_matrix=False)
+    x = np.random.default_rng(n).standard_normal(n)
+    y1, y2 = rhs.copy(), rhs.copy()
+    orc.otf_gemv(n, seed, d, -1.0, x, 1.0, y1)
+    R.ref_otf_gemv(n, b, seed, d.ctypes.data, -1.0, x.ctypes.data, 1.0, y2.ctypes.data)
+    scale = np.abs(orc.matgen_f64(n, seed, d)) @ np.abs(x) + np.abs(rhs)
+    assert np.all(np.abs(y1 - y2) <= 1e-14 * scale)
+
+
+@pytest.mark.parametrize("n", [256, 640])
+def test_reference_tuned_getrf(orc, n):
+    R = orc.ref()
+    A, _, _, _ = orc.matgen(n, 3)
+    A1, A2 = A.copy(order="F"), A.copy(order="F")
+    assert orc.lib().orc_getrf_nopiv(n, n, A1.ctypes.data, n) == 0
+    assert R.ref_getrf_diag(n, A2.ctypes.data, n) == 0
+    assert np.linalg.norm(A1 - A2) <= 1e-6 * np.linalg.norm(A1)
+
+
+def test_cpu_solve_with_reference_kernels(orc):
+    """The CPU baseline's solve with the reference's compiled diagonal LU and
+    residual kernel converges like the oracle's own."""
+    rc1, x1, st1 = orc.solve(2048, 256, 42)
+    rc2, x2, st2 = orc.solve(2048, 256, 42, ref_kernels=True)
+    assert rc1 >= 0 and rc2 >= 0 and abs(rc1 - rc2) <= 1
+    assert st2["hpl"] < 16.0
+    assert np.max(np.abs(x1 - x2)) <= 1e-10 * np.max(np.abs(x1))
