@@ -285,9 +285,50 @@ mxp_status mxp_otf_gemv(int n, uint64_t seed, const double *d_d, double alpha, c
  * the library, reserved on every GPU that loads it until the process exits.
  * Limit: n <= 262144, larger n returns MXP_INVALID_ARG.  The first call on a
  * device resolves the array's address (make it before any stream capture).
- * All calls share the array: calls that overlap on the GPU race. */
+ * The stream must belong to the current device (another device's stream
+ * returns MXP_INVALID_ARG).  All calls share the array: calls that overlap
+ * on the GPU race. */
 mxp_status mxp_otf_gemv_noalloc(int n, uint64_t seed, const double *d_d, double alpha,
                                 const double *d_x, double beta, double *d_y, void *stream);
+
+/* ---- Higham's HPL-AI matrix --------------------------------------------- */
+
+/* higham_mat_comp_beta (higham_mat_impl.cpp:98-130) and HMGen's alpha =
+ * rho * beta (highammgen.hpp:15-20): the parameters of Higham's matrix
+ * A = L U (L unit lower with strictly lower entries alpha, U unit upper with
+ * strictly upper entries beta) whose estimated cond(A, inf) is `cond`, by
+ * bisection on Fasi and Higham's closed-form estimate.  Host only. */
+mxp_status mxp_higham_params(int n, double cond, double rho, double *alpha, double *beta);
+
+/* pmatgen(HMGen) + pdiaggen (matgen.hpp:157-208, 399-417): A(i,j) = beta +
+ * ab*i above the diagonal, 1 + ab*i on it, alpha + ab*j below it (ab =
+ * alpha*beta; FP32, formed from the FP32-rounded parameters by one fused
+ * multiply-add each), d_i = 1 + ab*i (FP64), and the right-hand side from the
+ * LCG stream of `seed` (column n, as panel_colvgen, matgen.hpp:419-436).
+ * Any of d_A, d_d, d_rhs may be NULL. */
+mxp_status mxp_matgen_higham(int n, double alpha, double beta, uint64_t seed, float *d_A, int64_t lda,
+                             double *d_d, double *d_rhs, void *stream);
+
+/* otf_gemv for HMGen (panel_gemv.hpp:362-388; hmg_gemv_up / hmg_gemv_low /
+ * hmg_gemv_diag, otf_gemv.cpp:135-316): y = b*y + a*A*x with the entries of
+ * Higham's matrix regenerated in FP64 (never read), every row summed in
+ * column order with fused multiply-adds.  The diagonal blocks use the
+ * generator's entries (the reference's hmg_gemv_diag swaps alpha and beta
+ * there).  Deterministic. */
+mxp_status mxp_higham_gemv(int n, double alpha, double beta, double a, const double *d_x, double b,
+                           double *d_y, void *stream);
+
+/* higham_infnorm (panel_norm.hpp:136-175): ||A||_inf of Higham's matrix (all
+ * entries are positive: the largest row sum).  Host only. */
+mxp_status mxp_higham_infnorm(int n, double alpha, double beta, double *h_out);
+
+/* The refinement of this workspace (mxp_iterative_refinement, mxp_solve,
+ * mxp_solve_host) regenerates Higham's matrix with these parameters instead
+ * of the LCG matrix of the seed, and takes ||A||_inf from
+ * mxp_higham_infnorm when its norma argument is <= 0.  alpha = beta = 0
+ * goes back to the LCG matrix.  (The reference's HMGen overloads of
+ * otf_gemv / higham_infnorm, templated on the generator type.) */
+mxp_status mxp_workspace_set_matrix_higham(mxp_workspace *ws, double alpha, double beta);
 
 /* trsvL_h + trsvU_h (panel_trsv.hpp:308-597): x <- U^{-1} L^{-1} x with
  * the FP32 factors of mxp_panel_lu, vectors in FP64, block substitution.

@@ -119,6 +119,11 @@ _SIGS = {
     "mxp_batch_autotune": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _vp, C.POINTER(BatchStats)]),
     "mxp_batch_solve": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _vp, C.POINTER(BatchStats)]),
     "mxp_batch_results": (_i32, [_vp, C.POINTER(BatchResult)]),
+    "mxp_higham_params": (_i32, [_i32, _dbl, _dbl, C.POINTER(_dbl), C.POINTER(_dbl)]),
+    "mxp_matgen_higham": (_i32, [_i32, _dbl, _dbl, _u64, _vp, _i64, _vp, _vp, _vp]),
+    "mxp_higham_gemv": (_i32, [_i32, _dbl, _dbl, _dbl, _vp, _dbl, _vp, _vp]),
+    "mxp_higham_infnorm": (_i32, [_i32, _dbl, _dbl, C.POINTER(_dbl)]),
+    "mxp_workspace_set_matrix_higham": (_i32, [_vp, _dbl, _dbl]),
     "mxp_kernel_launches": (_i64, []),
     "mxp_reset_kernel_launches": (None, []),
 }
@@ -204,6 +209,10 @@ class Workspace:
     def set_option(self, key: int, value: int) -> None:
         check(lib().mxp_workspace_set_option(self.handle, key, value))
 
+    def set_matrix_higham(self, alpha: float, beta: float) -> None:
+        """Refine against Higham's matrix (alpha, beta); (0, 0): the LCG matrix."""
+        check(lib().mxp_workspace_set_matrix_higham(self.handle, alpha, beta))
+
     def panel_view(self, side: int) -> dict:
         """Device location of the low-precision L (side 0) or R (side 1) panel
         slots (mxp_workspace_panel_view)."""
@@ -274,8 +283,46 @@ def matgen_f64(n: int, seed: int = 42, diag_rule: int = DIAG_ROWSUM, A=None, lda
     return A
 
 
+# ---------------------------------------------------------------------------
+# Higham's HPL-AI matrix (HMGen, highammgen.hpp:4-30)
+# ---------------------------------------------------------------------------
+def higham_params(n: int, cond: float = 1e3, rho: float = 0.5):
+    """(alpha, beta) of Higham's matrix for the estimated cond(A, inf) = cond."""
+    a, b = C.c_double(), C.c_double()
+    check(lib().mxp_higham_params(n, cond, rho, C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+def higham_matgen(n: int, alpha: float, beta: float, seed: int = 42, device=None, stream=None) -> Problem:
+    """pmatgen(HMGen) + pdiaggen (matgen.hpp:157-208, 399-417) and the LCG
+    right-hand side of `seed`.  The Problem carries .alpha / .beta."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    A = torch.empty(n * n, dtype=torch.float32, device=dev)
+    d = torch.empty(n, dtype=torch.float64, device=dev)
+    rhs = torch.empty(n, dtype=torch.float64, device=dev)
+    check(lib().mxp_matgen_higham(n, alpha, beta, seed, _ptr(A), n, _ptr(d), _ptr(rhs), _stream(stream)))
+    p = Problem(n, seed, DIAG_ROWSUM, A, n, d, None, rhs)
+    p.alpha, p.beta = alpha, beta
+    return p
+
+
+def higham_gemv(n, alpha, beta, a, x, b, y, stream=None):
+    check(lib().mxp_higham_gemv(n, alpha, beta, a, _ptr(x), b, _ptr(y), _stream(stream)))
+
+
+def higham_infnorm(n: int, alpha: float, beta: float) -> float:
+    out = C.c_double()
+    check(lib().mxp_higham_infnorm(n, alpha, beta, C.byref(out)))
+    return out.value
+
+
 def regenerate(p: Problem, stream=None) -> None:
     """Refill p.A (and d / rowsum / rhs) in place."""
+    if getattr(p, "alpha", None) is not None:
+        check(lib().mxp_matgen_higham(p.n, p.alpha, p.beta, p.seed, _ptr(p.A), p.lda, _ptr(p.d), _ptr(p.rhs),
+                                      _stream(stream)))
+        return
     check(lib().mxp_matgen(p.n, p.seed, p.diag_rule, _ptr(p.A), p.lda, _ptr(p.d), _ptr(p.rowsum),
                            _ptr(p.rhs), _stream(stream)))
 

@@ -57,6 +57,9 @@ int num_sms() {
 using namespace mxp;
 
 namespace mxp {
+mxp_status launch_higham_gemv(int n, double alpha, double beta, double a, const double *x, double b, double *y,
+                              cudaStream_t st);
+double higham_infnorm(int n, double alpha, double beta);
 int gmres_dot_blocks(int n);
 mxp_status launch_mdot(int n, int nv, const double *V, int64_t ldv, const double *w,
                        double *partial, double *out, int accumulate, cudaStream_t st);
@@ -97,6 +100,10 @@ struct mxp_workspace {
     int *tile_ctr = nullptr;  // shared tile counter of the split trailing pass
     int *trsm_ctr = nullptr;  // tile counter of the TRSM-by-inverse products (claimed dynamically)
     int trsm_counter = 1;     // TRSM products take tiles from trsm_ctr (0: static round robin)
+    // matrix the refinement's residual regenerates: the LCG matrix of the
+    // seed (default) or Higham's matrix with parameters (h_alpha, h_beta)
+    int higham = 0;
+    double h_alpha = 0.0, h_beta = 0.0;
     size_t esize = 2;        // panel element size
     void *lpanel[2] = {nullptr, nullptr};
     void *rpanel[2] = {nullptr, nullptr};
@@ -358,6 +365,20 @@ extern "C" mxp_status mxp_workspace_set_option(mxp_workspace *ws, int key, int v
         default:
             return fail(MXP_INVALID_ARG, "set_option: unknown key");
     }
+}
+
+extern "C" mxp_status mxp_workspace_set_matrix_higham(mxp_workspace *ws, double alpha, double beta) {
+    if (!ws) return fail(MXP_INVALID_ARG, "set_matrix_higham: workspace is NULL");
+    if (alpha == 0.0 && beta == 0.0) {
+        ws->higham = 0;
+        return MXP_OK;
+    }
+    if (!(alpha > 0.0) || !(beta > 0.0) || !std::isfinite(alpha) || !std::isfinite(beta))
+        return fail(MXP_INVALID_ARG, "set_matrix_higham: alpha and beta must be positive (both 0: back to the LCG)");
+    ws->higham = 1;
+    ws->h_alpha = alpha;
+    ws->h_beta = beta;
+    return MXP_OK;
 }
 
 extern "C" mxp_status mxp_workspace_panel_view(const mxp_workspace *ws, int side, mxp_panel_view *out) {
@@ -818,6 +839,14 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
 // ---------------------------------------------------------------------------
 // refinement
 // ---------------------------------------------------------------------------
+// y = b y + a A x for the matrix the workspace refines against: regenerated
+// from the LCG of `seed`, or Higham's matrix when the workspace was set to it.
+static mxp_status residual_gemv(mxp_workspace *ws, int n, uint64_t seed, const double *dd, double a,
+                                const double *x, double b, double *y, cudaStream_t st) {
+    if (ws->higham) return launch_higham_gemv(n, ws->h_alpha, ws->h_beta, a, x, b, y, st);
+    return launch_otf_gemv(n, seed, dd, a, x, b, y, ws->partials, ws->max_splits, st);
+}
+
 // x <- U^{-1} L^{-1} x with the factor LU: by the stored inverses of the
 // diagonal blocks when they belong to this factor (the last mxp_panel_lu on
 // the workspace), else by the chain of 64-row blocks.
@@ -929,7 +958,7 @@ static mxp_status gmres_correction(int n, uint64_t seed, const float *LU, int64_
         }
         for (int j = 0; j < m; ++j) {
             double *vj = V + (int64_t)j * n;
-            s = timed(ms_gemv, [&] { return launch_otf_gemv(n, seed, dd, 1.0, vj, 0.0, w, ws->partials, ws->max_splits, st); });
+            s = timed(ms_gemv, [&] { return residual_gemv(ws, n, seed, dd, 1.0, vj, 0.0, w, st); });
             if (s == MXP_OK) s = timed(ms_trsv, [&] { return lu_solve_ws(ws, n, LU, lda, w, st); });
             // classical Gram-Schmidt, twice
             if (s == MXP_OK) s = launch_mdot(n, j + 1, V, n, w, ws->gpart, hcol, 0, st);
@@ -980,6 +1009,7 @@ extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float
     mxp_status s = MXP_OK;
     cudaEventRecord(e0, st);
     MXP_CUDA(cudaMemsetAsync(ws->status, 0, sizeof(DevStatus), st));
+    if (norma <= 0.0 && ws->higham) norma = higham_infnorm(n, ws->h_alpha, ws->h_beta);
     if (norma <= 0.0) {
         s = launch_norma(n, d_d, d_rowsum, sc + 2, st);
         if (s != MXP_OK) return s;
@@ -1001,7 +1031,7 @@ extern "C" mxp_status mxp_iterative_refinement(int n, uint64_t seed, const float
         s = launch_copy(n, d_rhs, r, st);
         if (s == MXP_OK) s = launch_infnorm(n, d_x, sc + 0, st);
         cudaEventRecord(g0, st);
-        if (s == MXP_OK) s = launch_otf_gemv(n, seed, d_d, -1.0, d_x, 1.0, r, ws->partials, ws->max_splits, st);
+        if (s == MXP_OK) s = residual_gemv(ws, n, seed, d_d, -1.0, d_x, 1.0, r, st);
         cudaEventRecord(g1, st);
         if (s == MXP_OK) s = launch_infnorm(n, r, sc + 1, st);
         if (s != MXP_OK) return s;

@@ -18,6 +18,9 @@
 //  * Its device address is looked up (cudaGetSymbolAddress) on the first call
 //    made on each device, with that device current; make that first call
 //    before any stream capture begins.
+//  * The stream must belong to the current device (the array used is the
+//    current device's copy); a stream of another device is rejected with
+//    MXP_INVALID_ARG.
 //  * Every call shares the one array and it keeps the last call's contents.
 //    Each call overwrites every partial sum it later reads, so nothing needs
 //    clearing between calls; calls that overlap on the GPU (different streams,
@@ -67,9 +70,17 @@ extern "C" mxp_status mxp_otf_gemv_noalloc(int n, uint64_t seed, const double *d
     if ((int64_t)n > kNoAllocMaxN)
         return fail(MXP_INVALID_ARG, "otf_gemv_noalloc: n exceeds the fixed scratch (maximum n = 262144); "
                                      "use mxp_otf_gemv with a workspace");
+    cudaStream_t st = as_stream(stream);
+    if (st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread) {  // those name the current device
+        int cur = 0, sdev = 0;
+        MXP_CUDA(cudaGetDevice(&cur));
+        MXP_CUDA(cudaStreamGetDevice(st, &sdev));
+        if (sdev != cur)
+            return fail(MXP_INVALID_ARG, "otf_gemv_noalloc: the stream belongs to another device than the current one");
+    }
     double *scratch = nullptr;
     mxp_status s = scratch_address(&scratch);
     if (s != MXP_OK) return s;
     const int max_splits = (int)imin64(16, kScratchDoubles / n);
-    return launch_otf_gemv(n, seed, d_d, alpha, d_x, beta, d_y, scratch, max_splits, as_stream(stream));
+    return launch_otf_gemv(n, seed, d_d, alpha, d_x, beta, d_y, scratch, max_splits, st);
 }

@@ -15,6 +15,7 @@
  *
  * Every function cites the reference file:line it restates.
  */
+#include <float.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -925,6 +926,161 @@ ORC_EXPORT int orc_solve_ex(int n, int b, uint64_t seed, int diag_rule, int form
     free(rs);
     free(rhs);
     return info ? -2 : ret;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Higham's HPL-AI matrix A = L U                                            */
+/* ------------------------------------------------------------------------ */
+/* L is unit lower triangular with every strictly lower entry alpha, U unit
+ * upper triangular with every strictly upper entry beta (highammgen.hpp:4-30),
+ * so a_ij = beta + alpha*beta*i (i < j), 1 + alpha*beta*i (i = j),
+ * alpha + alpha*beta*j (i > j) (pmatgen, matgen.hpp:157-208); the diagonal
+ * vector is d_i = 1 + alpha*beta*i (pdiaggen, matgen.hpp:399-417).  beta
+ * comes from the wanted infinity-norm condition number and rho = alpha/beta
+ * by bisection on Fasi and Higham's closed-form estimate of cond(A, inf)
+ * (higham_mat_impl.cpp:36-149, from the hpl-ai-matrix project). */
+
+/* The estimate of cond(A, inf) for the matrix with parameters (a, b): the
+ * largest of three candidate row sums of A times the largest of two
+ * candidate row sums of inv(A) (higham_mat_impl.cpp:36-64).  The integer
+ * terms are formed in 64 bits: the reference forms them in int, which
+ * overflows once n exceeds about 37800 (3 i'(i'-1)/2 with i' = n); below
+ * that the two agree bit for bit. */
+static double hg_cond_estimate(int n_, double a, double b) {
+    if (isnan(a)) a = b / 2;
+    const int64_t n = n_;
+    const int64_t ip = floor(1. / a) < (double)n ? (int64_t)floor(1. / a) : n;
+    const int64_t k = floor((1 + b) / b) < (double)(n - 1) ? (int64_t)floor((1 + b) / b) : n - 1;
+    const double row_1 = 1 + (n - 1) * b;
+    const double row_ip = 1 + (2 * k - ip + 1) * a + (n - ip) * b +
+                          (-k * k + k + 3 * ip * (ip - 1) / 2 - n * ip + n) * a * b;
+    const double row_n = 1 + (2 * k - n + 1) * a + (-k * k + k + n * (n - 1) / 2) * a * b;
+    double norm_a = row_1 > row_ip ? row_1 : row_ip;
+    norm_a = norm_a > row_n ? norm_a : row_n;
+    const double r = (1 + a) * (1 + b);
+    const double inv_1 = (1 + a) * (1. / (1 + a) + (r == 0. ? 0. : b * (1 - pow(r, n - 1)) / (1 - r)));
+    const double inv_n = pow(1 + a, n) * (1. / (1 + a));
+    const double norm_inv = inv_1 > inv_n ? inv_1 : inv_n;
+    const double c = norm_a * norm_inv;
+    return isinf(c) ? DBL_MAX : c;
+}
+
+/* Bisection for the root of f(x) = cond(rho x, x) - kappa between lo (f < 0)
+ * and hi (f > 0), to a relative width of about one ulp
+ * (higham_mat_impl.cpp:66-96). */
+static double hg_bisect(int n, double kappa, double rho, double lo, double hi) {
+    const double flo = hg_cond_estimate(n, rho * lo, lo) - kappa;
+    const double fhi = hg_cond_estimate(n, rho * hi, hi) - kappa;
+    if (flo > 0. || fhi < 0.) return NAN;
+    for (;;) {
+        if (hi - lo < (2. * fabs(hi) + 0.5) * DBL_EPSILON) break;
+        const double mid = (lo + hi) / 2;
+        if (mid == lo || mid == hi) break;
+        const double fm = hg_cond_estimate(n, rho * mid, mid) - kappa;
+        if (fm == 0.) return mid;
+        if (fm < 0.)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return hi;
+}
+
+/* beta for cond(A, inf) = kappa and alpha = rho beta (higham_mat_comp_beta,
+ * higham_mat_impl.cpp:98-130): the upper end starts at 1/rho and halves until
+ * the estimate exceeds kappa; if the root gives alpha > 1 the upper end is
+ * quartered and the search repeated. */
+ORC_EXPORT double orc_higham_beta(int n, double kappa, double rho) {
+    const double lo = DBL_EPSILON;
+    double hi = 1. / rho;
+    for (int k = 1; k < 100; ++k) {
+        const double f = hg_cond_estimate(n, rho * hi, hi) - kappa;
+        if (isfinite(f) && f > 0.) break;
+        hi *= 0.5;
+    }
+    double beta = hg_bisect(n, kappa, rho, lo, hi);
+    while (rho * beta > 1.) {
+        hi *= 0.25;
+        beta = hg_bisect(n, kappa, rho, lo, hi);
+    }
+    return beta;
+}
+
+/* FP32 matrix and FP64 diagonal vector.  The FP32 entries are formed in
+ * FP32 from the FP32-rounded parameters, one fused multiply-add each (the
+ * pmatgen<float> arithmetic, matgen.hpp:169-201, with the multiply-add
+ * fused). */
+ORC_EXPORT void orc_higham_matgen_cols(int n, double alpha, double beta, int64_t j0, int64_t ncols, float *A,
+                                       int64_t lda) {
+    const float fa = (float)alpha, fb = (float)beta, fab = fa * fb;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < ncols; ++c) {
+        const int64_t j = j0 + c;
+        float *col = A + lda * c;
+        const float low = fmaf(fab, (float)j, fa);
+        for (int64_t i = 0; i < n; ++i)
+            col[i] = i < j ? fmaf(fab, (float)i, fb) : (i == j ? fmaf(fab, (float)j, 1.0f) : low);
+    }
+}
+
+ORC_EXPORT void orc_higham_matgen(int n, double alpha, double beta, float *A, int64_t lda, double *d) {
+    const float fa = (float)alpha, fb = (float)beta, fab = fa * fb;
+    const double ab = alpha * beta;
+    if (A) {
+#pragma omp parallel for schedule(static)
+        for (int64_t j = 0; j < n; ++j) {
+            float *col = A + lda * j;
+            const float low = fmaf(fab, (float)j, fa);
+            for (int64_t i = 0; i < n; ++i)
+                col[i] = i < j ? fmaf(fab, (float)i, fb) : (i == j ? fmaf(fab, (float)j, 1.0f) : low);
+        }
+    }
+    if (d)
+        for (int64_t i = 0; i < n; ++i) d[i] = fma(ab, (double)i, 1.0);
+}
+
+/* FP64 entry (i, j) of the matrix the residual uses (the hmg_gemv_* values,
+ * otf_gemv.cpp:135-316, with alpha and beta in the places pmatgen gives
+ * them). */
+static inline double hg_elem(double alpha, double beta, double ab, int64_t i, int64_t j) {
+    if (i < j) return fma(ab, (double)i, beta);
+    if (i > j) return fma(ab, (double)j, alpha);
+    return fma(ab, (double)i, 1.0);
+}
+
+/* The FP64 matrix the residual uses, column-major (for FP64 references). */
+ORC_EXPORT void orc_higham_matgen_f64(int n, double alpha, double beta, double *A, int64_t lda) {
+    const double ab = alpha * beta;
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < n; ++j)
+        for (int64_t i = 0; i < n; ++i) A[i + lda * j] = hg_elem(alpha, beta, ab, i, j);
+}
+
+/* y = b y + a A x with A regenerated in FP64, each row summed in column
+ * order with fused multiply-adds (otf_gemv for HMGen, panel_gemv.hpp:362-388). */
+ORC_EXPORT void orc_higham_gemv(int n, double alpha, double beta, double a, const double *x, double b,
+                                double *y) {
+    const double ab = alpha * beta;
+#pragma omp parallel for schedule(static, 64)
+    for (int64_t i = 0; i < n; ++i) {
+        double t = 0.0;
+        for (int64_t j = 0; j < n; ++j) t = fma(hg_elem(alpha, beta, ab, i, j), x[j], t);
+        y[i] = b == 0.0 ? a * t : fma(b, y[i], a * t);
+    }
+}
+
+/* ||A||_inf: every entry is positive, so the largest row sum of the entries
+ * (higham_infnorm, panel_norm.hpp:136-175), each row summed in column order. */
+ORC_EXPORT double orc_higham_infnorm(int n, double alpha, double beta) {
+    const double ab = alpha * beta;
+    double m = 0.0;
+#pragma omp parallel for reduction(max : m) schedule(static, 64)
+    for (int64_t i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (int64_t j = 0; j < n; ++j) s += hg_elem(alpha, beta, ab, i, j);
+        m = m > s ? m : s;
+    }
+    return m;
 }
 
 ORC_EXPORT int orc_num_threads(void) {

@@ -71,6 +71,14 @@ def lib() -> C.CDLL:
         L.orc_getrf_nopiv_blocked.restype = i32
         L.orc_tri_inverses.argtypes = [i32, _vp, i64, _vp, _vp, i64, i32]
         L.orc_quantise.argtypes = [i32, i32, i32, i32, _vp, i64, i32, _vp]
+        L.orc_higham_beta.argtypes = [i32, dbl, dbl]
+        L.orc_higham_beta.restype = dbl
+        L.orc_higham_matgen.argtypes = [i32, dbl, dbl, _vp, i64, _vp]
+        L.orc_higham_matgen_cols.argtypes = [i32, dbl, dbl, i64, i64, _vp, i64]
+        L.orc_higham_gemv.argtypes = [i32, dbl, dbl, dbl, _vp, dbl, _vp]
+        L.orc_higham_matgen_f64.argtypes = [i32, dbl, dbl, _vp, i64]
+        L.orc_higham_infnorm.argtypes = [i32, dbl, dbl]
+        L.orc_higham_infnorm.restype = dbl
         L.orc_schur_update.argtypes = [i32, i32, i32, i32, _vp, i64, _vp, i64, _vp, i64]
         L.orc_panel_lu.argtypes = [i32, i32, _vp, i64, i32]
         L.orc_panel_lu.restype = i32
@@ -117,6 +125,9 @@ def ref() -> C.CDLL:
         R.ref_getrf_diag.argtypes = [i32, _vp, C.c_int64]
         R.ref_getrf_diag.restype = i32
         R.ref_otf_gemv.argtypes = [i32, i32, u64, _vp, dbl, _vp, dbl, _vp]
+        R.ref_higham_gemv.argtypes = [i32, i32, dbl, dbl, dbl, _vp, _vp]
+        R.higham_mat_comp_beta.argtypes = [i32, dbl, dbl]
+        R.higham_mat_comp_beta.restype = dbl
         _ref = R
     return _ref
 
@@ -244,3 +255,33 @@ def schur_update(form: int, C: np.ndarray, L: np.ndarray, U: np.ndarray) -> np.n
     U = np.asfortranarray(U, dtype=np.float32)
     lib().orc_schur_update(form, m, n, K, L.ctypes.data, m, U.ctypes.data, K, C.ctypes.data, m)
     return C
+
+
+# ----------------------------------------------------------------------------
+# Higham's HPL-AI matrix
+# ----------------------------------------------------------------------------
+def higham_params(n: int, cond: float, rho: float):
+    """(alpha, beta) with alpha = rho * beta for cond(A, inf) = cond."""
+    beta = lib().orc_higham_beta(n, cond, rho)
+    return rho * beta, beta
+
+
+def higham_matgen(n: int, alpha: float, beta: float, with_matrix: bool = True):
+    """(A float32 Fortran-ordered, d float64)."""
+    A = np.empty((n, n), np.float32, order="F") if with_matrix else None
+    d = np.empty(n, np.float64)
+    lib().orc_higham_matgen(n, alpha, beta, _p(A) if A is not None else None, n, _p(d))
+    return A, d
+
+
+def higham_matrix_f64(n: int, alpha: float, beta: float) -> np.ndarray:
+    """The FP64 matrix the residual uses (entries regenerated in FP64)."""
+    A = np.empty((n, n), np.float64, order="F")
+    lib().orc_higham_matgen_f64(n, alpha, beta, _p(A), n)
+    return A
+
+
+def higham_gemv(n, alpha, beta, a, x, b, y):
+    lib().orc_higham_gemv(n, alpha, beta, a, _p(x), b, _p(y))
+    return y
+

@@ -5,8 +5,10 @@
 // in oracle/_ref/.
 //
 // Pieces: the LCG generator (hpl_rand.hpp), the CPU on-the-fly GEMV kernel
-// (otf_gemv.cpp through svesim.hpp / fp16sim.hpp on x86), and the CPU no-pivot
-// LU (sgetrf_nopiv.cpp, naive and the 6-wide OpenMP variant).
+// (otf_gemv.cpp through svesim.hpp / fp16sim.hpp on x86), the CPU no-pivot
+// LU (sgetrf_nopiv.cpp, naive and the 6-wide OpenMP variant), and the
+// parameter search of Higham's HPL-AI matrix (higham_mat_impl.cpp; its
+// higham_mat_comp_beta has C linkage already).
 #define __HPLAI_DEVICE_MACROS__ 1
 #define __host__
 #define __device__
@@ -16,6 +18,7 @@ int grank = 0;  // declared extern by hpl_rand.hpp:10
 #include "hpl_rand.hpp"
 #include "otf_gemv.cpp"
 #include "sgetrf_nopiv.cpp"
+#include "higham_mat_impl.cpp"
 
 extern "C" {
 // fill_one_panel_with_rand (hpl_rand.hpp:158-198): FP32 block with the CPU
@@ -104,5 +107,24 @@ void ref_otf_gemv(int n, int b, uint64_t seed, const double *d, double alpha, co
             }
         }
     }
+}
+
+// y += a A x for Higham's matrix at a 1 x 1 grid, as otf_gemv for HMGen
+// (panel_gemv.hpp:362-388) drives the reference's kernels: b x b blocks above
+// the diagonal by hmg_gemv_up, below it by hmg_gemv_low, on it by
+// hmg_gemv_diag (otf_gemv.cpp:135-316), row blocks in parallel, the blocks of
+// a row block in column order.
+void ref_higham_gemv(int n, int b, double alpha, double beta, double a, const double *x, double *y) {
+    const int nb = n / b;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int pi = 0; pi < nb; ++pi)
+        for (int pj = 0; pj < nb; ++pj) {
+            if (pi < pj)
+                hmg_gemv_up(b * pi, alpha, beta, b, b, a, x + b * pj, y + b * pi);
+            else if (pi > pj)
+                hmg_gemv_low(b * pj, alpha, beta, b, b, a, x + b * pj, y + b * pi);
+            else
+                hmg_gemv_diag(b * pi, b * pj, alpha, beta, b, b, a, x + b * pj, y + b * pi);
+        }
 }
 }

@@ -25,7 +25,8 @@ def test_noalloc_gemv_matches_workspace_gemv_twice(mxp, orc, torch_cuda):
     L = mxp.lib()
     noalloc = _bind(L)
     stream = torch.cuda.current_stream().cuda_stream
-    cases = [(4096, 42, -1.0, 1.0), (122880, 7, 0.5, 0.0)]
+    # the largest n (two column splits fill the array exactly) and one just below it
+    cases = [(4096, 42, -1.0, 1.0), (122880, 7, 0.5, 0.0), (262144, 3, -1.0, 1.0), (262080, 11, 1.0, -0.5)]
     for n, seed, alpha, beta in cases:
         _, d, _, _ = orc.matgen(n, seed, with_matrix=False) if n <= 8192 else (None, None, None, None)
         if d is None:
