@@ -13,9 +13,12 @@ N = 10240 is one full group of four panels; N = 12800 is a group plus a
 one-panel tail.  Bars: relative Frobenius distance <= 1e-3 (the north-star
 bar for the FP16 forms) overall and on the strict lower and upper parts, and
 element-wise: every entry of a strict part within 1e-3 of that part's
-largest entry.  The low-precision panel copies the Schur update reads are
-checked byte for byte against the oracle's casts of the factors' FP32
-panels."""
+largest entry for the split-BF16 TRSM, within 2 * 2^-8 of it for the single
+BF16 product (the GPU and the oracle reach each operand through different
+Schur summation orders, so the same entry may round to neighbouring BF16
+values: one BF16 ulp, 2^-8 relative, in each of the two operands).  The
+low-precision panel copies the Schur update reads are checked byte for byte
+against the oracle's casts of the factors' FP32 panels."""
 import numpy as np
 import pytest
 
@@ -25,6 +28,7 @@ from tests.gpu_util import panel_slot, rel_fro, to_np_colmajor
 pytestmark = pytest.mark.gpu
 
 B = 2560
+ELEM_TOL = {"split": 1e-3, "single": 2.0 * 2.0 ** -8}
 ARMS = {  # name: (form, workspace trsm_single, oracle trsm)
     "fp16_split": (0, False, "split"),
     "fp8_single_fused": (2, True, "single"),
@@ -61,7 +65,7 @@ def test_factors_b2560(mxp, orc, torch_cuda, arm, n, seed):
     for part in (low, up):
         g, w = got[part].astype(np.float64), A[part].astype(np.float64)
         assert rel_fro(g, w) <= 1e-3
-        assert np.max(np.abs(g - w)) <= 1e-3 * np.max(np.abs(w))
+        assert np.max(np.abs(g - w)) <= ELEM_TOL[trsm] * np.max(np.abs(w))
     # the diagonal (the U pivots) too, entry by entry
     dg, dw = np.diag(got).astype(np.float64), np.diag(A).astype(np.float64)
     assert np.max(np.abs(dg - dw) / np.abs(dw)) <= 1e-5
