@@ -381,6 +381,15 @@ mxp_status mxp_solve_host(int n, int b, uint64_t seed, float *d_A, int64_t lda, 
  * Blocking. */
 mxp_status mxp_infnorm(int n, const double *d_x, double *h_out, mxp_workspace *ws, void *stream);
 
+/* Self-check of the branch-free FP32 reciprocal the 64 x 64 diagonal LU uses
+ * for its pivots (no reference counterpart; the reference's sgetrf_nopiv_naive
+ * divides by the pivot, sgetrf_nopiv.cpp:27-61, which is the same correctly
+ * rounded value): compares it bit for bit with the CUDA runtime's IEEE
+ * round-to-nearest reciprocal on 2 x 254 x 65536 normal inputs (every sign and
+ * exponent, mantissas spread over the range plus the extremes).  h_mismatches
+ * and h_checked receive the counts.  Blocking. */
+mxp_status mxp_check_reciprocal(uint64_t *h_mismatches, uint64_t *h_checked);
+
 /* Number of tcgen05 / other kernels this library launched on the calling
  * thread since the last reset (for launch accounting in benchmarks). */
 int64_t mxp_kernel_launches(void);

@@ -109,6 +109,7 @@ _SIGS = {
     "mxp_solve_host": (_i32, [_i32, _i32, _u64, _vp, _i64, _vp, _vp, _vp, _vp, _i32, _i32, _vp,
                               _vp, C.POINTER(LuStats), C.POINTER(IrStats)]),
     "mxp_infnorm": (_i32, [_i32, _vp, C.POINTER(_dbl), _vp, _vp]),
+    "mxp_check_reciprocal": (_i32, [C.POINTER(_u64), C.POINTER(_u64)]),
     "mxp_batch_sizes": (_i32, [_i32, _u64, C.POINTER(C.c_int)]),
     "mxp_batch_partition": (_i32, [_i32, C.POINTER(C.c_int), _i32, C.POINTER(C.c_int)]),
     "mxp_batch_create": (_i32, [_i32, C.POINTER(C.c_int), C.POINTER(C.c_uint64), _i32, C.POINTER(_vp)]),
@@ -433,6 +434,14 @@ def infnorm(x, ws: Workspace, stream=None) -> float:
     out = C.c_double(0.0)
     check(lib().mxp_infnorm(x.numel(), _ptr(x), C.byref(out), ws.handle, _stream(stream)))
     return out.value
+
+
+def check_reciprocal() -> tuple[int, int]:
+    """(mismatches, inputs checked) of the library's branch-free FP32
+    reciprocal against the CUDA runtime's IEEE reciprocal (mxp_check_reciprocal)."""
+    bad, n = _u64(0), _u64(0)
+    check(lib().mxp_check_reciprocal(C.byref(bad), C.byref(n)))
+    return int(bad.value), int(n.value)
 
 
 def kernel_launches() -> int:

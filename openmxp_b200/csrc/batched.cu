@@ -127,37 +127,25 @@ __device__ __forceinline__ void stage_zero_row(uint8_t *base, int nblk, int row,
 }
 
 // U-strip columns [c0, c0 + 256) of B (nb x ncols): X = L^{-1} B with L the unit
-// lower part of sm.t.  The 64 x 256 block goes through shared memory (stage:
-// 256 x 65 floats) with coalesced loads and stores; thread j solves column j.
+// lower part of the diagonal block (load_tri).  The 64 x 256 block goes
+// through shared memory (stage: 256 x 65 floats) with coalesced loads and
+// stores; thread j solves column j.
 constexpr size_t kColStageOff = 65536;  // after the Smem union
 constexpr size_t kColStageBytes = sizeof(float) * kCT * (kNB + 1);
 
 __device__ void trsm_cols_staged(Smem &sm, float *stage, int ncols, int nb, float *B, int64_t ldb, int c0) {
+#pragma unroll 16
     for (int idx = threadIdx.x; idx < kNB * kCT; idx += kCT) {
         const int k = idx % kNB, j = idx / kNB;
         stage[j * (kNB + 1) + k] = (k < nb && c0 + j < ncols) ? __ldcg(B + (int64_t)(c0 + j) * ldb + k) : 0.0f;
     }
     __syncthreads();
-    {  // right-looking: x_r -= l_rk x_k for r > k (l_.k contiguous in sm.t)
+    {  // right-looking: x_r -= l_rk x_k for r > k, rotated (trsm_col)
         const int j = threadIdx.x;
         float x[kNB];
 #pragma unroll
         for (int k = 0; k < kNB; ++k) x[k] = stage[j * (kNB + 1) + k];
-#pragma unroll
-        for (int k = 0; k < kNB - 1; ++k) {
-            if (k < nb) {
-#pragma unroll
-                for (int r4 = (k + 1) / 4; r4 < kNB / 4; ++r4) {
-                    const float4 l = *reinterpret_cast<const float4 *>(&sm.t.t[k][4 * r4]);
-                    if (4 * r4 + 0 > k) x[4 * r4 + 0] = fmaf(-l.x, x[k], x[4 * r4 + 0]);
-                    if (4 * r4 + 1 > k) x[4 * r4 + 1] = fmaf(-l.y, x[k], x[4 * r4 + 1]);
-                    if (4 * r4 + 2 > k) x[4 * r4 + 2] = fmaf(-l.z, x[k], x[4 * r4 + 2]);
-                    if (4 * r4 + 3 > k) x[4 * r4 + 3] = fmaf(-l.w, x[k], x[4 * r4 + 3]);
-                }
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kNB; ++k) stage[j * (kNB + 1) + k] = x[k];
+        trsm_col(sm, x, nb, stage + j * (kNB + 1));
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < kNB * kCT; idx += kCT) {

@@ -21,17 +21,59 @@ struct SmemGemm {
     float Bs[GBK][GBN + 4];
 };
 struct __align__(16) SmemTri {
-    float t[kNB][kNB + 4];   // t[col][row] of a 64 x 64 block (16-byte rows)
-    float tt[kNB][kNB + 4];  // tt[row][col]: the same block row-major
-    float ub[kNB][kNB + 1];  // staging of 64 U-strip columns, ub[col][row]
-    float prow[2][kNB];      // pivot row of the 64 x 64 LU, zero left of the pivot
+    union {
+        float t[kNB][kNB + 4];   // t[col][row] of a 64 x 64 block (16-byte rows)
+        float ub[kNB][kNB + 1];  // staging of 64 U-strip columns, ub[col][row] (t is dead by then)
+    };
+    float us[kNB][kNB];      // us[k][c] = U(k, k + 1 + c): row k of U right of the diagonal, zero past the block
+    float ls[kNB][kNB];      // ls[k][c] = L(k + 1 + c, k): column k of L below the diagonal, zero past the block
     float dinv[kNB];
-    float pivv[2];
+};
+struct __align__(16) SmemG64 {  // one 64 x 64 x 64 product staged whole
+    float As[kNB][kNB];       // As[k][row]
+    float Bs[kNB][kNB + 4];   // Bs[k][col]
 };
 union __align__(16) Smem {
     SmemGemm g;
     SmemTri t;
+    SmemG64 g64;
 };
+
+// A 64 x 64 block (rows r < nb, columns c < nb; zero elsewhere) from global
+// memory through L2 into registers: 16 values per thread, element q at
+// column (threadIdx.x + 256 q) / 64, row (threadIdx.x + 256 q) % 64.  All 16
+// loads are issued before any is used, so the block costs one L2 round trip.
+static_assert(kCT * 16 == kNB * kNB, "64 x 64 block = 16 values per thread");
+__device__ __forceinline__ void load_block64(float (&v)[16], const float *D, int64_t ld, int nr, int nc) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int idx = threadIdx.x + kCT * q;
+        const int r = idx % kNB, c = idx / kNB;
+        v[q] = (r < nr && c < nc) ? __ldcg(D + (int64_t)c * ld + r) : 0.0f;
+    }
+}
+
+// One pivot of a right-looking elimination on a row held in registers that
+// moves left by one column per pivot: x[c] = x[c + 1] - s[c] * v for c < W - 1,
+// x[W - 1] = 0.  With x[0] the pivot column and s the pivot row (or column)
+// right of the diagonal, this is x_j -= s_j v for j > k in the same operation
+// (one fmaf) as the unrotated loop, but every pivot runs the same code, so the
+// pivot loop stays rolled: fully unrolled 64-pivot eliminations are thousands
+// of straight-line instructions, and their instruction fetch, not the FMA
+// pipe, set their speed (~8-10 cycles per instruction in a per-step trace).
+// W (the live width, 64 - 16 p in phase p of a 64-wide elimination) skips the
+// columns the rotation has already emptied.  s is 16-byte aligned.
+template <int W>
+__device__ __forceinline__ void rot_axpy(float (&x)[kNB], const float *s, float v) {
+#pragma unroll
+    for (int c4 = 0; c4 < W / 4; ++c4) {
+        const float4 u = *reinterpret_cast<const float4 *>(s + 4 * c4);
+        x[4 * c4 + 0] = fmaf(-u.x, v, x[4 * c4 + 1]);
+        x[4 * c4 + 1] = fmaf(-u.y, v, x[4 * c4 + 2]);
+        x[4 * c4 + 2] = fmaf(-u.z, v, x[4 * c4 + 3]);
+        x[4 * c4 + 3] = (4 * c4 + 4 < W) ? fmaf(-u.w, v, x[4 * c4 + 4]) : 0.0f;
+    }
+}
 
 
 // ---- 128 x 128 SIMT GEMM tile ------------------------------------------------
@@ -141,23 +183,29 @@ __device__ void gemm_tile64(Smem &sm, int m, int n, int k, float alpha, const fl
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
-    for (int k0 = 0; k0 < k; k0 += GBK) {
-        __syncthreads();
+    for (int k0 = 0; k0 < k; k0 += kNB) {
+        // the whole 64-deep slice of both operands in one L2 round trip
+        const int kc = min(kNB, k - k0);
+        float va[16], vb[16];
+        load_block64(va, A + (int64_t)k0 * lda, lda, m, kc);  // va: A(r, k0 + c)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int idx = t + kCT * q;           // 0..1023
-            const int kk = idx / 64, r = idx % 64;
-            const int gk = k0 + kk;
-            sm.g.As[kk][r] = (r < m && gk < k) ? __ldcg(A + (int64_t)gk * lda + r) : 0.0f;
-            const int c = idx / GBK, kb = idx % GBK;
-            const int gkb = k0 + kb;
-            sm.g.Bs[kb][c] = (c < n && gkb < k) ? __ldcg(B + (int64_t)c * ldb + gkb) : 0.0f;
+        for (int q = 0; q < 16; ++q) {  // vb: B(k0 + kk, c), kk fastest
+            const int idx = t + kCT * q;
+            const int kk = idx % kNB, c = idx / kNB;
+            vb[q] = (kk < kc && c < n) ? __ldcg(B + (int64_t)c * ldb + k0 + kk) : 0.0f;
         }
         __syncthreads();
 #pragma unroll
-        for (int kk = 0; kk < GBK; ++kk) {
-            const float4 a = *reinterpret_cast<const float4 *>(&sm.g.As[kk][tx * 4]);
-            const float4 b = *reinterpret_cast<const float4 *>(&sm.g.Bs[kk][ty * 4]);
+        for (int q = 0; q < 16; ++q) {
+            const int idx = t + kCT * q;
+            sm.g64.As[idx / kNB][idx % kNB] = va[q];
+            sm.g64.Bs[idx % kNB][idx / kNB] = vb[q];
+        }
+        __syncthreads();
+#pragma unroll 16
+        for (int kk = 0; kk < kNB; ++kk) {
+            const float4 a = *reinterpret_cast<const float4 *>(&sm.g64.As[kk][tx * 4]);
+            const float4 b = *reinterpret_cast<const float4 *>(&sm.g64.Bs[kk][ty * 4]);
             const float av[4] = {a.x, a.y, a.z, a.w};
             const float bv[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
@@ -188,134 +236,182 @@ __device__ void gemm_tile64(Smem &sm, int m, int n, int k, float alpha, const fl
     __syncthreads();
 }
 
-// ---- 64 x 64 no-pivot LU of D (nb <= 64), one row per thread of warps 0-1 ----
+// ---- 64 x 64 no-pivot LU of D (nb <= 64), warp 0 alone --------------------------
 // sgetrf_nopiv_naive order (sgetrf_nopiv.cpp:27-61): scale by the reciprocal
-// pivot, then the rank-1 update.  The two working warps meet at a 64-thread
-// named barrier once per pivot; the rest of the CTA waits at the final
-// __syncthreads.
-__device__ __forceinline__ void bar_sync_rows() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
+// pivot, then the rank-1 update.  Lane l keeps rows l and l + 32 in
+// registers, each rotated (rot_axpy's scheme): at pivot k an active row holds
+// A(r, k ..) from index 0.  Per pivot, the lane owning row k hands its row to
+// the others by register shuffles (no barrier, no shared-memory round trip);
+// each active row forms its multiplier, updates the column that holds the
+// next pivot first, and the next pivot's reciprocal (rcp_rn_f32, branch-free)
+// is issued at once so its latency overlaps the rest of the row update.
+// Multipliers (column k of L) go to shared memory as they are formed; a row
+// stops rotating at its own pivot, so at the end each lane holds its rows of
+// U; the CTA then stores the block.  Timed alone in one CTA (clock64, 64 x 64):
+// 27.3 k cycles against 40 k for one row per thread of two warps with a named
+// barrier per pivot; the shuffles (~4 issue cycles each) and the per-pivot
+// chain (shuffle, reciprocal, multiply, update) set the pace.
+template <int W, bool TOP>
+__device__ __forceinline__ void getrf64_phase(float (*T)[kNB + 4], float (&a0)[kNB], float (&a1)[kNB], float &pv,
+                                              float &rp, int k0, int k1, int nb, DevStatus *dst, int pivot_base) {
+    const int ln = threadIdx.x;
+    const unsigned full = 0xffffffffu;
+#pragma unroll 1
+    for (int k = k0; k < k1; ++k) {
+        if (ln == 0 && (!(pv != 0.0f) || !isfinite(pv))) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
+        const int src = k & 31;  // row k: a0 of lane src (k < 32), else a1
+        const bool act0 = TOP && ln > k && ln < nb, act1 = ln + 32 > k && ln + 32 < nb;
+        const float l0 = act0 ? a0[0] * rp : 0.0f;
+        const float l1 = act1 ? a1[0] * rp : 0.0f;
+        const float u0 = __shfl_sync(full, TOP ? a0[1] : a1[1], src);
+        if (act0) a0[0] = fmaf(-u0, l0, a0[1]);
+        if (act1) a1[0] = fmaf(-u0, l1, a1[1]);
+        {  // the next pivot is final now (past the last pivot the value is not used)
+            const int kn = k + 1;
+            pv = __shfl_sync(full, kn < 32 ? a0[0] : a1[0], kn & 31);
+            rp = rcp_rn_f32(pv);
+        }
+        if (act0) T[k][ln] = l0;
+        if (act1) T[k][ln + 32] = l1;
+#pragma unroll
+        for (int c = 1; c < W - 1; ++c) {
+            const float u = __shfl_sync(full, TOP ? a0[c + 1] : a1[c + 1], src);
+            if (act0) a0[c] = fmaf(-u, l0, a0[c + 1]);
+            if (act1) a1[c] = fmaf(-u, l1, a1[c + 1]);
+        }
+        if (act0) a0[W - 1] = 0.0f;
+        if (act1) a1[W - 1] = 0.0f;
+    }
+}
 
-__device__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, DevStatus *dst, int pivot_base) {
-    const int i = threadIdx.x;
-    if (i < kNB) {
-        float a[kNB];
+__device__ __noinline__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, DevStatus *dst, int pivot_base) {
+    float(*T)[kNB + 4] = sm.t.t;  // T[c][r]: the factored block, written out at the end
+    if (threadIdx.x < 32) {
+        const int ln = threadIdx.x;
+        float a0[kNB], a1[kNB];
 #pragma unroll
-        for (int j = 0; j < kNB; ++j) a[j] = (i < nb && j < nb) ? __ldcg(D + (int64_t)j * lda + i) : 0.0f;
-#pragma unroll
-        for (int k = 0; k < kNB; ++k) {
-            if (k < nb) {  // uniform
-                float *pr = sm.t.prow[k & 1];
-                if (i == k) {  // publish the pivot row, zero at and left of the pivot
-#pragma unroll
-                    for (int j4 = k / 4; j4 < kNB / 4; ++j4) {
-                        float4 v;
-                        v.x = (4 * j4 + 0 > k) ? a[4 * j4 + 0] : 0.0f;
-                        v.y = (4 * j4 + 1 > k) ? a[4 * j4 + 1] : 0.0f;
-                        v.z = (4 * j4 + 2 > k) ? a[4 * j4 + 2] : 0.0f;
-                        v.w = (4 * j4 + 3 > k) ? a[4 * j4 + 3] : 0.0f;
-                        *reinterpret_cast<float4 *>(pr + 4 * j4) = v;
-                    }
-                    sm.t.pivv[k & 1] = a[k];
-                }
-                bar_sync_rows();
-                const float piv = sm.t.pivv[k & 1];
-                if (i == k && (!(piv != 0.0f) || !isfinite(piv))) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
-                const bool act = i > k && i < nb;
-                const float l = act ? a[k] * __frcp_rn(piv) : 0.0f;
-                if (act) a[k] = l;
-                // a(i, j) -= l * u(k, j) for j > k; the zeros of the published row
-                // leave columns <= k untouched (and rows <= k have l = 0)
-#pragma unroll
-                for (int j4 = k / 4; j4 < kNB / 4; ++j4) {
-                    const float4 p = *reinterpret_cast<const float4 *>(pr + 4 * j4);
-                    if (4 * j4 + 0 > k) a[4 * j4 + 0] = fmaf(-l, p.x, a[4 * j4 + 0]);
-                    if (4 * j4 + 1 > k) a[4 * j4 + 1] = fmaf(-l, p.y, a[4 * j4 + 1]);
-                    if (4 * j4 + 2 > k) a[4 * j4 + 2] = fmaf(-l, p.z, a[4 * j4 + 2]);
-                    if (4 * j4 + 3 > k) a[4 * j4 + 3] = fmaf(-l, p.w, a[4 * j4 + 3]);
-                }
-            }
+        for (int j = 0; j < kNB; ++j) {
+            a0[j] = (j < nb && ln < nb) ? __ldcg(D + (int64_t)j * lda + ln) : 0.0f;
+            a1[j] = (j < nb && ln + 32 < nb) ? __ldcg(D + (int64_t)j * lda + ln + 32) : 0.0f;
         }
-        if (i < nb) {
+        float pv = __shfl_sync(0xffffffffu, a0[0], 0);
+        float rp = rcp_rn_f32(pv);
+        getrf64_phase<64, true>(T, a0, a1, pv, rp, 0, min(nb, 16), nb, dst, pivot_base);
+        getrf64_phase<48, true>(T, a0, a1, pv, rp, 16, min(nb, 32), nb, dst, pivot_base);
+        getrf64_phase<32, false>(T, a0, a1, pv, rp, 32, min(nb, 48), nb, dst, pivot_base);
+        getrf64_phase<16, false>(T, a0, a1, pv, rp, 48, nb, nb, dst, pivot_base);
+        // rows of U: frozen in the registers since their own pivot, a[c] = U(r, r + c)
 #pragma unroll
-            for (int j = 0; j < kNB; ++j)
-                if (j < nb) D[(int64_t)j * lda + i] = a[j];
+        for (int c = 0; c < kNB; ++c) {
+            if (ln < nb && ln + c < nb) T[ln + c][ln] = a0[c];
+            if (ln + 32 < nb && ln + 32 + c < nb) T[ln + 32 + c][ln + 32] = a1[c];
         }
+    }
+    __syncthreads();
+    // the whole block in one coalesced pass: shared-memory stores inside the
+    // pivot loop instead of ~250 scattered global stores, which stalled the
+    // factor under the L2 traffic of the trailing update running beside it
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int idx = threadIdx.x + kCT * q;
+        const int r = idx % kNB, c = idx / kNB;
+        if (r < nb && c < nb) D[(int64_t)c * lda + r] = T[c][r];
     }
     __syncthreads();
 }
 
-// D (nb x nb, factored) into shared memory, t[col][row], plus reciprocal diagonal.
+// D (nb x nb, factored) into shared memory: t[col][row], the skewed rows of U
+// and columns of L the rotated strip solves read (us, ls), and the reciprocal
+// diagonal.
 __device__ void load_tri(Smem &sm, int nb, const float *D, int64_t lda) {
-    for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
-        const int r = idx % kNB, c = idx / kNB;
-        const float v = (r < nb && c < nb) ? __ldcg(D + (int64_t)c * lda + r) : 0.0f;
-        sm.t.t[c][r] = v;
-        sm.t.tt[r][c] = v;
+    float v[16];
+    load_block64(v, D, lda, nb, nb);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int idx = threadIdx.x + kCT * q;
+        sm.t.t[idx / kNB][idx % kNB] = v[q];
     }
     __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int idx = threadIdx.x + kCT * q;
+        const int k = idx / kNB, c = idx % kNB, j = k + 1 + c;
+        sm.t.us[k][c] = j < nb ? sm.t.t[j][k] : 0.0f;
+        sm.t.ls[k][c] = j < nb ? sm.t.t[k][j] : 0.0f;
+    }
     if (threadIdx.x < nb) sm.t.dinv[threadIdx.x] = 1.0f / sm.t.t[threadIdx.x][threadIdx.x];
     __syncthreads();
 }
 
 // L strip rows [r0, r0 + rows) of B (m x nb), rows <= kCT: X = B U^{-1}, U =
-// upper part of the diagonal block in sm.t.  Right-looking (x_k final, then
-// x_c -= u_kc x_k for c > k): per element the same operations in the same
-// order as the dot-product form, with independent updates instead of one
-// dependent chain per row; u_k. is read four at a time from the row-major copy.
+// upper part of the diagonal block (load_tri).  Right-looking, thread per row
+// (x_k final, then x_c -= u_kc x_k for c > k): per element the same
+// operations in the same order as the dot-product form; the row rotates
+// (rot_axpy) so the pivot loop stays rolled, and x_k is stored as soon as it
+// is final.
+template <int W>
+__device__ __forceinline__ void trsm_rows_phase(Smem &sm, float (&x)[kNB], int k0, int k1, float *B, int64_t ldb,
+                                                int i) {
+#pragma unroll 1
+    for (int k = k0; k < k1; ++k) {
+        const float xk = x[0] * sm.t.dinv[k];
+        B[(int64_t)k * ldb + i] = xk;
+        rot_axpy<W>(x, &sm.t.us[k][0], xk);
+    }
+}
+
 __device__ void trsm_rows(Smem &sm, int m, int nb, float *B, int64_t ldb, int r0, int rows = kCT) {
     const int i = r0 + threadIdx.x;
     if (threadIdx.x >= rows || i >= m) return;
     float x[kNB];
 #pragma unroll
     for (int c = 0; c < kNB; ++c) x[c] = (c < nb) ? __ldcg(B + (int64_t)c * ldb + i) : 0.0f;
-#pragma unroll
-    for (int k = 0; k < kNB; ++k) {
-        if (k < nb) {
-            x[k] *= sm.t.dinv[k];
-#pragma unroll
-            for (int c4 = (k + 1) / 4; c4 < kNB / 4; ++c4) {
-                const float4 u = *reinterpret_cast<const float4 *>(&sm.t.tt[k][4 * c4]);
-                if (4 * c4 + 0 > k) x[4 * c4 + 0] = fmaf(-u.x, x[k], x[4 * c4 + 0]);
-                if (4 * c4 + 1 > k) x[4 * c4 + 1] = fmaf(-u.y, x[k], x[4 * c4 + 1]);
-                if (4 * c4 + 2 > k) x[4 * c4 + 2] = fmaf(-u.z, x[k], x[4 * c4 + 2]);
-                if (4 * c4 + 3 > k) x[4 * c4 + 3] = fmaf(-u.w, x[k], x[4 * c4 + 3]);
-            }
-        }
+    trsm_rows_phase<64>(sm, x, 0, min(nb, 16), B, ldb, i);
+    trsm_rows_phase<48>(sm, x, 16, min(nb, 32), B, ldb, i);
+    trsm_rows_phase<32>(sm, x, 32, min(nb, 48), B, ldb, i);
+    trsm_rows_phase<16>(sm, x, 48, nb, B, ldb, i);
+}
+
+// One column of X = L^{-1} B (L unit lower, load_tri) in registers: x_r -=
+// l_rk x_k for r > k, rotated; x_k goes to out[k] as soon as it is final.
+template <int W>
+__device__ __forceinline__ void trsm_col_phase(Smem &sm, float (&x)[kNB], int k0, int k1, float *out) {
+#pragma unroll 1
+    for (int k = k0; k < k1; ++k) {
+        const float xk = x[0];
+        out[k] = xk;
+        rot_axpy<W>(x, &sm.t.ls[k][0], xk);
     }
-#pragma unroll
-    for (int c = 0; c < kNB; ++c)
-        if (c < nb) B[(int64_t)c * ldb + i] = x[c];
+}
+
+__device__ __forceinline__ void trsm_col(Smem &sm, float (&x)[kNB], int nb, float *out) {
+    trsm_col_phase<64>(sm, x, 0, min(nb, 16), out);
+    trsm_col_phase<48>(sm, x, 16, min(nb, 32), out);
+    trsm_col_phase<32>(sm, x, 32, min(nb, 48), out);
+    trsm_col_phase<16>(sm, x, 48, nb, out);
 }
 
 // U strip columns [c0, c0 + 64) of B (nb x ncols): X = L^{-1} B, L = unit lower
-// part of sm.t.  The 64 x 64 block moves through shared memory with coalesced
-// loads and stores; threads 0..63 solve one column each.
+// part of the diagonal block (load_tri).  The 64 x 64 block moves through
+// shared memory (ub, over the dead t) with coalesced loads and stores;
+// threads 0..63 solve one column each.
 __device__ void trsm_cols64(Smem &sm, int ncols, int nb, float *B, int64_t ldb, int c0) {
-    for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
-        const int k = idx % kNB, j = idx / kNB;
-        sm.t.ub[j][k] = (k < nb && c0 + j < ncols) ? __ldcg(B + (int64_t)(c0 + j) * ldb + k) : 0.0f;
+    {
+        float v[16];
+        load_block64(v, B + (int64_t)c0 * ldb, ldb, nb, ncols - c0);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int idx = threadIdx.x + kCT * q;
+            sm.t.ub[idx / kNB][idx % kNB] = v[q];
+        }
     }
     __syncthreads();
-    if (threadIdx.x < kNB) {  // right-looking: x_r -= l_rk x_k for r > k (l_.k contiguous in sm.t)
+    if (threadIdx.x < kNB) {
         const int j = threadIdx.x;
         float x[kNB];
 #pragma unroll
         for (int k = 0; k < kNB; ++k) x[k] = sm.t.ub[j][k];
-#pragma unroll
-        for (int k = 0; k < kNB - 1; ++k) {
-            if (k < nb) {
-#pragma unroll
-                for (int r4 = (k + 1) / 4; r4 < kNB / 4; ++r4) {
-                    const float4 l = *reinterpret_cast<const float4 *>(&sm.t.t[k][4 * r4]);
-                    if (4 * r4 + 0 > k) x[4 * r4 + 0] = fmaf(-l.x, x[k], x[4 * r4 + 0]);
-                    if (4 * r4 + 1 > k) x[4 * r4 + 1] = fmaf(-l.y, x[k], x[4 * r4 + 1]);
-                    if (4 * r4 + 2 > k) x[4 * r4 + 2] = fmaf(-l.z, x[k], x[4 * r4 + 2]);
-                    if (4 * r4 + 3 > k) x[4 * r4 + 3] = fmaf(-l.w, x[k], x[4 * r4 + 3]);
-                }
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kNB; ++k) sm.t.ub[j][k] = x[k];
+        trsm_col(sm, x, nb, &sm.t.ub[j][0]);
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
@@ -331,9 +427,14 @@ __device__ void inv_diag_block(Smem &sm, int n, const float *T, int64_t ldt, flo
                                int blk, bool upper) {
     const int r0 = blk * kNB;
     const int nb = min(kNB, n - r0);
-    for (int idx = threadIdx.x; idx < kNB * kNB; idx += kCT) {
-        const int r = idx % kNB, c = idx / kNB;
-        sm.t.t[c][r] = (r < nb && c < nb) ? __ldcg(T + (int64_t)(r0 + c) * ldt + r0 + r) : 0.0f;
+    {
+        float v[16];
+        load_block64(v, T + r0 + (int64_t)r0 * ldt, ldt, nb, nb);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int idx = threadIdx.x + kCT * q;
+            sm.t.t[idx / kNB][idx % kNB] = v[q];
+        }
     }
     __syncthreads();
     const int i = threadIdx.x;

@@ -157,7 +157,45 @@ int coop_grid(int device) {
     return cached[device];
 }
 
+// rcp_rn_f32 against the runtime's IEEE reciprocal: sign (bit 0 of i),
+// exponent 1..254 and 65536 mantissas per exponent (the extremes near 0 and
+// near 0x7fffff, the rest spread by a multiplicative hash).
+__global__ void check_reciprocal_kernel(unsigned long long *counts) {
+    unsigned long long bad = 0, n = 0;
+    const unsigned total = 2u * 254u * 65536u;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const unsigned sign = (i & 1u) << 31;
+        const unsigned e = 1u + (i >> 1) % 254u;
+        const unsigned q = (i >> 1) / 254u;
+        const unsigned mant = q < 64 ? (q == 0 ? 0u : 0x7fffffu - (q - 1)) : (q * 2654435761u) & 0x7fffffu;
+        const float x = __uint_as_float(sign | (e << 23) | mant);
+        ++n;
+        if (__float_as_uint(__frcp_rn(x)) != __float_as_uint(rcp_rn_f32(x))) ++bad;
+    }
+    atomicAdd(counts, bad);
+    atomicAdd(counts + 1, n);
+}
+
 }  // namespace
+
+extern "C" mxp_status mxp_check_reciprocal(uint64_t *h_mismatches, uint64_t *h_checked) {
+    if (!h_mismatches || !h_checked) return fail(MXP_INVALID_ARG, "check_reciprocal: NULL argument");
+    unsigned long long *d = nullptr;
+    MXP_CUDA(cudaMalloc(&d, 2 * sizeof(unsigned long long)));
+    unsigned long long h[2] = {0, 0};
+    cudaError_t e = cudaMemset(d, 0, sizeof(h));
+    if (e == cudaSuccess) {
+        check_reciprocal_kernel<<<1184, 256>>>(d);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) count_launch();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "check_reciprocal");
+    *h_mismatches = h[0];
+    *h_checked = h[1];
+    return MXP_OK;
+}
 
 size_t diag_factor_tmp_floats(int n) { return (size_t)n * n / 2 + (size_t)64 * n; }
 

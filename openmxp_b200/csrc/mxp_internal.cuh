@@ -57,6 +57,29 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
+
+// Round-to-nearest FP32 reciprocal without a branch: the hardware FP64
+// approximation (rcp.approx.ftz.f64) refined by two Newton-Raphson steps
+// r += r (1 - x r) in FP64, then rounded once to FP32.  For a normal FP32 x,
+// 1/x is never exactly halfway between two FP32 values and never closer to
+// such a point than about 2^-49 (relative), while the refined FP64 value is
+// within about 2^-52 of 1/x, so the single rounding gives the correctly
+// rounded reciprocal.  It serves where the reciprocal is
+// on a latency chain: the IEEE reciprocal of the CUDA runtime takes a
+// data-dependent branch that keeps later independent instructions from being
+// issued ahead of it.  Checked bit for bit against that reciprocal by
+// mxp_check_reciprocal.  Zero, infinite and NaN inputs give NaN (callers
+// report such pivots as errors).
+__device__ __forceinline__ float rcp_rn_f32(float x) {
+    const double d = (double)x;
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+    double e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    return __double2float_rn(r);
+}
 #endif
 
 // ---------------------------------------------------------------------------

@@ -131,3 +131,13 @@ def test_inv_tc_option_bounds(mxp, torch_cuda):
         with pytest.raises(mxp.MxpError):
             ws.set_option(mxp.OPT_INV_TC, bad)
     ws.set_option(mxp.OPT_INV_TC, 0)
+
+
+def test_branch_free_reciprocal(mxp, torch_cuda):
+    """The 64 x 64 LU forms its multipliers with a branch-free FP32 reciprocal
+    (FP64 Newton steps from the hardware approximation, rounded once); it must
+    equal the CUDA runtime's IEEE round-to-nearest reciprocal bit for bit on
+    every normal input checked (all signs and exponents, 65536 mantissas each)."""
+    bad, n = mxp.check_reciprocal()
+    assert n == 2 * 254 * 65536
+    assert bad == 0
