@@ -719,6 +719,92 @@ def run_batched(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# one system over a P x Q grid of GPUs (2D block-cyclic driver, strong scaling)
+# ---------------------------------------------------------------------------
+def run_grid(args):
+    """Credited TFLOP/s of ONE system of order --n factored and refined by a
+    P x Q grid of GPUs (openmxp_b200.grid: block-cyclic layout, the factored
+    diagonal block and the low-precision panels broadcast over NCCL along
+    process rows and columns, STRSM panels, tcgen05 Schur update, refinement
+    with the local regenerating GEMV summed over all ranks).  One step = one
+    solve of the freshly regenerated local blocks; the time is LU +
+    refinement, max over ranks."""
+    import torch
+
+    import openmxp_b200 as mxp
+    from openmxp_b200 import grid as G
+    P, Q = (int(v) for v in args.grid.lower().split("x"))
+    world, rank, local = dist_env()
+    if P * Q != world:
+        raise SystemExit(f"--grid {args.grid} needs {P * Q} ranks, got {world}")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = init_dist("nccl") if world > 1 else None
+    form = mxp.FORMS[args.form]
+    g = G.ProcessGrid(P, Q, dist=dist)
+    be = G.CudaBackend(args.b, form)
+    s = G.BlockCyclicSolver(g, args.n, args.b, args.seed, be, form=form, diag_rule=args.diag_rule)
+    h_rhs = s.rhs.cpu().pin_memory()
+    h_x = torch.empty(args.n, dtype=torch.float64).pin_memory()
+
+    def step(e2e: bool):
+        s.regenerate()
+        torch.cuda.synchronize()
+        barrier(dist)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        if e2e:
+            s.rhs.copy_(h_rhs, non_blocking=True)
+        s.factor()
+        x, st = s.refine(maxit=args.maxit)
+        if e2e:
+            h_x.copy_(x, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), dist, dev), st
+
+    for _ in range(args.warmup):
+        step(False)
+    clocks = ClockSampler(local)
+    clocks.start()
+    mxp.reset_kernel_launches()
+    ms, st = [], None
+    for _ in range(args.steps):
+        t, st = step(False)
+        ms.append(t)
+    launches = int(sum_over_ranks(mxp.kernel_launches(), dist, dev))
+    clk = clocks.stop()
+    e2e_ms = [step(True)[0] for _ in range(max(1, args.e2e_steps))]
+    flops = hpl_flops(args.n)
+    t = sum(ms) / len(ms) / 1e3
+    te = sum(e2e_ms) / len(e2e_ms) / 1e3
+    out = {"metric": METRIC, "value": flops / t / 1e12, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "strong",
+           "vs_baseline": None, "dtype": {"fp16": "f16", "bf16x2": "bf16", "fp8": "e4m3"}[args.form],
+           "data": "synthetic (HPL-MxP LCG generator; generation excluded from t)",
+           "config": {"workload": f"HPL-MxP solve N={args.n} B={args.b} seed={args.seed} {args.form}-Schur + "
+                                  f"FP64 classic IR over a {P}x{Q} process grid (2D block-cyclic)",
+                      "n": args.n, "b": args.b, "seed": args.seed, "form": args.form, "grid": f"{P}x{Q}",
+                      "parallelism": f"2D block-cyclic {P}x{Q}, NCCL broadcasts of the factored diagonal "
+                                     "block and the low-precision panels",
+                      "trsm": "STRSM (SIMT FP32) on the local panels",
+                      "l2": "inputs larger than L2" if args.n * args.n * 4 // world > 126e6 else "fits L2"},
+           "ir": {"iterations": st.iterations, "converged": int(st.converged), "hpl_harness": st.hpl_harness,
+                  "residual": st.residual},
+           "e2e": {"value": flops / te / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": 8 * args.n,
+                   "d2h_bytes_per_step": 8 * args.n,
+                   "api": "BlockCyclicSolver.factor + refine, pinned host rhs in / x out on every rank"},
+           "gpu_launches": launches, "clocks": clk}
+    be.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    barrier(dist)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def parse(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -774,6 +860,9 @@ def parse(argv=None):
     ap.add_argument("--batch-config", default="", help="b,tile_n,stages (default: autotune)")
     ap.add_argument("--batch-loop-sample", type=int, default=128,
                     help="systems timed through the per-system loop for comparison")
+    ap.add_argument("--grid", default="",
+                    help="PxQ: solve ONE system over a P x Q grid of GPUs (2D block-cyclic; launch "
+                         "P*Q ranks with torchrun); strong scaling")
     ap.add_argument("--distinct-seeds", action="store_true",
                     help="rank r solves seed+r instead of the same system")
     return ap.parse_args(argv)
@@ -791,6 +880,8 @@ def main(argv=None):
         return run_micro(args)
     if args.batched:
         return run_batched(args)
+    if args.grid:
+        return run_grid(args)
     return run_gpu(args)
 
 

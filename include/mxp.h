@@ -395,6 +395,37 @@ mxp_status mxp_check_reciprocal(uint64_t *h_mismatches, uint64_t *h_checked);
 int64_t mxp_kernel_launches(void);
 void mxp_reset_kernel_launches(void);
 
+/* ---- 2D block-cyclic process grid -----------------------------------------
+ * Device pieces of the multi-GPU driver (openmxp_b200/grid.py; the
+ * reference's panel_trf / iterative_refinement over a P x Q Grid, grid.hpp:
+ * 25-80): global b x b block (I, J) lives on process (I mod P, J mod Q), kept
+ * in one column-major local matrix at local block (I div P, J div Q).  The
+ * LU steps use the granular entry points above on local views. */
+
+/* Rows (or columns) of the local matrix of process coordinate me among nproc:
+ * b times the number of block indices I < n/b with I mod nproc == me. */
+mxp_status mxp_local_extent(int n, int b, int nproc, int me, int64_t *h_extent);
+
+/* panel_matgen_dev for one process of a P x Q grid (matgen.hpp:84-117): its
+ * local blocks of the generator matrix, bit-exact with mxp_matgen's, the
+ * diagonal A(i,i) = float(d_i) taken from d_d (all n entries, as mxp_matgen
+ * computes them).  lda >= the local row count. */
+mxp_status mxp_matgen_local(int n, int b, uint64_t seed, int nprow, int npcol, int myrow, int mycol,
+                            const double *d_d, float *d_A, int64_t lda, void *stream);
+
+/* The per-process part of panel_gemv_h (panel_gemv.hpp:119-176), before the
+ * sum across the process row (:177): for this process's rows i,
+ * y_i += alpha * sum over its columns j of a_ij x_j, a_ij regenerated in FP64
+ * (a_ii = d_i).  x, y and d are whole-length (n) device vectors; entries of y
+ * outside this process's rows are left alone.  b <= 6144. */
+mxp_status mxp_otf_gemv_local(int n, int b, uint64_t seed, int nprow, int npcol, int myrow, int mycol,
+                              const double *d_d, double alpha, const double *d_x, double *d_y, void *stream);
+
+/* HPLMXP_gemv (panel_trsv.hpp:13-225): y = beta y + alpha A x with A FP32
+ * (m x n, column-major, lda) and x, y FP64; deterministic summation order. */
+mxp_status mxp_block_gemv(int m, int n, double alpha, const float *d_A, int64_t lda, const double *d_x,
+                          double beta, double *d_y, void *stream);
+
 /* ---- batched form ----------------------------------------------------------
  * Many independent systems of uneven orders (each n a multiple of 128, at most
  * 8192), every one generated, factored and refined exactly as the single-system

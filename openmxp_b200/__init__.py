@@ -110,6 +110,10 @@ _SIGS = {
                               _vp, C.POINTER(LuStats), C.POINTER(IrStats)]),
     "mxp_infnorm": (_i32, [_i32, _vp, C.POINTER(_dbl), _vp, _vp]),
     "mxp_check_reciprocal": (_i32, [C.POINTER(_u64), C.POINTER(_u64)]),
+    "mxp_local_extent": (_i32, [_i32, _i32, _i32, _i32, C.POINTER(_i64)]),
+    "mxp_matgen_local": (_i32, [_i32, _i32, _u64, _i32, _i32, _i32, _i32, _vp, _vp, _i64, _vp]),
+    "mxp_otf_gemv_local": (_i32, [_i32, _i32, _u64, _i32, _i32, _i32, _i32, _vp, _dbl, _vp, _vp, _vp]),
+    "mxp_block_gemv": (_i32, [_i32, _i32, _dbl, _vp, _i64, _vp, _dbl, _vp, _vp]),
     "mxp_batch_sizes": (_i32, [_i32, _u64, C.POINTER(C.c_int)]),
     "mxp_batch_partition": (_i32, [_i32, C.POINTER(C.c_int), _i32, C.POINTER(C.c_int)]),
     "mxp_batch_create": (_i32, [_i32, C.POINTER(C.c_int), C.POINTER(C.c_uint64), _i32, C.POINTER(_vp)]),
