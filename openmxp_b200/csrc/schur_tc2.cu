@@ -157,10 +157,12 @@ schur_tc2_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     const int total_tiles = tiles.tiles_m * tiles.tiles_n;
     const int nk = (K + Cfg::kKPerStage - 1) / Cfg::kKPerStage;
     const int rtiles = (N + 127) / 128;
-    auto needed = [&](int kb, int tm, int tn) -> bool {
-        if (tri_mode == 0) return true;
-        const int off = (kb * Cfg::kKPerStage) % seg;
-        return off < (tri_mode == 1 ? (tn + 1) * kN2 : (tm + 1) * kM2);
+    // needed K stages: the first stage_count of each segment of seg_st stages
+    // (walked with a position counter, no per-stage modulo)
+    const int seg_st = tri_mode ? seg / Cfg::kKPerStage : nk;
+    auto stage_count = [&](int tm, int tn) -> int {
+        if (tri_mode == 0) return nk;
+        return min(seg_st, (tri_mode == 1 ? (tn + 1) * kN2 : (tm + 1) * kM2) / Cfg::kKPerStage);
     };
 
     if (threadIdx.x == 0) {
@@ -197,8 +199,15 @@ schur_tc2_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
         for (int t = cluster; t < total_tiles && ok; t += nclusters) {
             int tm, tn;
             tiles.get(t, tm, tn);
+            const int cnt = stage_count(tm, tn);
+            int pos = -1;
             for (int kb = 0; kb < nk; ++kb) {
-                if (!needed(kb, tm, tn)) continue;
+                if (++pos == seg_st) pos = 0;
+                if (pos >= cnt) {
+                    kb += seg_st - 1 - pos;
+                    pos = seg_st - 1;
+                    continue;
+                }
                 int got = 1;
                 if (lane == 0) got = mbar_wait(smem_u32(&empty[stage]), phase ^ 1u, abort_flag) ? 1 : 0;
                 got = __shfl_sync(0xffffffffu, got, 0);
@@ -255,8 +264,15 @@ schur_tc2_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                 tc_fence_after();
                 const uint32_t d_tmem = tmem_base + acc * kN2;
                 bool first = true;
+                const int cnt = stage_count(tm, tn);
+                int pos = -1;
                 for (int kb = 0; kb < nk; ++kb) {
-                    if (!needed(kb, tm, tn)) continue;
+                    if (++pos == seg_st) pos = 0;
+                    if (pos >= cnt) {
+                        kb += seg_st - 1 - pos;
+                        pos = seg_st - 1;
+                        continue;
+                    }
                     if (!mbar_wait(smem_u32(&full[stage]), phase, abort_flag)) {
                         ok = false;
                         break;
