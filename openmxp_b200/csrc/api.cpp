@@ -97,6 +97,7 @@ struct mxp_workspace {
     int overlap_min = 6;     // minimum trailing size, in blocks
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_inv[2] = {nullptr, nullptr};  // fork / join of the two inverse chains
     int *tile_ctr = nullptr;  // shared tile counter of the split trailing pass
     int *trsm_ctr = nullptr;  // tile counter of the TRSM-by-inverse products (claimed dynamically)
     int trsm_counter = 1;     // TRSM products take tiles from trsm_ctr (0: static round robin)
@@ -208,6 +209,8 @@ extern "C" mxp_status mxp_workspace_destroy(mxp_workspace *ws) {
     if (ws->ev_join) cudaEventDestroy(ws->ev_join);
     for (cudaEvent_t e : ws->ev_trsv)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ws->ev_inv)
+        if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ws->ev_ir)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ws->ev_pool)
@@ -276,6 +279,8 @@ extern "C" mxp_status mxp_workspace_create(int n, int b, int form, int device, m
              cudaEventCreateWithFlags(&ws->ev_join, cudaEventDisableTiming) == cudaSuccess;
         for (int e = 0; e < 4 && ok; ++e)
             ok = cudaEventCreateWithFlags(&ws->ev_trsv[e], cudaEventDisableTiming) == cudaSuccess;
+        for (int e = 0; e < 2 && ok; ++e)
+            ok = cudaEventCreateWithFlags(&ws->ev_inv[e], cudaEventDisableTiming) == cudaSuccess;
         for (int e = 0; e < 6 && ok; ++e) ok = cudaEventCreate(&ws->ev_ir[e]) == cudaSuccess;
     }
     if (!ok) {
@@ -438,16 +443,21 @@ extern "C" mxp_status mxp_matgen_f64(int n, uint64_t seed, int diag_rule, double
 // form: MXP_FORM_BF16X2 (three split products, near FP32) or kFormBf16 (one
 // product).  T: S * s2 floats of scratch; the operands go through the
 // workspace's split buffers.
-static mxp_status finish_inverses_tc(int n, const float *A, int64_t lda, float *XU, float *XL, int64_t ldx,
-                                     int s_start, int form, float *T, mxp_workspace *ws, cudaStream_t st) {
+// The doubling levels of one triangle's inverse from s_start up, as
+// tensor-core products in `form` (split BF16 or one BF16 product) on stream
+// `st`, with the operand casts in P and Q (each b rows x ldk3) and T as the
+// level's temporary: for U, T = U12 inv(U22) then X12 = -inv(U11) T; for L,
+// T = L21 inv(L11) then X21 = -inv(L22) T.
+static mxp_status inverse_chain(bool upper, int n, const float *A, int64_t lda, float *X, int64_t ldx, int s_start,
+                                int form, float *T, void *P, void *Q, mxp_workspace *ws, cudaStream_t st) {
     // C (m x nn) = P (m x K) Q (K x nn), or its negative; column-major FP32
-    auto gemm = [&](int m, int nn, int K, const float *P, int64_t ldp, const float *Q, int64_t ldq, float *C,
+    auto gemm = [&](int m, int nn, int K, const float *Pm, int64_t ldp, const float *Qm, int64_t ldq, float *C,
                     int64_t ldc, bool neg) -> mxp_status {
-        mxp_status q = launch_cast_left(form, m, K, P, ldp, ws->split_l, ws->ldk3, nullptr, st);
-        if (q == MXP_OK) q = launch_cast_right(form, nn, K, Q, ldq, ws->split_u, ws->ldk3, nullptr, st);
+        mxp_status q = launch_cast_left(form, m, K, Pm, ldp, P, ws->ldk3, nullptr, st);
+        if (q == MXP_OK) q = launch_cast_right(form, nn, K, Qm, ldq, Q, ws->ldk3, nullptr, st);
         if (q == MXP_OK)
-            q = launch_schur(form, m, nn, K, ws->split_l, ws->ldk3, nullptr, ws->split_u, ws->ldk3, nullptr, C, ldc,
-                             ws->status, st, neg ? 2 : 1, 0, 0, 0, 0);
+            q = launch_schur(form, m, nn, K, P, ws->ldk3, nullptr, Q, ws->ldk3, nullptr, C, ldc, ws->status, st,
+                             neg ? 2 : 1, 0, 0, 0, 0);
         return q;
     };
     mxp_status q = MXP_OK;
@@ -458,16 +468,45 @@ static mxp_status finish_inverses_tc(int n, const float *A, int64_t lda, float *
             const int s2 = p < np ? S : c;
             if (s2 <= 0) break;
             const int64_t r0 = (int64_t)p * 2 * S, r1 = r0 + S;
-            // U: T = U12 inv(U22) (S x s2), then X12 = -inv(U11) T
-            q = gemm(S, s2, s2, A + r0 + r1 * lda, lda, XU + r1 + r1 * ldx, ldx, T, S, false);
-            if (q == MXP_OK) q = gemm(S, s2, S, XU + r0 + r0 * ldx, ldx, T, S, XU + r0 + r1 * ldx, ldx, true);
-            // L: T = L21 inv(L11) (s2 x S), then X21 = -inv(L22) T
-            if (q == MXP_OK) q = gemm(s2, S, S, A + r1 + r0 * lda, lda, XL + r0 + r0 * ldx, ldx, T, s2, false);
-            if (q == MXP_OK)
-                q = gemm(s2, S, s2, XL + r1 + r1 * ldx, ldx, T, s2, XL + r1 + r0 * ldx, ldx, true);
+            if (upper) {
+                q = gemm(S, s2, s2, A + r0 + r1 * lda, lda, X + r1 + r1 * ldx, ldx, T, S, false);
+                if (q == MXP_OK) q = gemm(S, s2, S, X + r0 + r0 * ldx, ldx, T, S, X + r0 + r1 * ldx, ldx, true);
+            } else {
+                q = gemm(s2, S, S, A + r1 + r0 * lda, lda, X + r0 + r0 * ldx, ldx, T, s2, false);
+                if (q == MXP_OK) q = gemm(s2, S, s2, X + r1 + r1 * ldx, ldx, T, s2, X + r1 + r0 * ldx, ldx, true);
+            }
         }
     }
     return q;
+}
+
+// Both triangles' tensor-core levels.  The U and L chains share nothing, so
+// when the workspace's panel-operand buffer has room for a second pair of
+// operand casts (n >= 3b) the L chain runs on the side stream beside the U
+// chain on `st` (each level is a few products on at most 32 tiles, far from
+// filling the GPU), with its own temporary TL; otherwise one after the other.
+// Either way every product is the same, so the inverses are bit-identical.
+static mxp_status finish_inverses_tc(int n, const float *A, int64_t lda, float *XU, float *XL, int64_t ldx,
+                                     int s_start, int form, float *T, float *TL, mxp_workspace *ws,
+                                     cudaStream_t st) {
+    const int64_t big_rows = ws->n > ws->b ? ws->n - ws->b : 1;
+    const bool two = TL && ws->side && ws->ev_inv[0] && big_rows >= 2 * (int64_t)ws->b;
+    if (!two) {
+        mxp_status q = inverse_chain(true, n, A, lda, XU, ldx, s_start, form, T, ws->split_l, ws->split_u, ws, st);
+        if (q == MXP_OK)
+            q = inverse_chain(false, n, A, lda, XL, ldx, s_start, form, T, ws->split_l, ws->split_u, ws, st);
+        return q;
+    }
+    uint8_t *big = (uint8_t *)ws->split_big;
+    void *P2 = big, *Q2 = big + (size_t)ws->b * ws->ldk3 * 2;
+    MXP_CUDA(cudaEventRecord(ws->ev_inv[0], st));
+    MXP_CUDA(cudaStreamWaitEvent(ws->side, ws->ev_inv[0], 0));
+    mxp_status qL = inverse_chain(false, n, A, lda, XL, ldx, s_start, form, TL, P2, Q2, ws, ws->side);
+    mxp_status qU = inverse_chain(true, n, A, lda, XU, ldx, s_start, form, T, ws->split_l, ws->split_u, ws, st);
+    // join even after an error, so nothing is left running on the side stream unseen
+    MXP_CUDA(cudaEventRecord(ws->ev_inv[1], ws->side));
+    MXP_CUDA(cudaStreamWaitEvent(st, ws->ev_inv[1], 0));
+    return qU != MXP_OK ? qU : qL;
 }
 
 // Tensor-core inverse levels apply from this block size (0: none), when the
@@ -502,7 +541,8 @@ extern "C" mxp_status mxp_getrf_nopiv_inv(int n, float *d_A, int64_t lda, float 
                                tc);
         if (s == MXP_OK && tc > 0)
             s = finish_inverses_tc(n, d_A, lda, d_XU, d_XL, ldx, tc,
-                                   ws->trsm_single ? kFormBf16 : MXP_FORM_BF16X2, ws->coop_tmp, ws, st);
+                                   ws->trsm_single ? kFormBf16 : MXP_FORM_BF16X2, ws->coop_tmp,
+                                   ws->coop_tmp + diag_factor_tmp_floats(ws->b), ws, st);
     } else {
         s = launch_getrf_blocked(n, d_A, lda, ws->status, 0, st);
         if (s == MXP_OK) s = launch_tri_inv_upper(n, d_A, lda, d_XU, ldx, ws->tinv_tmp, st);
@@ -649,7 +689,7 @@ extern "C" mxp_status mxp_panel_lu(int n, int b, float *d_A, int64_t lda, mxp_wo
                                           tmpU, tmpL, ws->coop_sync, ws->status, (int)kk, on, max_grid, tc);
         if (q == MXP_OK && tc > 0)
             q = finish_inverses_tc(b, Akk, lda, XU, XL, b, tc, ws->trsm_single ? kFormBf16 : MXP_FORM_BF16X2,
-                                   tmpU, ws, on);
+                                   tmpU, tmpL, ws, on);
         return q;
     };
     // Factor the diagonal block of step kk (unless diag_done: it was factored

@@ -150,3 +150,24 @@ def test_inverses_tensor_levels(mxp, orc, torch_cuda, single, n, seed):
     for g, w in ((gu, wu), (gl, wl)):
         assert rel_fro(g, w) <= tol
         assert np.max(np.abs(g.astype(np.float64) - w)) <= tol * np.max(np.abs(w))
+
+
+@pytest.mark.parametrize("single", [False, True])
+def test_inverse_chains_concurrent_bit_identical(mxp, torch_cuda, single):
+    """The U and L tensor-core inverse chains run on two streams when the
+    workspace has room for a second pair of operand casts (n >= 3b), one after
+    the other otherwise: the same products either way, so the same bits."""
+    torch = torch_cuda
+    n = B
+    out = []
+    for ws_n in (3 * B, B):  # concurrent chains, then serial
+        p = mxp.panel_matgen(n, 9)
+        XU = torch.empty(n * n, device="cuda")
+        XL = torch.empty(n * n, device="cuda")
+        ws = mxp.Workspace(ws_n, B, 0, trsm_single=single)
+        mxp.getrf_nopiv_inv(p.A, n, n, XU, XL, n, ws)
+        torch.cuda.synchronize()
+        out.append((p.A.clone(), XU, XL))
+        ws.close()
+    for a, b in zip(out[0], out[1]):
+        assert torch.equal(a.view(torch.int32), b.view(torch.int32))
