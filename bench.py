@@ -531,6 +531,39 @@ def run_micro(args):
         def launch():
             mxp.otf_gemv(m, 7, d, -1.0, x, 1.0, y, ws)
         flops = 2.0 * m * m
+    elif args.micro == "trsm":
+        # one panel solve by inverse (mxp_trsm_inv_*: casts + triangular product), m = --n, b = --b,
+        # the right side (B <- B inv(U)) and the left side (B <- inv(L) B) in turn
+        single = args.trsm == "single"
+        ws = mxp.Workspace(m + b, b, mxp.FORM_FP16, trsm_single=single)
+        P = (torch.rand(m * b, device="cuda", generator=g) - 0.5).float()
+        X = torch.eye(b, device="cuda").t().contiguous()
+        X += torch.triu(torch.rand(b, b, device="cuda", generator=g) * 1e-3, 1).t()  # column-major upper
+        X = X.reshape(-1)
+        XLm = X.view(b, b).t().contiguous().reshape(-1)  # its transpose: unit lower, column-major
+        res = {}
+        for side in ("right", "left"):
+            def launch(side=side):
+                if side == "right":
+                    mxp.trsm_inv_right_upper(m, b, X, b, P, m, ws, single=single)
+                else:
+                    mxp.trsm_inv_left_lower(b, m, XLm, b, P, b, ws, single=single)
+            for _ in range(args.warmup):
+                launch()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.steps):
+                launch()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            fl = float(m) * b * b * (1 if single else 3)  # triangular: m b^2 (x3 split)
+            res[side] = {"ms_per_call": ms, "tflops": fl / ms / 1e9}
+        out.update(res, trsm="single BF16" if single else "split BF16 x3")
+        ws.close()
+        print(json.dumps(out), flush=True)
+        return 0
     elif args.micro == "diag":
         # diagonal-block factorisation alone (n = --b): LU, and LU + both triangular
         # inverses, as one cooperative launch and as the per-step launch chain
@@ -833,7 +866,7 @@ def parse(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--micro", choices=["schur", "otf_gemv", "cublas", "diag"], default=None,
+    ap.add_argument("--micro", choices=["schur", "otf_gemv", "cublas", "diag", "trsm"], default=None,
                     help="time one kernel alone at m=--n, k=--b (for profiler captures)")
     ap.add_argument("--micro-seconds", type=float, default=0.0,
                     help="micro: run the launch this long before timing (sustained clocks)")

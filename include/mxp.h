@@ -223,6 +223,19 @@ mxp_status mxp_trsm_right_upper(int m, int n, const float *d_U, int64_t ldu, flo
 mxp_status mxp_trsm_left_lower_unit(int m, int n, const float *d_L, int64_t ldl, float *d_B,
                                     int64_t ldb, void *stream);
 
+/* update_left_panels_wGPU_alt / update_right_panels_wGPU_alt
+ * (panel_trf_gdirect.hpp:73-142), the reference's Alt-TRSM: the panel solve
+ * as a product with the triangle's inverse (from mxp_getrf_nopiv_inv) on the
+ * tensor cores, in place.  right_upper: B (m x b) <- B * X_U; left_lower:
+ * B (b x m) <- X_L * B.  single != 0: both operands rounded to BF16 once (the
+ * reference rounds them to FP16); 0: three split-BF16 products (hi*hi + hi*lo
+ * + lo*hi, near FP32).  FP32 accumulation; zero blocks of the triangular
+ * inverse are skipped.  b <= the workspace's b and m <= its n - b.  Async. */
+mxp_status mxp_trsm_inv_right_upper(int m, int b, const float *d_XU, int64_t ldx, float *d_B, int64_t ldb,
+                                    int single, mxp_workspace *ws, void *stream);
+mxp_status mxp_trsm_inv_left_lower(int b, int m, const float *d_XL, int64_t ldx, float *d_B, int64_t ldb,
+                                   int single, mxp_workspace *ws, void *stream);
+
 /* half_conversion_left (fp16_gpu_kernels.h:26-27, .cpp:180-192): FP32 m x b
  * block (column-major, plda) -> FP16 column-major (lplda), round to nearest.
  * Reference layout; bit-exact with copyCoalesced. */

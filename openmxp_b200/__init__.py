@@ -110,6 +110,8 @@ _SIGS = {
                               _vp, C.POINTER(LuStats), C.POINTER(IrStats)]),
     "mxp_infnorm": (_i32, [_i32, _vp, C.POINTER(_dbl), _vp, _vp]),
     "mxp_check_reciprocal": (_i32, [C.POINTER(_u64), C.POINTER(_u64)]),
+    "mxp_trsm_inv_right_upper": (_i32, [_i32, _i32, _vp, _i64, _vp, _i64, _i32, _vp, _vp]),
+    "mxp_trsm_inv_left_lower": (_i32, [_i32, _i32, _vp, _i64, _vp, _i64, _i32, _vp, _vp]),
     "mxp_local_extent": (_i32, [_i32, _i32, _i32, _i32, C.POINTER(_i64)]),
     "mxp_matgen_local": (_i32, [_i32, _i32, _u64, _i32, _i32, _i32, _i32, _vp, _vp, _i64, _vp]),
     "mxp_otf_gemv_local": (_i32, [_i32, _i32, _u64, _i32, _i32, _i32, _i32, _vp, _dbl, _vp, _vp, _vp]),
@@ -356,6 +358,18 @@ def trsm_right_upper(m, n, U, ldu, B, ldb, stream=None):
 
 def trsm_left_lower_unit(m, n, L, ldl, B, ldb, stream=None):
     check(lib().mxp_trsm_left_lower_unit(m, n, _ptr(L), ldl, _ptr(B), ldb, _stream(stream)))
+
+
+def trsm_inv_right_upper(m, b, XU, ldx, B, ldb, ws: "Workspace", single: bool = False, stream=None):
+    """B (m x b) <- B * XU on the tensor cores (the reference's Alt-TRSM)."""
+    check(lib().mxp_trsm_inv_right_upper(m, b, _ptr(XU), ldx, _ptr(B), ldb, int(single), ws.handle,
+                                         _stream(stream)))
+
+
+def trsm_inv_left_lower(b, m, XL, ldx, B, ldb, ws: "Workspace", single: bool = False, stream=None):
+    """B (b x m) <- XL * B on the tensor cores (the reference's Alt-TRSM)."""
+    check(lib().mxp_trsm_inv_left_lower(b, m, _ptr(XL), ldx, _ptr(B), ldb, int(single), ws.handle,
+                                        _stream(stream)))
 
 
 def half_conversion_left(Cm, m, b, plda, lp, lplda, stream=None):

@@ -562,6 +562,51 @@ extern "C" mxp_status mxp_trsm_left_lower_unit(int m, int n, const float *d_L, i
     return launch_trsm_llnu(m, n, d_L, ldl, d_B, ldb, as_stream(stream));
 }
 
+// TRSM by inverse on the tensor cores, one panel side at a time: the panel and
+// the triangular inverse cast to BF16 (one product, single != 0) or split
+// BF16 (hi*hi + hi*lo + lo*hi), then one store-mode product with the
+// triangular K-skip, the panel overwritten in place (its cast is taken first).
+// The same steps mxp_panel_lu runs per panel.
+static mxp_status trsm_inv(bool right_upper, int m, int b, const float *X, int64_t ldx, float *B, int64_t ldb,
+                           int single, mxp_workspace *ws, cudaStream_t st) {
+    if (!ws || !X || !B) return fail(MXP_INVALID_ARG, "trsm_inv: NULL argument");
+    if (m < 0 || b <= 0 || b > ws->b) return fail(MXP_INVALID_ARG, "trsm_inv: b must be in 1..b of the workspace");
+    const int64_t big_rows = ws->n > ws->b ? ws->n - ws->b : 1;
+    if (m > big_rows) return fail(MXP_INVALID_ARG, "trsm_inv: panel longer than the workspace's n - b");
+    if (ldx < b || (right_upper ? ldb < m : ldb < b)) return fail(MXP_INVALID_ARG, "trsm_inv: bad leading dimension");
+    if (m == 0) return MXP_OK;
+    const int bf = single ? kFormBf16 : MXP_FORM_BF16X2;
+    SchurSched ts;
+    ts.counter = ws->trsm_ctr;
+    mxp_status q;
+    if (right_upper) {  // B (m x b) <- B * X, X upper
+        q = launch_cast_left(bf, m, b, B, ldb, ws->split_big, ws->ldk3, nullptr, st);
+        if (q == MXP_OK) q = launch_cast_right(bf, b, b, X, ldx, ws->split_u, ws->ldk3, nullptr, st);
+        if (q == MXP_OK) MXP_CUDA(cudaMemsetAsync(ws->trsm_ctr, 0, sizeof(int), st));
+        if (q == MXP_OK)
+            q = launch_schur(bf, m, b, b, ws->split_big, ws->ldk3, nullptr, ws->split_u, ws->ldk3, nullptr, B, ldb,
+                             ws->status, st, /*store=*/1, 0, 0, /*tri=*/1, 0, &ts);
+    } else {            // B (b x m) <- X * B, X unit lower
+        q = launch_cast_left(bf, b, b, X, ldx, ws->split_l, ws->ldk3, nullptr, st);
+        if (q == MXP_OK) q = launch_cast_right(bf, m, b, B, ldb, ws->split_big, ws->ldk3, nullptr, st);
+        if (q == MXP_OK) MXP_CUDA(cudaMemsetAsync(ws->trsm_ctr, 0, sizeof(int), st));
+        if (q == MXP_OK)
+            q = launch_schur(bf, b, m, b, ws->split_l, ws->ldk3, nullptr, ws->split_big, ws->ldk3, nullptr, B, ldb,
+                             ws->status, st, /*store=*/1, 0, 0, /*tri=*/2, 0, &ts);
+    }
+    return q;
+}
+
+extern "C" mxp_status mxp_trsm_inv_right_upper(int m, int b, const float *d_XU, int64_t ldx, float *d_B,
+                                               int64_t ldb, int single, mxp_workspace *ws, void *stream) {
+    return trsm_inv(true, m, b, d_XU, ldx, d_B, ldb, single, ws, as_stream(stream));
+}
+
+extern "C" mxp_status mxp_trsm_inv_left_lower(int b, int m, const float *d_XL, int64_t ldx, float *d_B,
+                                              int64_t ldb, int single, mxp_workspace *ws, void *stream) {
+    return trsm_inv(false, m, b, d_XL, ldx, d_B, ldb, single, ws, as_stream(stream));
+}
+
 extern "C" mxp_status mxp_half_conversion_left(const float *d_C, int m, int b, int64_t plda,
                                                uint16_t *d_lp, int64_t lplda, void *stream) {
     return launch_half_left_ref(d_C, m, b, plda, d_lp, lplda, as_stream(stream));
