@@ -452,7 +452,17 @@ schur_tc_f16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
     __syncthreads();
     if (*abort_flag) {
         // Let any TMA copy / MMA still in flight land before TMEM and shared
-        // memory are released (bounded: ~50 us).
+        // memory are released.  The abort is raised only by a role whose wait
+        // ran out (2 s); every other role leaves at its next bounded wait, so
+        // the producer issues nothing after it sees the flag and at most
+        // kStages stages of loads (and the MMAs of as many stages) can still
+        // be in flight.  Each completes within the memory latency and one
+        // stage's MMA time, a few microseconds even under the full load of
+        // the GPU (the per-stage traces of these kernels show ~1-2 us from a
+        // load's issue to its data); 50 us is an order of magnitude above
+        // that.  A wait on the stages' own barriers is not used here because
+        // a barrier whose phase was never completed would make this path
+        // wait out another timeout.
         if (threadIdx.x == 0) {
             const unsigned long long t0 = globaltimer_ns();
             while (globaltimer_ns() - t0 < 50000ull) {
