@@ -28,6 +28,7 @@ struct __align__(16) SmemTri {
     float us[kNB][kNB];      // us[k][c] = U(k, k + 1 + c): row k of U right of the diagonal, zero past the block
     float ls[kNB][kNB];      // ls[k][c] = L(k + 1 + c, k): column k of L below the diagonal, zero past the block
     float dinv[kNB];
+    int ready[32];           // 64 x 64 factor: multipliers of pivot k published (getrf64)
 };
 struct __align__(16) SmemG64 {  // one 64 x 64 x 64 product staged whole
     float As[kNB][kNB];       // As[k][row]
@@ -236,46 +237,53 @@ __device__ void gemm_tile64(Smem &sm, int m, int n, int k, float alpha, const fl
     __syncthreads();
 }
 
-// ---- 64 x 64 no-pivot LU of D (nb <= 64), warp 0 alone --------------------------
+// ---- 64 x 64 no-pivot LU of D (nb <= 64), warps 0 and 1 ---------------------
 // sgetrf_nopiv_naive order (sgetrf_nopiv.cpp:27-61): scale by the reciprocal
-// pivot, then the rank-1 update.  Lane l keeps rows l and l + 32 in
-// registers, each rotated (rot_axpy's scheme): at pivot k an active row holds
-// A(r, k ..) from index 0.  Per pivot, the lane owning row k hands its row to
-// the others by register shuffles (no barrier, no shared-memory round trip);
-// each active row forms its multiplier, updates the column that holds the
-// next pivot first, and the next pivot's reciprocal (rcp_rn_f32, branch-free)
-// is issued at once so its latency overlaps the rest of the row update.
-// Multipliers (column k of L) go to shared memory as they are formed; a row
-// stops rotating at its own pivot, so at the end each lane holds its rows of
-// U; the CTA then stores the block.  Timed alone in one CTA (clock64, 64 x 64):
-// 27.3 k cycles against 40 k for one row per thread of two warps with a named
-// barrier per pivot; the shuffles (~4 issue cycles each) and the per-pivot
-// chain (shuffle, reciprocal, multiply, update) set the pace.
-template <int W, bool TOP>
-__device__ __forceinline__ void getrf64_phase(float (*T)[kNB + 4], float (&a0)[kNB], float (&a1)[kNB], float &pv,
-                                              float &rp, int k0, int k1, int nb, DevStatus *dst, int pivot_base) {
-    const int ln = threadIdx.x;
+// pivot, then the rank-1 update.  Lane l of each warp keeps rows l and l + 32;
+// warp 0 holds columns 0..31, warp 1 columns 32..63.
+//  pivots 0..31: warp 0 factors its columns, each row rotated (rot_axpy's
+//    scheme: at pivot k an active row holds A(r, k ..) from index 0), the
+//    pivot row by register shuffles, the next pivot's reciprocal
+//    (rcp_rn_f32, branch-free) issued as soon as that pivot is final; it
+//    publishes each pivot's multipliers (column k of L) in shared memory and
+//    raises ready[k].  Warp 1 follows pivot by pivot: it waits for ready[k]
+//    (bounded), takes the multipliers and the pivot row's right half (row k
+//    is in its own registers, by shuffles) and updates its columns;
+//  pivots 32..63: warp 1 alone on rows 32..63 of its columns, rotated.
+// Every element receives the same fmaf updates in the same order as in the
+// one-warp form, so the factors are bit-identical; splitting the columns
+// halves the shuffles on the pivot chain (~4 issue cycles each).  Rows stop
+// rotating at their own pivot, so at the end each lane holds its rows of U;
+// the factor goes through shared memory (T = t[col][row]) to one coalesced
+// store (scattered global stores stalled it under the L2 traffic of the
+// trailing update running beside it).  Warps 2..7 wait at the barriers.
+template <int W>
+__device__ __forceinline__ void getrf64_left(float (*T)[kNB + 4], volatile int *ready, float (&a0)[32],
+                                             float (&a1)[32], float &pv, float &rp, int k0, int k1, int nb,
+                                             DevStatus *dst, int pivot_base) {
+    const int ln = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
 #pragma unroll 1
     for (int k = k0; k < k1; ++k) {
         if (ln == 0 && (!(pv != 0.0f) || !isfinite(pv))) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
-        const int src = k & 31;  // row k: a0 of lane src (k < 32), else a1
-        const bool act0 = TOP && ln > k && ln < nb, act1 = ln + 32 > k && ln + 32 < nb;
+        const bool act0 = ln > k && ln < nb, act1 = ln + 32 < nb;
         const float l0 = act0 ? a0[0] * rp : 0.0f;
         const float l1 = act1 ? a1[0] * rp : 0.0f;
-        const float u0 = __shfl_sync(full, TOP ? a0[1] : a1[1], src);
-        if (act0) a0[0] = fmaf(-u0, l0, a0[1]);
-        if (act1) a1[0] = fmaf(-u0, l1, a1[1]);
-        {  // the next pivot is final now (past the last pivot the value is not used)
-            const int kn = k + 1;
-            pv = __shfl_sync(full, kn < 32 ? a0[0] : a1[0], kn & 31);
-            rp = rcp_rn_f32(pv);
-        }
         if (act0) T[k][ln] = l0;
         if (act1) T[k][ln + 32] = l1;
+        __threadfence_block();
+        __syncwarp();
+        if (ln == 0) ready[k] = 1;
+        const float u0 = __shfl_sync(full, a0[1], k);
+        if (act0) a0[0] = fmaf(-u0, l0, a0[1]);
+        if (act1) a1[0] = fmaf(-u0, l1, a1[1]);
+        if (k + 1 < 32) {  // uniform: the next pivot is final now
+            pv = __shfl_sync(full, a0[0], k + 1);
+            rp = rcp_rn_f32(pv);
+        }
 #pragma unroll
         for (int c = 1; c < W - 1; ++c) {
-            const float u = __shfl_sync(full, TOP ? a0[c + 1] : a1[c + 1], src);
+            const float u = __shfl_sync(full, a0[c + 1], k);
             if (act0) a0[c] = fmaf(-u, l0, a0[c + 1]);
             if (act1) a1[c] = fmaf(-u, l1, a1[c + 1]);
         }
@@ -284,33 +292,99 @@ __device__ __forceinline__ void getrf64_phase(float (*T)[kNB + 4], float (&a0)[k
     }
 }
 
+template <int W>
+__device__ __forceinline__ void getrf64_lower_right(float (*T)[kNB + 4], float (&b1)[32], float &pv, float &rp,
+                                                    int k0, int k1, int nb, DevStatus *dst, int pivot_base) {
+    const int ln = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+#pragma unroll 1
+    for (int k = k0; k < k1; ++k) {
+        if (ln == 0 && (!(pv != 0.0f) || !isfinite(pv))) report(dst, MXP_ZERO_PIVOT, pivot_base + k + 1, 0);
+        const int src = k - 32;  // row k: b1 of lane k - 32
+        const bool act1 = ln + 32 > k && ln + 32 < nb;
+        const float l1 = act1 ? b1[0] * rp : 0.0f;
+        const float u0 = __shfl_sync(full, b1[1], src);
+        if (act1) b1[0] = fmaf(-u0, l1, b1[1]);
+        {  // the next pivot (past the last one the value is not used)
+            pv = __shfl_sync(full, b1[0], (k + 1) & 31);
+            rp = rcp_rn_f32(pv);
+        }
+        if (act1) T[k][ln + 32] = l1;
+#pragma unroll
+        for (int c = 1; c < W - 1; ++c) {
+            const float u = __shfl_sync(full, b1[c + 1], src);
+            if (act1) b1[c] = fmaf(-u, l1, b1[c + 1]);
+        }
+        if (act1) b1[W - 1] = 0.0f;
+    }
+}
+
 __device__ __noinline__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, DevStatus *dst, int pivot_base) {
     float(*T)[kNB + 4] = sm.t.t;  // T[c][r]: the factored block, written out at the end
-    if (threadIdx.x < 32) {
-        const int ln = threadIdx.x;
-        float a0[kNB], a1[kNB];
+    volatile int *ready = sm.t.ready;
+    if (threadIdx.x < 32) ready[threadIdx.x] = 0;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    if (warp == 0) {
+        float a0[32], a1[32];
 #pragma unroll
-        for (int j = 0; j < kNB; ++j) {
+        for (int j = 0; j < 32; ++j) {
             a0[j] = (j < nb && ln < nb) ? __ldcg(D + (int64_t)j * lda + ln) : 0.0f;
             a1[j] = (j < nb && ln + 32 < nb) ? __ldcg(D + (int64_t)j * lda + ln + 32) : 0.0f;
         }
-        float pv = __shfl_sync(0xffffffffu, a0[0], 0);
+        float pv = __shfl_sync(full, a0[0], 0);
         float rp = rcp_rn_f32(pv);
-        getrf64_phase<64, true>(T, a0, a1, pv, rp, 0, min(nb, 16), nb, dst, pivot_base);
-        getrf64_phase<48, true>(T, a0, a1, pv, rp, 16, min(nb, 32), nb, dst, pivot_base);
-        getrf64_phase<32, false>(T, a0, a1, pv, rp, 32, min(nb, 48), nb, dst, pivot_base);
-        getrf64_phase<16, false>(T, a0, a1, pv, rp, 48, nb, nb, dst, pivot_base);
-        // rows of U: frozen in the registers since their own pivot, a[c] = U(r, r + c)
+        getrf64_left<32>(T, ready, a0, a1, pv, rp, 0, min(nb, 16), nb, dst, pivot_base);
+        getrf64_left<16>(T, ready, a0, a1, pv, rp, 16, min(nb, 32), nb, dst, pivot_base);
+        // rows 0..31 of U in columns 0..31: a0[c] = U(l, l + c)
 #pragma unroll
-        for (int c = 0; c < kNB; ++c) {
-            if (ln < nb && ln + c < nb) T[ln + c][ln] = a0[c];
-            if (ln + 32 < nb && ln + 32 + c < nb) T[ln + 32 + c][ln + 32] = a1[c];
+        for (int c = 0; c < 32; ++c)
+            if (ln < nb && ln + c < min(nb, 32)) T[ln + c][ln] = a0[c];
+    } else if (warp == 1) {
+        float b0[32], b1[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            b0[j] = (32 + j < nb && ln < nb) ? __ldcg(D + (int64_t)(32 + j) * lda + ln) : 0.0f;
+            b1[j] = (32 + j < nb && ln + 32 < nb) ? __ldcg(D + (int64_t)(32 + j) * lda + ln + 32) : 0.0f;
+        }
+        if (nb > 32) {
+#pragma unroll 1
+            for (int k = 0; k < 32; ++k) {
+                // warp 0's multipliers of pivot k (bounded wait)
+                const unsigned long long t0 = globaltimer_ns();
+                while (ready[k] == 0) {
+                    if (globaltimer_ns() - t0 > kWaitTimeoutNs) {
+                        if (ln == 0) report(dst, MXP_TIMEOUT, 40, blockIdx.x);
+                        break;
+                    }
+                }
+                __threadfence_block();
+                const bool act0 = ln > k && ln < nb, act1 = ln + 32 < nb;
+                const float l0 = act0 ? T[k][ln] : 0.0f;
+                const float l1 = act1 ? T[k][ln + 32] : 0.0f;
+#pragma unroll
+                for (int c = 0; c < 32; ++c) {  // row k's right half: b0 of lane k
+                    const float u = __shfl_sync(full, b0[c], k);
+                    if (act0) b0[c] = fmaf(-u, l0, b0[c]);
+                    if (act1) b1[c] = fmaf(-u, l1, b1[c]);
+                }
+            }
+            // rows 0..31 of U in columns 32..63
+#pragma unroll
+            for (int c = 0; c < 32; ++c)
+                if (ln < nb && 32 + c < nb) T[32 + c][ln] = b0[c];
+            float pv = __shfl_sync(full, b1[0], 0);
+            float rp = rcp_rn_f32(pv);
+            getrf64_lower_right<32>(T, b1, pv, rp, 32, min(nb, 48), nb, dst, pivot_base);
+            getrf64_lower_right<16>(T, b1, pv, rp, 48, nb, nb, dst, pivot_base);
+#pragma unroll
+            for (int c = 0; c < 32; ++c)
+                if (ln + 32 < nb && ln + 32 + c < nb) T[ln + 32 + c][ln + 32] = b1[c];
         }
     }
     __syncthreads();
-    // the whole block in one coalesced pass: shared-memory stores inside the
-    // pivot loop instead of ~250 scattered global stores, which stalled the
-    // factor under the L2 traffic of the trailing update running beside it
+    // the whole block in one coalesced pass
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
         const int idx = threadIdx.x + kCT * q;
