@@ -155,11 +155,26 @@ __device__ void trsm_cols_staged(Smem &sm, float *stage, int ncols, int nb, floa
     __syncthreads();
 }
 
+// one accumulating rank-64 tile of the panel (its own register allocation: the
+// persistent kernel around it is at the register limit)
+__device__ __noinline__ void panel_tile_v(SmemGV &sv, int m, int n, const float *A, const float *B, float *C,
+                                          int64_t ld, int m0, int n0) {
+    gemm_tile_v(sv, m, n, 0, kNB, -1.0f, A, ld, B, ld, true, C, ld, m0, n0);
+}
+
 // ---- panel factorisation of one block step (SIMT FP32, whole CTA) -----------
 // D = A(k0, k0) (bk x bk), L strip = A(k0+bk.., k0..) (m x bk), U strip =
 // A(k0.., k0+bk..) (bk x m); lda = n.
 __device__ void factor_step(Smem &sm, float *stage, float *A, int n, int k0, int bk, DevStatus *dst) {
     const int64_t lda = n;
+    // the rank-64 updates as cp.async-staged tiles when the system allows
+    // 16-byte copies (its base 16-byte aligned, n a multiple of 4)
+    SmemGV &sv = *reinterpret_cast<SmemGV *>(&sm);
+    const bool vec = gemm_tile_v_ok(A, lda, A, lda, A, lda, 0);
+    auto tile = [&](int tm_, int tn_, const float *Ap, const float *Bp, float *Cp, int m0, int n0) {
+        if (vec) panel_tile_v(sv, tm_, tn_, Ap, Bp, Cp, lda, m0, n0);
+        else gemm_tile(sm, tm_, tn_, 0, kNB, -1.0f, Ap, lda, Bp, lda, true, Cp, lda, m0, n0);
+    };
     float *D = A + k0 + (int64_t)k0 * lda;
     const int m = n - k0 - bk;
     // diagonal block: blocked by 64, whole CTA
@@ -174,8 +189,8 @@ __device__ void factor_step(Smem &sm, float *stage, float *A, int n, int k0, int
         __syncthreads();
         const int tm = (rem + GBM - 1) / GBM;
         for (int t = 0; t < tm * tm; ++t)
-            gemm_tile(sm, rem, rem, 0, kNB, -1.0f, Dj + kNB, lda, Dj + (int64_t)kNB * lda, lda, true,
-                      Dj + kNB + (int64_t)kNB * lda, lda, (t % tm) * GBM, (t / tm) * GBN);
+            tile(rem, rem, Dj + kNB, Dj + (int64_t)kNB * lda, Dj + kNB + (int64_t)kNB * lda, (t % tm) * GBM,
+                 (t / tm) * GBN);
     }
     if (m <= 0) return;
     float *Ls = D + bk;                     // m x bk
@@ -189,9 +204,8 @@ __device__ void factor_step(Smem &sm, float *stage, float *A, int n, int k0, int
         if (rest > 0) {
             const int tm = (m + GBM - 1) / GBM, tn = (rest + GBN - 1) / GBN;
             for (int t = 0; t < tm * tn; ++t)
-                gemm_tile(sm, m, rest, 0, kNB, -1.0f, Ls + (int64_t)c * lda, lda,
-                          D + c + (int64_t)(c + kNB) * lda, lda, true, Ls + (int64_t)(c + kNB) * lda, lda,
-                          (t % tm) * GBM, (t / tm) * GBN);
+                tile(m, rest, Ls + (int64_t)c * lda, D + c + (int64_t)(c + kNB) * lda, Ls + (int64_t)(c + kNB) * lda,
+                     (t % tm) * GBM, (t / tm) * GBN);
         }
     }
     // U strip: L X = B, one 64-row block at a time
@@ -203,8 +217,7 @@ __device__ void factor_step(Smem &sm, float *stage, float *A, int n, int k0, int
         if (rest > 0) {
             const int tm = (rest + GBM - 1) / GBM, tn = (m + GBN - 1) / GBN;
             for (int t = 0; t < tm * tn; ++t)
-                gemm_tile(sm, rest, m, 0, kNB, -1.0f, D + c + kNB + (int64_t)c * lda, lda, Us + c, lda, true,
-                          Us + c + kNB, lda, (t % tm) * GBM, (t / tm) * GBN);
+                tile(rest, m, D + c + kNB + (int64_t)c * lda, Us + c, Us + c + kNB, (t % tm) * GBM, (t / tm) * GBN);
         }
     }
 }
@@ -694,6 +707,7 @@ size_t smem_bytes(const mxp_batch *bt, const BatchConfig &c) {
     size_t s = ring_bytes(c.tile_n, c.stages) + kCbufBytes;
     s = std::max(s, (size_t)16 * bt->nmax + sizeof(float) * kNB * (kNB + 1));  // x, r (FP64) + a 64 x 64 block
     s = std::max(s, kColStageOff + kColStageBytes);
+    s = std::max(s, sizeof(SmemGV));  // the panel's cp.async-staged update tiles
     return s + 1024;                          // 1024-byte alignment of the ring
 }
 

@@ -45,7 +45,9 @@ union __align__(16) Smem {
 // column (threadIdx.x + 256 q) / 64, row (threadIdx.x + 256 q) % 64.  All 16
 // loads are issued before any is used, so the block costs one L2 round trip.
 static_assert(kCT * 16 == kNB * kNB, "64 x 64 block = 16 values per thread");
-__device__ __forceinline__ void load_block64(float (&v)[16], const float *D, int64_t ld, int nr, int nc) {
+template <int N>
+__device__ __forceinline__ void load_block64(float (&v)[N], const float *D, int64_t ld, int nr, int nc) {
+    static_assert(N >= 16, "16 values per thread");
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
         const int idx = threadIdx.x + kCT * q;
@@ -173,17 +175,193 @@ __device__ void gemm_tile(Smem &sm, int m, int n, int kb, int ke, float alpha,
     __syncthreads();  // shared tiles are reused by the caller's next item
 }
 
-// C[0:m, 0:n] += alpha * A(:, 0:k) B(0:k, :) for m, n <= 64 (one 64 x 64 tile,
-// 4 x 4 outputs per thread): the look-ahead update of the next diagonal block.
-__device__ void gemm_tile64(Smem &sm, int m, int n, int k, float alpha, const float *__restrict__ A, int64_t lda,
-                            const float *__restrict__ B, int64_t ldb, float *C, int64_t ldc) {
+// ---- 128 x 128 SIMT GEMM tile staged by cp.async -----------------------------
+// The same tile as gemm_tile with the same per-element operation order (each
+// output is one fmaf chain over k ascending from 0, then times alpha, then
+// plus C), so the two give identical bits; only the data movement differs.
+// gemm_tile moves 16-deep slices through registers with two CTA barriers
+// each and reads C by scattered scalar loads after the products, which puts
+// four L2 round trips and 64 uncoalesced requests per thread on every
+// 128 x 128 x 64 tile.  Here 16-byte cp.async copies (L2 only, .cg: the data
+// may come from other CTAs behind a grid barrier) bring a whole 64-deep
+// slice of both operands and, for an accumulating tile, the C tile into
+// shared memory at once, the next slice streams into the second buffer
+// while the current one is multiplied, and C is written back by float4
+// stores.  Needs 16-byte aligned bases, leading dimensions that are
+// multiples of 4 floats and kb % 4 == 0 (gemm_tile_v_ok); ragged edges are
+// zero-filled through cp.async's source size.
+struct __align__(16) SmemGVBuf {
+    float As[kNB][GBM];      // As[k][row]
+    float Bs[GBN][kNB + 4];  // Bs[col][k]
+};
+struct __align__(16) SmemGV {
+    SmemGVBuf buf[2];  // two 64-deep operand slices; a C tile Cs[col][row] (pitch 132) in buf[1]
+};
+static_assert(sizeof(SmemGVBuf) == sizeof(float) * GBN * (GBM + 4), "the C tile fills one operand buffer");
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int bytes) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
+__device__ __forceinline__ bool gemm_tile_v_ok(const float *A, int64_t lda, const float *B, int64_t ldb,
+                                               const float *C, int64_t ldc, int kb) {
+    return aligned16(A) && aligned16(B) && aligned16(C) && ((lda | ldb | ldc) & 3) == 0 && (kb & 3) == 0;
+}
+
+// bytes of a 4-float group starting at index i of an extent e (0 .. 16)
+__device__ __forceinline__ int grp_bytes(int i, int e) { return 4 * max(0, min(4, e - i)); }
+
+// one 64-deep slice [k0, k0 + 64) ∩ [k0, ke) of A(m0:m0+128, :) and B(:, n0:n0+128)
+__device__ __forceinline__ void gv_load_slice(SmemGVBuf &b, int m, int n, int k0, int ke, const float *A,
+                                              int64_t lda, const float *B, int64_t ldb, int m0, int n0) {
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {  // A: 64 k x 32 row groups
+        const int idx = t + kCT * q;
+        const int kk = idx >> 5, r = (idx & 31) * 4;
+        const int gk = k0 + kk, gr = m0 + r;
+        const int by = gk < ke ? grp_bytes(gr, m) : 0;
+        cp_async16(&b.As[kk][r], by ? A + (int64_t)gk * lda + gr : A, by);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {  // B: 128 columns x 16 k groups
+        const int idx = t + kCT * q;
+        const int c = idx >> 4, kk = (idx & 15) * 4;
+        const int gc = n0 + c, gk = k0 + kk;
+        const int by = gc < n ? grp_bytes(gk, ke) : 0;
+        cp_async16(&b.Bs[c][kk], by ? B + (int64_t)gc * ldb + gk : B, by);
+    }
+}
+
+__device__ void gemm_tile_v(SmemGV &sv, int m, int n, int kb, int ke, float alpha, const float *__restrict__ A,
+                            int64_t lda, const float *__restrict__ B, int64_t ldb, bool accumulate, float *C,
+                            int64_t ldc, int m0, int n0, int skip = 0) {
     const int t = threadIdx.x;
     const int tx = t % 16, ty = t / 16;
-    float acc[4][4];
+    float(*Cs)[GBM + 4] = reinterpret_cast<float(*)[GBM + 4]>(&sv.buf[1]);
+    const int nch = ke > kb ? (ke - kb + kNB - 1) / kNB : 0;
+    const bool c_early = accumulate && nch <= 1;  // C shares buf[1] with the second slice
+    __syncthreads();  // the caller's previous use of this memory is over
+    if (nch > 0) gv_load_slice(sv.buf[0], m, n, kb, ke, A, lda, B, ldb, m0, n0);
+    cp_async_commit();
+    auto load_c = [&]() {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {  // 128 columns x 32 row groups
+            const int idx = t + kCT * q;
+            const int c = idx >> 5, r = (idx & 31) * 4;
+            const int gc = n0 + c, gr = m0 + r;
+            const int by = gc < n ? grp_bytes(gr, m) : 0;
+            cp_async16(&Cs[c][r], by ? C + (int64_t)gc * ldc + gr : C, by);
+        }
+        cp_async_commit();
+    };
+    if (c_early) load_c();
+
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+
+    for (int ch = 0; ch < nch; ++ch) {
+        const int k0 = kb + ch * kNB;
+        if (ch + 1 < nch) {
+            gv_load_slice(sv.buf[(ch + 1) & 1], m, n, k0 + kNB, ke, A, lda, B, ldb, m0, n0);
+            cp_async_commit();
+            cp_async_wait<1>();  // slice ch has landed, ch + 1 may be in flight
+        } else if (c_early) {
+            cp_async_wait<1>();  // slice ch has landed, C may be in flight
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const SmemGVBuf &b = sv.buf[ch & 1];
+        const int nk4 = (min(kNB, ke - k0) + 3) / 4;
+#pragma unroll 1
+        for (int k4 = 0; k4 < nk4; ++k4) {
+            float4 bq[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                bq[j] = *reinterpret_cast<const float4 *>(&b.Bs[j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4)][4 * k4]);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const float4 a0 = *reinterpret_cast<const float4 *>(&b.As[4 * k4 + s][tx * 4]);
+                const float4 a1 = *reinterpret_cast<const float4 *>(&b.As[4 * k4 + s][64 + tx * 4]);
+                const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+                float bv[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) bv[j] = s == 0 ? bq[j].x : s == 1 ? bq[j].y : s == 2 ? bq[j].z : bq[j].w;
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+            }
+        }
+        __syncthreads();  // buf[ch & 1] is refilled two slices on (or holds C)
+    }
+    if (accumulate) {
+        if (!c_early) load_c();
+        cp_async_wait<0>();
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int cl = j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4);
+        const int gc = n0 + cl;
+        if (gc >= n) continue;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int rl = h * 64 + tx * 4, gr = m0 + rl;
+            float v[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) v[e] = acc[4 * h + e][j] * alpha;
+            if (accumulate) {
+                const float4 c4 = *reinterpret_cast<const float4 *>(&Cs[cl][rl]);
+                v[0] += c4.x;
+                v[1] += c4.y;
+                v[2] += c4.z;
+                v[3] += c4.w;
+            }
+            // element (rl + e, cl) of the tile is left alone when rl + e < skip and cl < skip
+            float *dst = C + (int64_t)gc * ldc + gr;
+            if (gr + 3 < m && (cl >= skip || rl >= skip)) {
+                *reinterpret_cast<float4 *>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+                continue;
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (gr + e < m && !(cl < skip && rl + e < skip)) dst[e] = v[e];
+        }
+    }
+    __syncthreads();  // shared memory is reused by the caller's next item
+}
+
+// C[0:m, 0:n] += alpha * A(:, 0:k) B(0:k, :) for m, n <= 64 (one 64 x 64 tile,
+// 4 x 4 outputs per thread): the look-ahead update of the next diagonal block.
+// C is read together with the first operand slice (one L2 round trip for
+// all three).  to_smem: the result goes to sm.t.t[col][row] instead of C, for
+// getrf64(..., in_smem = true) to factor without a global round trip (the
+// caller then owns writing it back; getrf64 does).
+__device__ void gemm_tile64(Smem &sm, int m, int n, int k, float alpha, const float *__restrict__ A, int64_t lda,
+                            const float *__restrict__ B, int64_t ldb, float *C, int64_t ldc, bool to_smem = false) {
+    const int t = threadIdx.x;
+    const int tx = t % 16, ty = t / 16;
+    float acc[4][4], cv[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+        for (int j = 0; j < 4; ++j) {
+            acc[i][j] = 0.0f;
+            const int gr = tx * 4 + i, gc = ty * 4 + j;
+            cv[i][j] = (gr < m && gc < n) ? __ldcg(C + (int64_t)gc * ldc + gr) : 0.0f;
+        }
     for (int k0 = 0; k0 < k; k0 += kNB) {
         // the whole 64-deep slice of both operands in one L2 round trip
         const int kc = min(kNB, k - k0);
@@ -222,16 +400,18 @@ __device__ void gemm_tile64(Smem &sm, int m, int n, int k, float alpha, const fl
         for (int i = 0; i < 4; ++i) {
             const int gr = tx * 4 + i;
             acc[i][j] *= alpha;
-            if (gr < m && gc < n) acc[i][j] += __ldcg(C + (int64_t)gc * ldc + gr);
+            if (gr < m && gc < n) acc[i][j] += cv[i][j];
         }
     }
+    if (to_smem) __syncthreads();  // the operand slices share memory with t
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int gc = ty * 4 + j;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int gr = tx * 4 + i;
-            if (gr < m && gc < n) C[(int64_t)gc * ldc + gr] = acc[i][j];
+            if (to_smem) sm.t.t[gc][gr] = acc[i][j];
+            else if (gr < m && gc < n) C[(int64_t)gc * ldc + gr] = acc[i][j];
         }
     }
     __syncthreads();
@@ -319,7 +499,10 @@ __device__ __forceinline__ void getrf64_lower_right(float (*T)[kNB + 4], float (
     }
 }
 
-__device__ __noinline__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, DevStatus *dst, int pivot_base) {
+// in_smem: the block to factor is already in sm.t.t[col][row] (gemm_tile64's
+// to_smem output), not read from D; either way the factors are written to D.
+__device__ __noinline__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, DevStatus *dst, int pivot_base,
+                                     bool in_smem = false) {
     float(*T)[kNB + 4] = sm.t.t;  // T[c][r]: the factored block, written out at the end
     volatile int *ready = sm.t.ready;
     if (threadIdx.x < 32) ready[threadIdx.x] = 0;
@@ -330,8 +513,9 @@ __device__ __noinline__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, De
         float a0[32], a1[32];
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
-            a0[j] = (j < nb && ln < nb) ? __ldcg(D + (int64_t)j * lda + ln) : 0.0f;
-            a1[j] = (j < nb && ln + 32 < nb) ? __ldcg(D + (int64_t)j * lda + ln + 32) : 0.0f;
+            a0[j] = (j < nb && ln < nb) ? (in_smem ? T[j][ln] : __ldcg(D + (int64_t)j * lda + ln)) : 0.0f;
+            a1[j] = (j < nb && ln + 32 < nb) ? (in_smem ? T[j][ln + 32] : __ldcg(D + (int64_t)j * lda + ln + 32))
+                                             : 0.0f;
         }
         float pv = __shfl_sync(full, a0[0], 0);
         float rp = rcp_rn_f32(pv);
@@ -345,8 +529,11 @@ __device__ __noinline__ void getrf64(Smem &sm, int nb, float *D, int64_t lda, De
         float b0[32], b1[32];
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
-            b0[j] = (32 + j < nb && ln < nb) ? __ldcg(D + (int64_t)(32 + j) * lda + ln) : 0.0f;
-            b1[j] = (32 + j < nb && ln + 32 < nb) ? __ldcg(D + (int64_t)(32 + j) * lda + ln + 32) : 0.0f;
+            b0[j] = (32 + j < nb && ln < nb) ? (in_smem ? T[32 + j][ln] : __ldcg(D + (int64_t)(32 + j) * lda + ln))
+                                             : 0.0f;
+            b1[j] = (32 + j < nb && ln + 32 < nb)
+                        ? (in_smem ? T[32 + j][ln + 32] : __ldcg(D + (int64_t)(32 + j) * lda + ln + 32))
+                        : 0.0f;
         }
         if (nb > 32) {
 #pragma unroll 1
@@ -434,16 +621,29 @@ __device__ __forceinline__ void trsm_rows_phase(Smem &sm, float (&x)[kNB], int k
     }
 }
 
-__device__ void trsm_rows(Smem &sm, int m, int nb, float *B, int64_t ldb, int r0, int rows = kCT) {
+// The row of B this thread solves (zero when it has none), and the solve of a
+// row loaded that way: split so a caller can issue the loads before load_tri.
+__device__ __forceinline__ void trsm_rows_load(float (&x)[kNB], int m, int nb, const float *B, int64_t ldb, int r0,
+                                               int rows) {
+    const int i = r0 + threadIdx.x;
+    const bool act = threadIdx.x < rows && i < m;
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) x[c] = (act && c < nb) ? __ldcg(B + (int64_t)c * ldb + i) : 0.0f;
+}
+__device__ __forceinline__ void trsm_rows_solve(Smem &sm, float (&x)[kNB], int m, int nb, float *B, int64_t ldb,
+                                                int r0, int rows) {
     const int i = r0 + threadIdx.x;
     if (threadIdx.x >= rows || i >= m) return;
-    float x[kNB];
-#pragma unroll
-    for (int c = 0; c < kNB; ++c) x[c] = (c < nb) ? __ldcg(B + (int64_t)c * ldb + i) : 0.0f;
     trsm_rows_phase<64>(sm, x, 0, min(nb, 16), B, ldb, i);
     trsm_rows_phase<48>(sm, x, 16, min(nb, 32), B, ldb, i);
     trsm_rows_phase<32>(sm, x, 32, min(nb, 48), B, ldb, i);
     trsm_rows_phase<16>(sm, x, 48, nb, B, ldb, i);
+}
+
+__device__ void trsm_rows(Smem &sm, int m, int nb, float *B, int64_t ldb, int r0, int rows = kCT) {
+    float x[kNB];
+    trsm_rows_load(x, m, nb, B, ldb, r0, rows);
+    trsm_rows_solve(sm, x, m, nb, B, ldb, r0, rows);
 }
 
 // One column of X = L^{-1} B (L unit lower, load_tri) in registers: x_r -=
@@ -469,15 +669,14 @@ __device__ __forceinline__ void trsm_col(Smem &sm, float (&x)[kNB], int nb, floa
 // part of the diagonal block (load_tri).  The 64 x 64 block moves through
 // shared memory (ub, over the dead t) with coalesced loads and stores;
 // threads 0..63 solve one column each.
-__device__ void trsm_cols64(Smem &sm, int ncols, int nb, float *B, int64_t ldb, int c0) {
-    {
-        float v[16];
-        load_block64(v, B + (int64_t)c0 * ldb, ldb, nb, ncols - c0);
+// v[0..15]: the block, already loaded by load_block64(v, B + c0 ldb, ldb, nb, ncols - c0)
+template <int N>
+__device__ void trsm_cols64_loaded(Smem &sm, const float (&v)[N], int ncols, int nb, float *B, int64_t ldb,
+                                   int c0) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const int idx = threadIdx.x + kCT * q;
-            sm.t.ub[idx / kNB][idx % kNB] = v[q];
-        }
+    for (int q = 0; q < 16; ++q) {
+        const int idx = threadIdx.x + kCT * q;
+        sm.t.ub[idx / kNB][idx % kNB] = v[q];
     }
     __syncthreads();
     if (threadIdx.x < kNB) {
@@ -493,6 +692,12 @@ __device__ void trsm_cols64(Smem &sm, int ncols, int nb, float *B, int64_t ldb, 
         if (k < nb && c0 + j < ncols) B[(int64_t)(c0 + j) * ldb + k] = sm.t.ub[j][k];
     }
     __syncthreads();
+}
+
+__device__ void trsm_cols64(Smem &sm, int ncols, int nb, float *B, int64_t ldb, int c0) {
+    float v[16];
+    load_block64(v, B + (int64_t)c0 * ldb, ldb, nb, ncols - c0);
+    trsm_cols64_loaded(sm, v, ncols, nb, B, ldb, c0);
 }
 
 // Inverse of the 64 x 64 diagonal block `blk` of an upper non-unit (upper = true)
@@ -552,7 +757,9 @@ struct Job {
     int64_t ldc, sC;
 };
 
-__device__ void run_jobs(Smem &sm, const Job *jobs, int njobs, int cta, int ncta) {
+// sv (when not null, with at least sizeof(SmemGV) bytes behind it): tiles
+// whose operands allow it run as gemm_tile_v.
+__device__ void run_jobs(Smem &sm, const Job *jobs, int njobs, int cta, int ncta, SmemGV *sv = nullptr) {
     int tiles[4] = {0, 0, 0, 0}, total = 0;
     for (int q = 0; q < njobs; ++q) {
         tiles[q] = ((jobs[q].m + GBM - 1) / GBM) * ((jobs[q].n + GBN - 1) / GBN) * jobs[q].batch;
@@ -571,8 +778,12 @@ __device__ void run_jobs(Smem &sm, const Job *jobs, int njobs, int cta, int ncta
         if (J.tri == 2) ke = min(J.K, m0 + GBM);
         if (J.tri == 3) ke = min(J.K, n0 + GBN);
         if (J.tri == 4) kb = n0;
-        gemm_tile(sm, J.m, J.n, kb, ke, J.alpha, J.A + J.sA * z, J.lda, J.B + J.sB * z, J.ldb, false,
-                  J.C + J.sC * z, J.ldc, m0, n0);
+        const float *Az = J.A + J.sA * z, *Bz = J.B + J.sB * z;
+        float *Cz = J.C + J.sC * z;
+        if (sv && gemm_tile_v_ok(Az, J.lda, Bz, J.ldb, Cz, J.ldc, kb))
+            gemm_tile_v(*sv, J.m, J.n, kb, ke, J.alpha, Az, J.lda, Bz, J.ldb, false, Cz, J.ldc, m0, n0);
+        else
+            gemm_tile(sm, J.m, J.n, kb, ke, J.alpha, Az, J.lda, Bz, J.ldb, false, Cz, J.ldc, m0, n0);
     }
 }
 
@@ -587,7 +798,8 @@ __device__ void run_jobs(Smem &sm, const Job *jobs, int njobs, int cta, int ncta
 // blocks of size s_stop (the caller finishes those levels elsewhere).
 template <typename Sync>
 __device__ bool tri_inverses(Smem &sm, int n, const float *A, int64_t lda, float *XU, float *XL, int64_t ldx,
-                             float *tmpU, float *tmpL, int cta, int G, Sync sync, int s_stop = 0) {
+                             float *tmpU, float *tmpL, int cta, int G, Sync sync, int s_stop = 0,
+                             SmemGV *sv = nullptr) {
     const int nsteps = (n + kNB - 1) / kNB;
     // invert the diagonal 64 x 64 blocks and zero the opposite block-triangle
     const int nblk = nsteps;
@@ -623,7 +835,7 @@ __device__ bool tri_inverses(Smem &sm, int n, const float *A, int64_t lda, float
             jb[nj++] = Job{c, S, S, 1, 4, 1.0f, L + (r0 + S) + r0 * ldl, ldl, 0, XL + r0 + r0 * ldx, ldx, 0,
                            tmpL + np * SS, c, 0};
         }
-        run_jobs(sm, jb, nj, cta, G);
+        run_jobs(sm, jb, nj, cta, G, sv);
         if (!sync(24)) return false;
         // phase b:  X12 = -inv(U11) T_U;  X21 = -inv(L22) T_L
         nj = 0;
@@ -638,7 +850,7 @@ __device__ bool tri_inverses(Smem &sm, int n, const float *A, int64_t lda, float
             jb[nj++] = Job{c, S, c, 1, 2, -1.0f, XL + (r0 + S) + (r0 + S) * ldx, ldx, 0, tmpL + np * SS, c, 0,
                            XL + (r0 + S) + r0 * ldx, ldx, 0};
         }
-        run_jobs(sm, jb, nj, cta, G);
+        run_jobs(sm, jb, nj, cta, G, sv);
         if (!sync(25)) return false;
     }
     return true;

@@ -88,11 +88,15 @@ __device__ bool grid_sync(const Ctl &c, unsigned int &epoch, int where) {
     return ok_sh != 0;
 }
 
+// dynamic shared memory: the Smem union and gemm_tile_v's two slices share it
+constexpr size_t kCoopSmem = sizeof(Smem) > sizeof(SmemGV) ? sizeof(Smem) : sizeof(SmemGV);
+
 __global__ void __launch_bounds__(kCT, 1)
 diag_factor_kernel(int n, float *A, int64_t lda, float *XU, float *XL, int64_t ldx, float *tmpU,
                    float *tmpL, Ctl ctl, int pivot_base, int inv_stop) {
     extern __shared__ __align__(16) unsigned char coop_smem[];
     Smem &sm = *reinterpret_cast<Smem *>(coop_smem);
+    SmemGV &sv = *reinterpret_cast<SmemGV *>(coop_smem);  // the same memory, for gemm_tile_v
     const int G = gridDim.x, cta = blockIdx.x;
     unsigned int epoch = 0;
     const int nsteps = (n + kNB - 1) / kNB;
@@ -111,8 +115,17 @@ diag_factor_kernel(int n, float *A, int64_t lda, float *XU, float *XL, int64_t l
         // strips
         const int lit = (rem + kNB - 1) / kNB, uit = (rem + kNB - 1) / kNB;  // 64-row / 64-column items
         if (cta < lit + uit) {
+            // the first item's operands are requested before the diagonal
+            // block, so the two L2 round trips overlap
+            // (a row of the L strip in x, or the U strip block in x[0..15])
+            float x[kNB];
+            const int it0 = cta;
+            if (it0 < lit) trsm_rows_load(x, rem, nbk, Lstrip, lda, it0 * kNB, kNB);
+            else load_block64(x, Ustrip + (int64_t)(it0 - lit) * kNB * lda, lda, nbk, rem - (it0 - lit) * kNB);
             load_tri(sm, nbk, Djj, lda);
-            for (int it = cta; it < lit + uit; it += G) {
+            if (it0 < lit) trsm_rows_solve(sm, x, rem, nbk, Lstrip, lda, it0 * kNB, kNB);
+            else trsm_cols64_loaded(sm, x, rem, nbk, Ustrip, lda, (it0 - lit) * kNB);
+            for (int it = cta + G; it < lit + uit; it += G) {
                 if (it < lit) trsm_rows(sm, rem, nbk, Lstrip, lda, it * kNB, kNB);
                 else trsm_cols64(sm, rem, nbk, Ustrip, lda, (it - lit) * kNB);
             }
@@ -125,15 +138,21 @@ diag_factor_kernel(int n, float *A, int64_t lda, float *XU, float *XL, int64_t l
         const int tm = (rem + GBM - 1) / GBM;
         const int ntiles = tm * tm;
         const int dn = min(kNB, rem);
-        if (cta == 0) {
-            gemm_tile64(sm, dn, dn, nbk, -1.0f, Lstrip, lda, Ustrip, lda, C, lda);
-            getrf64(sm, dn, C, lda, ctl.dst, pivot_base + jb + nbk);
+        if (cta == 0) {  // the updated block stays in shared memory for the factor
+            gemm_tile64(sm, dn, dn, nbk, -1.0f, Lstrip, lda, Ustrip, lda, C, lda, /*to_smem=*/true);
+            getrf64(sm, dn, C, lda, ctl.dst, pivot_base + jb + nbk, /*in_smem=*/true);
         }
         if (G == 1 || cta > 0) {
             const int first = G == 1 ? 0 : cta - 1, stride = G == 1 ? 1 : G - 1;
-            for (int t = first; t < ntiles; t += stride)
-                gemm_tile(sm, rem, rem, 0, nbk, -1.0f, Lstrip, lda, Ustrip, lda, true, C, lda,
-                          (t % tm) * GBM, (t / tm) * GBN, t == 0 ? kNB : 0);
+            const bool vec = gemm_tile_v_ok(Lstrip, lda, Ustrip, lda, C, lda, 0);
+            for (int t = first; t < ntiles; t += stride) {
+                if (vec)
+                    gemm_tile_v(sv, rem, rem, 0, nbk, -1.0f, Lstrip, lda, Ustrip, lda, true, C, lda,
+                                (t % tm) * GBM, (t / tm) * GBN, t == 0 ? kNB : 0);
+                else
+                    gemm_tile(sm, rem, rem, 0, nbk, -1.0f, Lstrip, lda, Ustrip, lda, true, C, lda,
+                              (t % tm) * GBM, (t / tm) * GBN, t == 0 ? kNB : 0);
+            }
         }
         if (!grid_sync(ctl, epoch, 22)) return;
     }
@@ -141,7 +160,7 @@ diag_factor_kernel(int n, float *A, int64_t lda, float *XU, float *XL, int64_t l
 
     // ---------------- triangular inverses ----------------
     auto gsync = [&](int where) { return grid_sync(ctl, epoch, where); };
-    tri_inverses(sm, n, A, lda, XU, XL, ldx, tmpU, tmpL, cta, G, gsync, inv_stop);
+    tri_inverses(sm, n, A, lda, XU, XL, ldx, tmpU, tmpL, cta, G, gsync, inv_stop, &sv);
 }
 
 int coop_grid(int device) {
@@ -150,8 +169,8 @@ int coop_grid(int device) {
     if (!cached[device]) {
         int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        cudaFuncSetAttribute(diag_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, diag_factor_kernel, kCT, sizeof(Smem));
+        cudaFuncSetAttribute(diag_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoopSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, diag_factor_kernel, kCT, kCoopSmem);
         cached[device] = per_sm > 0 ? sms : -1;
     }
     return cached[device];
@@ -217,7 +236,7 @@ mxp_status launch_diag_factor(int n, float *A, int64_t lda, float *XU, float *XL
     Ctl ctl{sync_words, reinterpret_cast<int *>(sync_words + 1), dst};
     void *args[] = {&n, &A, &lda, &XU, &XL, &ldx, &tmpU, &tmpL, &ctl, &pivot_base, &inv_stop};
     MXP_CUDA(cudaLaunchCooperativeKernel((const void *)diag_factor_kernel, dim3(grid), dim3(kCT), args,
-                                         sizeof(Smem), st));
+                                         kCoopSmem, st));
     MXP_LAUNCHED();
     return MXP_OK;
 }
