@@ -757,12 +757,14 @@ def run_batched(args):
 # ---------------------------------------------------------------------------
 def run_grid(args):
     """Credited TFLOP/s of ONE system of order --n factored and refined by a
-    P x Q grid of GPUs (openmxp_b200.grid: block-cyclic layout, the factored
-    diagonal block and the low-precision panels broadcast over NCCL along
-    process rows and columns, STRSM panels, tcgen05 Schur update, refinement
-    with the local regenerating GEMV summed over all ranks).  One step = one
-    solve of the freshly regenerated local blocks; the time is LU +
-    refinement, max over ranks."""
+    P x Q grid of GPUs (openmxp_b200.grid: block-cyclic layout, the diagonal
+    block's triangular inverses (or, with --trsm simt, the factored block) and
+    the low-precision panels broadcast over NCCL along process rows and
+    columns, panels by inverse on the tensor cores, depth-1 look-ahead unless
+    --no-lookahead, tcgen05 Schur update, refinement with the local
+    regenerating GEMV summed over all ranks).  One step = one solve of the
+    freshly regenerated local blocks; the time is LU + refinement, max over
+    ranks."""
     import torch
 
     import openmxp_b200 as mxp
@@ -777,7 +779,9 @@ def run_grid(args):
     form = mxp.FORMS[args.form]
     g = G.ProcessGrid(P, Q, dist=dist)
     be = G.CudaBackend(args.b, form)
-    s = G.BlockCyclicSolver(g, args.n, args.b, args.seed, be, form=form, diag_rule=args.diag_rule)
+    gtrsm = {"tensor": "split", "single": "single", "simt": "strsm"}[args.trsm]
+    s = G.BlockCyclicSolver(g, args.n, args.b, args.seed, be, form=form, diag_rule=args.diag_rule, trsm=gtrsm,
+                            lookahead=not args.no_lookahead)
     h_rhs = s.rhs.cpu().pin_memory()
     h_x = torch.empty(args.n, dtype=torch.float64).pin_memory()
 
@@ -819,9 +823,12 @@ def run_grid(args):
            "config": {"workload": f"HPL-MxP solve N={args.n} B={args.b} seed={args.seed} {args.form}-Schur + "
                                   f"FP64 classic IR over a {P}x{Q} process grid (2D block-cyclic)",
                       "n": args.n, "b": args.b, "seed": args.seed, "form": args.form, "grid": f"{P}x{Q}",
-                      "parallelism": f"2D block-cyclic {P}x{Q}, NCCL broadcasts of the factored diagonal "
-                                     "block and the low-precision panels",
-                      "trsm": "STRSM (SIMT FP32) on the local panels",
+                      "parallelism": f"2D block-cyclic {P}x{Q}, NCCL broadcasts of the diagonal block "
+                                     "(its inverses) and the low-precision panels",
+                      "trsm": {"split": "by inverse, three split-BF16 tensor-core products",
+                               "single": "by inverse, one BF16 tensor-core product",
+                               "strsm": "STRSM (SIMT FP32)"}[gtrsm] + " on the local panels",
+                      "lookahead": int(s.lookahead),
                       "l2": "inputs larger than L2" if args.n * args.n * 4 // world > 126e6 else "fits L2"},
            "ir": {"iterations": st.iterations, "converged": int(st.converged), "hpl_harness": st.hpl_harness,
                   "residual": st.residual},
@@ -861,6 +868,8 @@ def parse(argv=None):
                          "(its panels are E4M3 next), tensor otherwise")
     ap.add_argument("--compare-trsm", choices=["tensor", "single", "simt"], default="tensor",
                     help="panel TRSM of the --compare arm (the plain method: FP32-accurate)")
+    ap.add_argument("--no-lookahead", action="store_true",
+                    help="--grid: update the whole trailing matrix before forming the next panel")
     ap.add_argument("--no-same-trsm", action="store_true",
                     help="skip the third arm: --form again with --compare-trsm (the like-for-like ratio)")
     ap.add_argument("--e2e-steps", type=int, default=2)

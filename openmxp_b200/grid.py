@@ -16,15 +16,27 @@ between GPUs, gloo for the CPU tests) in place of MPI:
   vectors on every process;
 * LU step k (panel_lu_async_wGPU's loop body): the owner of block (k, k)
   factors it (mxp_getrf_nopiv_inv, keeping both triangular inverses for the
-  refinement); the factored block goes along its process row and column
-  (broadcast_pivlu, panel_trf.hpp:60-107); the processes of column k mod Q
-  solve their rows of the L panel (STRSM right-upper) and cast them, those of
-  row k mod P their columns of the U panel (STRSM left-lower-unit); the
-  low-precision L panel is broadcast along each process row and the R panel
-  along each process column (broadcast_left/right_panels, panel_trf.hpp:
-  127-170); every process applies the tcgen05 Schur update to its trailing
-  local blocks.  A received panel lands in the process's own device memory
-  before the Schur kernel reads it (no kernel reads another GPU's memory);
+  refinement).  Panel solves by inverse (trsm "split" or "single", the
+  reference's -alt path, panel_trf_gdirect.hpp:73-142): inv(U_kk) goes along
+  the owner's process column and inv(L_kk) along its process row, and the
+  processes of column k mod Q form their rows of the L panel as A21 inv(U_kk)
+  and those of row k mod P their columns of the U panel as inv(L_kk) A12 on
+  the tensor cores (mxp_trsm_inv_*); with trsm "strsm" the factored block goes
+  along both (broadcast_pivlu, panel_trf.hpp:60-107) for SIMT STRSMs.  The
+  panels are cast, the low-precision L panel is broadcast along each process
+  row and the R panel along each process column (broadcast_left/right_panels,
+  panel_trf.hpp:127-170), and every process applies the tcgen05 Schur update
+  to its trailing local blocks.  A received panel lands in the process's own
+  device memory before the Schur kernel reads it (no kernel reads another
+  GPU's memory);
+* look-ahead (depth 1, panel_trf.hpp:470-867 and the gdirect driver's
+  panel_trf_gdirect.hpp:777-1172): step k's update is applied first to block
+  column k+1 and block row k+1, panel k+1 is formed and its broadcasts are
+  started, and only then is the rest of step k's trailing update applied, so
+  the panel broadcasts run beside it (asynchronous collectives on the
+  communication stream; two sets of panel buffers).  Every element still
+  receives its updates in step order, so the factors are the same bit for bit
+  with and without it;
 * refinement (iterative_refinement.hpp:141-171): x, r and the corrections are
   whole-length FP64 vectors on every process; the residual is the local
   regenerating GEMV (mxp_otf_gemv_local) summed over all processes
@@ -109,14 +121,22 @@ class ProcessGrid:
     def rank_of(self, prow: int, pcol: int) -> int:
         return prow + pcol * self.nprow
 
-    # collectives (no-ops on a one-process grid or a one-member group)
-    def bcast_row(self, t, root_col: int) -> None:
+    # collectives (no-ops on a one-process grid or a one-member group).  With
+    # async_op the broadcast is only started: the returned handles (a list,
+    # empty when nothing was issued) are waited on before the tensor is used.
+    def bcast_row(self, t, root_col: int, async_op: bool = False):
         if self.npcol > 1:
-            self.dist.broadcast(t, src=self.rank_of(self.myrow, root_col), group=self.row_group)
+            w = self.dist.broadcast(t, src=self.rank_of(self.myrow, root_col), group=self.row_group,
+                                    async_op=async_op)
+            return [w] if async_op else []
+        return []
 
-    def bcast_col(self, t, root_row: int) -> None:
+    def bcast_col(self, t, root_row: int, async_op: bool = False):
         if self.nprow > 1:
-            self.dist.broadcast(t, src=self.rank_of(root_row, self.mycol), group=self.col_group)
+            w = self.dist.broadcast(t, src=self.rank_of(root_row, self.mycol), group=self.col_group,
+                                    async_op=async_op)
+            return [w] if async_op else []
+        return []
 
     def reduce_row(self, t, root_col: int) -> None:
         if self.npcol > 1:
@@ -144,7 +164,8 @@ class CudaBackend:
         self.lib = lib()
         self.dev = torch.device("cuda", torch.cuda.current_device())
         self.form = form
-        self.ws = Workspace(b, b, form)
+        # on this process's GPU (one process per GPU: the current device)
+        self.ws = Workspace(b, b, form, device=self.dev.index)
 
     # storage
     def empty(self, numel: int, dtype):
@@ -188,8 +209,25 @@ class CudaBackend:
         self._ck(self.lib.mxp_getrf_nopiv_inv(b, self._p(A, off), lda, self._p(XU), self._p(XL), b,
                                               self.ws.handle, self._s()))
 
+    def reserve(self, rows: int) -> None:
+        """Make the workspace hold panel products of up to `rows` rows (the
+        TRSM by inverse stages its operands there)."""
+        if rows > self.ws.n - self.ws.b:
+            from . import Workspace
+            b = self.ws.b
+            self.ws.close()
+            self.ws = Workspace(rows + b, b, self.form, device=self.dev.index)
+
     def trsm_right_upper(self, m: int, b: int, U, ldu: int, A, off: int, lda: int) -> None:
         self._ck(self.lib.mxp_trsm_right_upper(m, b, self._p(U), ldu, self._p(A, off), lda, self._s()))
+
+    def trsm_inv_right_upper(self, m: int, b: int, XU, ldx: int, A, off: int, lda: int, single: bool) -> None:
+        self._ck(self.lib.mxp_trsm_inv_right_upper(m, b, self._p(XU), ldx, self._p(A, off), lda, int(single),
+                                                   self.ws.handle, self._s()))
+
+    def trsm_inv_left_lower(self, b: int, ncols: int, XL, ldx: int, A, off: int, lda: int, single: bool) -> None:
+        self._ck(self.lib.mxp_trsm_inv_left_lower(b, ncols, self._p(XL), ldx, self._p(A, off), lda, int(single),
+                                                  self.ws.handle, self._s()))
 
     def trsm_left_lower_unit(self, b: int, ncols: int, L, ldl: int, A, off: int, lda: int) -> None:
         self._ck(self.lib.mxp_trsm_left_lower_unit(b, ncols, self._p(L), ldl, self._p(A, off), lda, self._s()))
@@ -236,32 +274,49 @@ class BlockCyclicSolver:
     refinement.  `backend` supplies the per-process kernels (CudaBackend on
     GPUs); torch tensors hold every buffer."""
 
+    TRSMS = ("split", "single", "strsm")
+
     def __init__(self, grid: ProcessGrid, n: int, b: int, seed: int, backend, form: int = FORM_FP16,
-                 diag_rule: int = 0):
+                 diag_rule: int = 0, trsm: str = "split", lookahead: bool = True):
+        """trsm: the panel solves, "split" (three split-BF16 products against
+        the FP32 inverse, near FP32), "single" (one BF16 product) or "strsm"
+        (FP32 SIMT triangular solves); lookahead: depth-1 look-ahead (needs
+        b % 128 == 0 in the FP8 form, whose panel scales are per 128 rows;
+        off otherwise)."""
         if n <= 0 or b <= 0 or n % b:
             raise ValueError("n must be a positive multiple of b")
+        if trsm not in self.TRSMS:
+            raise ValueError(f"trsm must be one of {self.TRSMS}")
         import torch
         self.torch = torch
         self.g, self.n, self.b, self.seed, self.form = grid, n, b, seed, form
         self.diag_rule = diag_rule
+        self.trsm = trsm
+        self.lookahead = bool(lookahead) and (form != FORM_FP8 or b % 128 == 0)
         self.be = backend
         self.nb = n // b
         self.mloc = local_extent(n, b, grid.nprow, grid.myrow)
         self.nloc = local_extent(n, b, grid.npcol, grid.mycol)
         self.lda = max(self.mloc, 1)
+        if trsm != "strsm" and hasattr(backend, "reserve"):
+            backend.reserve(max(self.mloc, self.nloc))
         self.A = backend.empty(self.lda * self.nloc, torch.float32)
         self.d, self.rhs = backend.vectors(n, seed, diag_rule)
         if self.mloc and self.nloc:
             backend.matgen_local(grid, n, b, seed, self.d, self.A, self.lda)
         ldk, es, nsc = backend.panel_layout(self.mloc, b)
         self.ldk_l, self.es = ldk, es
-        self.Lp = backend.empty(self.mloc * ldk * es, torch.uint8)
-        self.Ls = backend.empty(nsc, torch.uint8) if nsc else None
         ldk_r, _, nsc_r = backend.panel_layout(self.nloc, b)
         self.ldk_r = ldk_r
-        self.Rp = backend.empty(self.nloc * ldk_r * es, torch.uint8)
-        self.Rs = backend.empty(nsc_r, torch.uint8) if nsc_r else None
+        self.sct = -(-b // 128)  # FP8 scale bytes per 128 panel rows
+        nbuf = 2 if self.lookahead else 1
+        self.Lp = [backend.empty(self.mloc * ldk * es, torch.uint8) for _ in range(nbuf)]
+        self.Ls = [backend.empty(nsc, torch.uint8) if nsc else None for _ in range(nbuf)]
+        self.Rp = [backend.empty(self.nloc * ldk_r * es, torch.uint8) for _ in range(nbuf)]
+        self.Rs = [backend.empty(nsc_r, torch.uint8) if nsc_r else None for _ in range(nbuf)]
         self.D = backend.empty(b * b, torch.float32)
+        self.XUb = backend.empty(b * b, torch.float32)  # inv(U_kk) on the owner's process column
+        self.XLb = backend.empty(b * b, torch.float32)  # inv(L_kk) on the owner's process row
         self.diag = {}  # k -> (unit-lower L_kk, U_kk, inv(L_kk), inv(U_kk)) on the owner
 
     def regenerate(self) -> None:
@@ -278,48 +333,113 @@ class BlockCyclicSolver:
         return lrow + lcol * self.lda
 
     # --- LU ----------------------------------------------------------------
-    def factor(self) -> None:
+    def _start(self, k: int) -> tuple[int, int, int, int]:
+        """(first local row of the blocks below k, first local column of the
+        blocks right of k, their counts of rows and columns)."""
+        g, b = self.g, self.b
+        r0 = blocks_upto(k, g.nprow, g.myrow) * b
+        c0 = blocks_upto(k, g.npcol, g.mycol) * b
+        return r0, c0, self.mloc - r0, self.nloc - c0
+
+    def _form_panel(self, k: int, buf: int) -> list:
+        """Step k's panels into panel buffer `buf`: diagonal factor (and
+        inverses) on the owner, the triangle or its inverse along the owner's
+        row and column, the panel solves, the casts; then the panel
+        broadcasts are started.  Returns their handles."""
         torch, g, b, be = self.torch, self.g, self.b, self.be
-        for k in range(self.nb):
-            io, jo = self.owner(k)
-            lik, ljk = k // g.nprow, k // g.npcol
-            r0 = blocks_upto(k, g.nprow, g.myrow) * b   # first local row of blocks below k
-            c0 = blocks_upto(k, g.npcol, g.mycol) * b   # first local column right of k
-            mb, nr = self.mloc - r0, self.nloc - c0
-            if g.myrow == io and g.mycol == jo:
-                off = self._off(lik * b, ljk * b)
-                XU, XL = be.empty(b * b, torch.float32), be.empty(b * b, torch.float32)
-                be.getrf_inv(b, self.A, off, self.lda, XU, XL)
-                blk = self.A.as_strided((b, b), (1, self.lda), off)  # [r, c] of the factored block
-                self.D.view(b, b).copy_(blk.t())                     # D column-major, ld = b
-                Dm = self.D.view(b, b).t()                           # Dm[r, c]
-                Lf = torch.tril(Dm, -1) + torch.eye(b, dtype=Dm.dtype, device=Dm.device)
-                Uf = torch.triu(Dm)
-                # column-major copies for the block GEMVs
-                self.diag[k] = (Lf.t().contiguous().view(-1), Uf.t().contiguous().view(-1), XL, XU)
-            if g.myrow == io:
-                g.bcast_row(self.D, jo)   # L_kk to the U-panel solves of this process row
+        io, jo = self.owner(k)
+        lik, ljk = k // g.nprow, k // g.npcol
+        r0, c0, mb, nr = self._start(k)
+        inv = self.trsm != "strsm"
+        single = self.trsm == "single"
+        if g.myrow == io and g.mycol == jo:
+            off = self._off(lik * b, ljk * b)
+            XU, XL = be.empty(b * b, torch.float32), be.empty(b * b, torch.float32)
+            be.getrf_inv(b, self.A, off, self.lda, XU, XL)
+            blk = self.A.as_strided((b, b), (1, self.lda), off)  # [r, c] of the factored block
+            self.D.view(b, b).copy_(blk.t())                     # D column-major, ld = b
+            Dm = self.D.view(b, b).t()                           # Dm[r, c]
+            Lf = torch.tril(Dm, -1) + torch.eye(b, dtype=Dm.dtype, device=Dm.device)
+            Uf = torch.triu(Dm)
+            # column-major copies for the block GEMVs
+            self.diag[k] = (Lf.t().contiguous().view(-1), Uf.t().contiguous().view(-1), XL, XU)
+            if inv:
+                self.XUb.copy_(XU)
+                self.XLb.copy_(XL)
+        if inv:
             if g.mycol == jo:
-                g.bcast_col(self.D, io)   # U_kk to the L-panel solves of this process column
-            if g.mycol == jo and mb > 0:
-                off = self._off(r0, ljk * b)
+                g.bcast_col(self.XUb, io)  # inv(U_kk) to the L-panel products of this process column
+            if g.myrow == io:
+                g.bcast_row(self.XLb, jo)  # inv(L_kk) to the U-panel products of this process row
+        else:
+            if g.myrow == io:
+                g.bcast_row(self.D, jo)    # L_kk to the U-panel solves of this process row
+            if g.mycol == jo:
+                g.bcast_col(self.D, io)    # U_kk to the L-panel solves of this process column
+        Lp, Ls, Rp, Rs = self.Lp[buf], self.Ls[buf], self.Rp[buf], self.Rs[buf]
+        if g.mycol == jo and mb > 0:
+            off = self._off(r0, ljk * b)
+            if inv:
+                be.trsm_inv_right_upper(mb, b, self.XUb, b, self.A, off, self.lda, single)
+            else:
                 be.trsm_right_upper(mb, b, self.D, b, self.A, off, self.lda)
-                be.cast_left(mb, b, self.A, off, self.lda, self.Lp, self.ldk_l, self.Ls)
-            if g.myrow == io and nr > 0:
-                off = self._off(lik * b, c0)
+            be.cast_left(mb, b, self.A, off, self.lda, Lp, self.ldk_l, Ls)
+        if g.myrow == io and nr > 0:
+            off = self._off(lik * b, c0)
+            if inv:
+                be.trsm_inv_left_lower(b, nr, self.XLb, b, self.A, off, self.lda, single)
+            else:
                 be.trsm_left_lower_unit(b, nr, self.D, b, self.A, off, self.lda)
-                be.cast_right(nr, b, self.A, off, self.lda, self.Rp, self.ldk_r, self.Rs)
-            if mb > 0:  # uniform across the process row
-                g.bcast_row(self.Lp[: mb * self.ldk_l * self.es], jo)
-                if self.Ls is not None:
-                    g.bcast_row(self.Ls[: (-(-mb // 128)) * (-(-b // 128))], jo)
-            if nr > 0:  # uniform across the process column
-                g.bcast_col(self.Rp[: nr * self.ldk_r * self.es], io)
-                if self.Rs is not None:
-                    g.bcast_col(self.Rs[: (-(-nr // 128)) * (-(-b // 128))], io)
-            if mb > 0 and nr > 0:
-                be.schur(mb, nr, b, self.Lp, self.ldk_l, self.Ls, self.Rp, self.ldk_r, self.Rs, self.A,
-                         self._off(r0, c0), self.lda)
+            be.cast_right(nr, b, self.A, off, self.lda, Rp, self.ldk_r, Rs)
+        works = []
+        if mb > 0:  # uniform across the process row
+            works += g.bcast_row(Lp[: mb * self.ldk_l * self.es], jo, async_op=True)
+            if Ls is not None:
+                works += g.bcast_row(Ls[: (-(-mb // 128)) * self.sct], jo, async_op=True)
+        if nr > 0:  # uniform across the process column
+            works += g.bcast_col(Rp[: nr * self.ldk_r * self.es], io, async_op=True)
+            if Rs is not None:
+                works += g.bcast_col(Rs[: (-(-nr // 128)) * self.sct], io, async_op=True)
+        return works
+
+    def _schur(self, k: int, buf: int, dr: int, dc: int, m: int, ncols: int) -> None:
+        """Step k's update of the trailing rows [r0 + dr, r0 + dr + m) x
+        columns [c0 + dc, c0 + dc + ncols) (r0, c0: the first trailing local
+        row and column), from panel rows dr.. and dc.. of buffer `buf`."""
+        if m <= 0 or ncols <= 0:
+            return
+        r0, c0, _, _ = self._start(k)
+        es = self.es
+        Ls, Rs = self.Ls[buf], self.Rs[buf]
+        self.be.schur(m, ncols, self.b, self.Lp[buf][dr * self.ldk_l * es:], self.ldk_l,
+                      None if Ls is None else Ls[(dr // 128) * self.sct:],
+                      self.Rp[buf][dc * self.ldk_r * es:], self.ldk_r,
+                      None if Rs is None else Rs[(dc // 128) * self.sct:],
+                      self.A, self._off(r0 + dr, c0 + dc), self.lda)
+
+    def factor(self) -> None:
+        g, b = self.g, self.b
+        works = self._form_panel(0, 0)
+        for k in range(self.nb):
+            for w in works:
+                w.wait()
+            works = []
+            buf = k % 2 if self.lookahead else 0
+            _, _, mb, nr = self._start(k)
+            nxt = k + 1 < self.nb
+            if nxt and self.lookahead:
+                # block column k+1 and block row k+1 first (those of this
+                # process, when it owns them), then panel k+1, then the rest
+                ac = b if g.mycol == (k + 1) % g.npcol else 0
+                ar = b if g.myrow == (k + 1) % g.nprow else 0
+                self._schur(k, buf, 0, 0, mb, ac)
+                self._schur(k, buf, 0, ac, ar, nr - ac)
+                works = self._form_panel(k + 1, (k + 1) % 2)
+                self._schur(k, buf, ar, ac, mb - ar, nr - ac)
+            else:
+                self._schur(k, buf, 0, 0, mb, nr)
+                if nxt:
+                    works = self._form_panel(k + 1, 0)
 
     # --- triangular solves over the grid ----------------------------------
     def _diag_solve(self, k: int, t, lower: bool):

@@ -2,8 +2,15 @@
 tests of the 2D block-cyclic driver.  Test infrastructure only: every step is
 the oracle's restatement (oracle/mxp_oracle.c) on torch CPU tensors, so the
 driver's schedule, ownership and collectives run unchanged across CPU ranks.
-Panels stay FP32 here (4-byte elements); the Schur update quantises them to
-the form (orc_schur_update), exactly as the oracle's single-process LU does.
+Panels stay FP32 here (4-byte elements) in the product's panel layout (row i
+of a panel holds its K values contiguously, ld = b), so the driver's row
+offsets into them work unchanged; the Schur update quantises them to the form
+(orc_schur_update), exactly as the oracle's single-process LU does.  The
+panel products of the TRSM by inverse are the same routine on a zero C
+(C = -quant(P) quant(X), negated back exactly): the operands quantised as the
+tensor-core products quantise them (BF16, or hi|hi|lo x hi|lo|hi split BF16)
+and summed in FP32 in a fixed order, so every element's value depends only
+on its own row or column, whatever the grid.
 """
 from __future__ import annotations
 
@@ -13,6 +20,7 @@ import numpy as np
 import torch
 
 from oracle import oracle as O
+from oracle.blocked import FORM_BF16
 
 
 class OracleBackend:
@@ -69,19 +77,38 @@ class OracleBackend:
     def trsm_left_lower_unit(self, b, ncols, Lm, ldl, A, off, lda):
         self.L.orc_trsm_llnu(b, ncols, self._p(Lm), ldl, self._p(A, off), lda)
 
+    def _product(self, m, ncols, P, ldp, X, ldx, single, A, off, lda):
+        """A block (m x ncols at off) = P (m x K) X (K x ncols), K = b, both
+        quantised as the TRSM by inverse quantises them."""
+        tform = FORM_BF16 if single else O.FORM_BF16X2
+        C = np.zeros((ncols, m), np.float32)  # column-major m x ncols
+        self.L.orc_schur_update(tform, m, ncols, self.b, P, ldp, X, ldx, C.ctypes.data, m)
+        A.as_strided((ncols, m), (lda, 1), off).numpy()[:] = -C
+
+    def trsm_inv_right_upper(self, m, b, XU, ldx, A, off, lda, single):
+        P = np.array(self._block(A, off, lda, m, b))  # [k, i]: column-major m x b, ld = m
+        self._product(m, b, P.ctypes.data, m, self._p(XU), ldx, single, A, off, lda)
+
+    def trsm_inv_left_lower(self, b, ncols, XL, ldx, A, off, lda, single):
+        B = np.array(self._block(A, off, lda, b, ncols))  # [j, k]: column-major b x ncols, ld = b
+        self._product(b, ncols, self._p(XL), ldx, B.ctypes.data, b, single, A, off, lda)
+
     def _block(self, A, off, lda, m, ncols):
         return A.as_strided((ncols, m), (lda, 1), off).numpy()  # [c, r]
 
     def cast_left(self, m, b, A, off, lda, out, ldk, scales):
-        # the L panel column-major m x b, ld = m
-        out.view(torch.float32)[: m * b].numpy().reshape(b, m)[:] = self._block(A, off, lda, m, b)
+        # row i of the L panel: its b values of K
+        out.view(torch.float32)[: m * b].numpy().reshape(m, b)[:] = self._block(A, off, lda, m, b).T
 
     def cast_right(self, ncols, b, A, off, lda, out, ldk, scales):
-        # the U panel column-major b x ncols, ld = b
+        # row j of the R panel: column j of the U panel, its b values of K
         out.view(torch.float32)[: ncols * b].numpy().reshape(ncols, b)[:] = self._block(A, off, lda, b, ncols)
 
     def schur(self, m, ncols, b, Lp, ldl, ls, Rp, ldr, rs, A, off, lda):
-        self.L.orc_schur_update(self.form, m, ncols, b, self._p(Lp.view(torch.float32)), m,
+        # orc_schur_update takes L column-major (m x b) and U as K x ncols
+        # column-major, which is the R panel's layout (ld = b)
+        Lcm = np.asfortranarray(Lp.view(torch.float32)[: m * b].numpy().reshape(m, b))
+        self.L.orc_schur_update(self.form, m, ncols, b, Lcm.ctypes.data, m,
                                 self._p(Rp.view(torch.float32)), b, self._p(A, off), lda)
 
     def otf_gemv_local(self, g, n, b, seed, d, alpha, x, y):

@@ -9,9 +9,10 @@ gloo tests on the CPU; every call here has one GPU).
   mxp_otf_gemv's product (FP64 rounding of different summation orders);
 - mxp_block_gemv against an FP64 torch product;
 - BlockCyclicSolver on a 1 x 1 grid with the CUDA backend: factors bit for bit
-  equal to mxp_panel_lu run with the same steps (STRSM panels, one panel per
-  Schur pass), refinement to scaled residual < 16, and the solution against
-  an FP64 solve."""
+  equal to mxp_panel_lu run with the same steps (one panel per Schur pass;
+  STRSM panels, or panels by inverse on the tensor cores with the separate
+  FP8 cast), with the look-ahead schedule on and off, refinement to scaled
+  residual < 16, and the solution against an FP64 solve."""
 import numpy as np
 import pytest
 
@@ -79,19 +80,23 @@ def test_block_gemv(mxp, torch_cuda, m, k):
     assert float((y - want).abs().max()) <= 1e-13 * float(want.abs().max())
 
 
-@pytest.mark.parametrize("form", [0, 2])
-def test_one_process_grid_solver(mxp, orc, torch_cuda, form):
+@pytest.mark.parametrize("form,trsm,lookahead", [(0, "strsm", True), (2, "strsm", True), (0, "split", True),
+                                                 (2, "split", True), (2, "single", False)])
+def test_one_process_grid_solver(mxp, orc, torch_cuda, form, trsm, lookahead):
     torch = torch_cuda
     from openmxp_b200 import grid as G
     n, b, seed = 2048, 256, 42
     be = G.CudaBackend(b, form)
-    s = G.BlockCyclicSolver(G.ProcessGrid(1, 1), n, b, seed, be, form=form)
+    s = G.BlockCyclicSolver(G.ProcessGrid(1, 1), n, b, seed, be, form=form, trsm=trsm, lookahead=lookahead)
     s.factor()
     got = to_np_colmajor(s.A, n, n, n)
-    # the single-GPU LU with the same steps: STRSM panels, one panel per Schur pass
+    # the single-GPU LU with the same steps: one panel per Schur pass, the
+    # same panel solves, the FP8 panels from the separate cast
     p = mxp.panel_matgen(n, seed)
     ws = mxp.Workspace(n, b, form)
-    ws.set_option(mxp.OPT_TRSM_TENSOR, 0)
+    ws.set_option(mxp.OPT_TRSM_TENSOR, 0 if trsm == "strsm" else 1)
+    ws.set_option(mxp.OPT_TRSM_SINGLE, 1 if trsm == "single" else 0)
+    ws.set_option(mxp.OPT_FP8_FUSED_CAST, 0)
     ws.set_option(mxp.OPT_MERGE_PANELS, 0)
     mxp.panel_lu(p, b, ws)
     want = to_np_colmajor(p.A, n, n, n)
@@ -103,6 +108,10 @@ def test_one_process_grid_solver(mxp, orc, torch_cuda, form):
     assert np.max(np.abs(x.cpu().numpy() - xt)) / np.max(np.abs(xt)) < 1e-10
     # and the oracle's restatement of the same algorithm, at the north-star bar
     LU = A.copy(order="F")
-    assert orc.panel_lu(LU, b, form) == 0
+    if trsm == "strsm":
+        assert orc.panel_lu(LU, b, form) == 0
+    else:
+        from oracle import blocked as BO
+        assert BO.panel_lu(LU, b, form, trsm=trsm) == 0
     assert rel_fro(got, LU) <= 1e-3
     be.close()
