@@ -805,10 +805,19 @@ __device__ bool tri_inverses(Smem &sm, int n, const float *A, int64_t lda, float
     const int nblk = nsteps;
     for (int it = cta; it < 2 * nblk; it += G)
         inv_diag_block(sm, n, A, lda, it < nblk ? XU : XL, ldx, it % nblk, it < nblk);
-    for (int64_t idx = (int64_t)cta * kCT + threadIdx.x; idx < (int64_t)n * n; idx += (int64_t)G * kCT) {
-        const int r = (int)(idx % n), c = (int)(idx / n);
-        if (r / kNB > c / kNB) XU[(int64_t)c * ldx + r] = 0.0f;
-        if (r / kNB < c / kNB) XL[(int64_t)c * ldx + r] = 0.0f;
+    {   // zero the opposite block-triangles: a column per warp, rows by lanes
+        // (a flat index split by 64-bit division cost ~30 us per 2560 block)
+        constexpr int W = kCT / 32;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int c = cta * W + warp; c < n; c += G * W) {
+            const int cb = c / kNB;
+            float *xu = XU + (int64_t)c * ldx, *xl = XL + (int64_t)c * ldx;
+            for (int r = lane; r < n; r += 32) {
+                const int rb = r / kNB;
+                if (rb > cb) xu[r] = 0.0f;
+                if (rb < cb) xl[r] = 0.0f;
+            }
+        }
     }
     if (!sync(23)) return false;
 
