@@ -208,16 +208,26 @@ __device__ void factor_step(Smem &sm, float *stage, float *A, int n, int k0, int
                      (t % tm) * GBM, (t / tm) * GBN);
         }
     }
-    // U strip: L X = B, one 64-row block at a time
-    for (int c = 0; c < bk; c += kNB) {
-        load_tri(sm, kNB, D + c + (int64_t)c * lda, lda);
-        for (int c0 = 0; c0 < m; c0 += kCT) trsm_cols_staged(sm, stage, m, kNB, Us + c, lda, c0);
-        __syncthreads();
-        const int rest = bk - c - kNB;
-        if (rest > 0) {
-            const int tm = (rest + GBM - 1) / GBM, tn = (m + GBN - 1) / GBN;
-            for (int t = 0; t < tm * tn; ++t)
-                tile(rest, m, D + c + kNB + (int64_t)c * lda, Us + c, Us + c + kNB, (t % tm) * GBM, (t / tm) * GBN);
+    // U strip: L X = B, one 64-row block at a time, one group of 256 columns
+    // after another.  Its columns are independent, so every element receives
+    // the same operations in the same order as with the row blocks outermost;
+    // but a column's 64-row slices (256 bytes each) are then read while the
+    // group is still in L2, instead of four passes over the whole strip from
+    // DRAM (C5: U strip 163 -> 135 ms per CTA, the diagonal triangle reloaded
+    // per group costs little).
+    for (int g0 = 0; g0 < m; g0 += kCT) {
+        const int ge = min(m, g0 + kCT);
+        for (int c = 0; c < bk; c += kNB) {
+            load_tri(sm, kNB, D + c + (int64_t)c * lda, lda);
+            trsm_cols_staged(sm, stage, m, kNB, Us + c, lda, g0);
+            __syncthreads();
+            const int rest = bk - c - kNB;
+            if (rest > 0) {
+                const int tm = (rest + GBM - 1) / GBM, tn = (ge - g0 + GBN - 1) / GBN;
+                for (int t = 0; t < tm * tn; ++t)
+                    tile(rest, ge, D + c + kNB + (int64_t)c * lda, Us + c, Us + c + kNB, (t % tm) * GBM,
+                         g0 + (t / tm) * GBN);
+            }
         }
     }
 }
