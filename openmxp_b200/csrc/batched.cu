@@ -128,16 +128,43 @@ __device__ __forceinline__ void stage_zero_row(uint8_t *base, int nblk, int row,
 
 // U-strip columns [c0, c0 + 256) of B (nb x ncols): X = L^{-1} B with L the unit
 // lower part of the diagonal block (load_tri).  The 64 x 256 block goes
-// through shared memory (stage: 256 x 65 floats) with coalesced loads and
-// stores; thread j solves column j.
+// through shared memory (stage: 256 x 65 floats) with coalesced 16-byte loads
+// and stores, all of a thread's loads in flight at once; thread j solves
+// column j.  Not inlined: the persistent kernel around it is at the register
+// limit, and the sixteen loads in flight spilled there.
 constexpr size_t kColStageOff = 65536;  // after the Smem union
 constexpr size_t kColStageBytes = sizeof(float) * kCT * (kNB + 1);
 
-__device__ void trsm_cols_staged(Smem &sm, float *stage, int ncols, int nb, float *B, int64_t ldb, int c0) {
+__device__ __noinline__ void trsm_cols_staged(Smem &sm, float *stage, int ncols, int nb, float *B, int64_t ldb,
+                                              int c0) {
+    // 16-byte loads, all sixteen of a thread in flight at once, when the
+    // columns allow them (nb = 64, B and ldb 16-byte aligned)
+    const bool vec = nb == kNB && ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && (ldb & 3) == 0;
+    if (vec) {
+        float4 v[kNB * kCT / 4 / kCT];
+#pragma unroll
+        for (int q = 0; q < kNB * kCT / 4 / kCT; ++q) {
+            const int idx = threadIdx.x + kCT * q;
+            const int k4 = idx % (kNB / 4), j = idx / (kNB / 4);
+            v[q] = c0 + j < ncols ? __ldcg(reinterpret_cast<const float4 *>(B + (int64_t)(c0 + j) * ldb) + k4)
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int q = 0; q < kNB * kCT / 4 / kCT; ++q) {
+            const int idx = threadIdx.x + kCT * q;
+            const int k4 = idx % (kNB / 4), j = idx / (kNB / 4);
+            float *st = stage + j * (kNB + 1) + 4 * k4;
+            st[0] = v[q].x;
+            st[1] = v[q].y;
+            st[2] = v[q].z;
+            st[3] = v[q].w;
+        }
+    } else {
 #pragma unroll 16
-    for (int idx = threadIdx.x; idx < kNB * kCT; idx += kCT) {
-        const int k = idx % kNB, j = idx / kNB;
-        stage[j * (kNB + 1) + k] = (k < nb && c0 + j < ncols) ? __ldcg(B + (int64_t)(c0 + j) * ldb + k) : 0.0f;
+        for (int idx = threadIdx.x; idx < kNB * kCT; idx += kCT) {
+            const int k = idx % kNB, j = idx / kNB;
+            stage[j * (kNB + 1) + k] = (k < nb && c0 + j < ncols) ? __ldcg(B + (int64_t)(c0 + j) * ldb + k) : 0.0f;
+        }
     }
     __syncthreads();
     {  // right-looking: x_r -= l_rk x_k for r > k, rotated (trsm_col)
@@ -148,9 +175,21 @@ __device__ void trsm_cols_staged(Smem &sm, float *stage, int ncols, int nb, floa
         trsm_col(sm, x, nb, stage + j * (kNB + 1));
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kNB * kCT; idx += kCT) {
-        const int k = idx % kNB, j = idx / kNB;
-        if (k < nb && c0 + j < ncols) B[(int64_t)(c0 + j) * ldb + k] = stage[j * (kNB + 1) + k];
+    if (vec) {
+#pragma unroll
+        for (int q = 0; q < kNB * kCT / 4 / kCT; ++q) {
+            const int idx = threadIdx.x + kCT * q;
+            const int k4 = idx % (kNB / 4), j = idx / (kNB / 4);
+            if (c0 + j < ncols) {
+                const float *st = stage + j * (kNB + 1) + 4 * k4;
+                reinterpret_cast<float4 *>(B + (int64_t)(c0 + j) * ldb)[k4] = make_float4(st[0], st[1], st[2], st[3]);
+            }
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < kNB * kCT; idx += kCT) {
+            const int k = idx % kNB, j = idx / kNB;
+            if (k < nb && c0 + j < ncols) B[(int64_t)(c0 + j) * ldb + k] = stage[j * (kNB + 1) + k];
+        }
     }
     __syncthreads();
 }
