@@ -117,6 +117,33 @@ __device__ __forceinline__ void stage_row(uint8_t *base, int nblk, int row, int 
     }
 }
 
+// The same for a row whose bk values are contiguous and 16-byte aligned in
+// memory (a column of the U strip, i.e. a row of R = U^T): eight values per
+// chunk as two 16-byte loads (a whole 32-byte sector per thread; the scalar
+// form read 4 bytes of a sector per load across 32 columns per warp).
+__device__ __forceinline__ void stage_row_contig(uint8_t *base, int nblk, int row, int bk, const float *src) {
+    const int rt = row >> 7, r = row & 127;
+    for (int s = 0; s < bk / kSliceK; ++s) {
+        uint8_t *blk = base + ((int64_t)s * nblk + rt) * kBlockBytes;
+        float4 lo[8], hi[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const float4 *p4 = reinterpret_cast<const float4 *>(src + s * kSliceK + c * 8);
+            lo[c] = __ldcg(p4);
+            hi[c] = __ldcg(p4 + 1);
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            uint4 q;
+            q.x = pack_h2(lo[c].x, lo[c].y);
+            q.y = pack_h2(lo[c].z, lo[c].w);
+            q.z = pack_h2(hi[c].x, hi[c].y);
+            q.w = pack_h2(hi[c].z, hi[c].w);
+            *reinterpret_cast<uint4 *>(blk + sw128_offset(r, c)) = q;
+        }
+    }
+}
+
 __device__ __forceinline__ void stage_zero_row(uint8_t *base, int nblk, int row, int bk) {
     const int rt = row >> 7, r = row & 127;
     for (int s = 0; s < bk / kSliceK; ++s) {
@@ -670,8 +697,11 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batched_kernel(BatchKernelAr
                 else
                     stage_zero_row(Lst, mp / 128, row, bk);
             }
+            const bool rvec = ((reinterpret_cast<uintptr_t>(Us) & 15) == 0) && (lda & 3) == 0;
             for (int j = threadIdx.x; j < np; j += kBatchThreads) {
-                if (j < m)
+                if (j < m && rvec)
+                    stage_row_contig(Rst, np / 128, j, bk, Us + (int64_t)j * lda);
+                else if (j < m)
                     stage_row(Rst, np / 128, j, bk, [&](int k) { return __ldcg(Us + k + (int64_t)j * lda); });
                 else
                     stage_zero_row(Rst, np / 128, j, bk);
