@@ -222,10 +222,12 @@ __device__ __noinline__ void trsm_cols_staged(Smem &sm, float *stage, int ncols,
 }
 
 // one accumulating rank-64 tile of the panel (its own register allocation: the
-// persistent kernel around it is at the register limit)
+// persistent kernel around it is at the register limit); MI / NJ = 4 for the
+// 64-row / 64-column remainders of the strips, whose padding half is skipped
+template <int MI, int NJ>
 __device__ __noinline__ void panel_tile_v(SmemGV &sv, int m, int n, const float *A, const float *B, float *C,
                                           int64_t ld, int m0, int n0) {
-    gemm_tile_v(sv, m, n, 0, kNB, -1.0f, A, ld, B, ld, true, C, ld, m0, n0);
+    gemm_tile_v<MI, NJ>(sv, m, n, 0, kNB, -1.0f, A, ld, B, ld, true, C, ld, m0, n0);
 }
 
 // ---- panel factorisation of one block step (SIMT FP32, whole CTA) -----------
@@ -238,7 +240,13 @@ __device__ void factor_step(Smem &sm, float *stage, float *A, int n, int k0, int
     SmemGV &sv = *reinterpret_cast<SmemGV *>(&sm);
     const bool vec = gemm_tile_v_ok(A, lda, A, lda, A, lda, 0);
     auto tile = [&](int tm_, int tn_, const float *Ap, const float *Bp, float *Cp, int m0, int n0) {
-        if (vec) panel_tile_v(sv, tm_, tn_, Ap, Bp, Cp, lda, m0, n0);
+        if (vec) {
+            const bool hm = tm_ - m0 <= kNB, hn = tn_ - n0 <= kNB;
+            if (hm && hn) panel_tile_v<4, 4>(sv, tm_, tn_, Ap, Bp, Cp, lda, m0, n0);
+            else if (hm) panel_tile_v<4, 8>(sv, tm_, tn_, Ap, Bp, Cp, lda, m0, n0);
+            else if (hn) panel_tile_v<8, 4>(sv, tm_, tn_, Ap, Bp, Cp, lda, m0, n0);
+            else panel_tile_v<8, 8>(sv, tm_, tn_, Ap, Bp, Cp, lda, m0, n0);
+        }
         else gemm_tile(sm, tm_, tn_, 0, kNB, -1.0f, Ap, lda, Bp, lda, true, Cp, lda, m0, n0);
     };
     float *D = A + k0 + (int64_t)k0 * lda;

@@ -240,9 +240,14 @@ __device__ __forceinline__ void gv_load_slice(SmemGVBuf &b, int m, int n, int k0
     }
 }
 
+// MI = 4 (NJ = 4): the tile's live rows (columns) are its first 64 only, the
+// caller guarantees m - m0 <= 64 (n - n0 <= 64), and the padding half is
+// neither multiplied nor stored (the live elements' operations unchanged).
+template <int MI = 8, int NJ = 8>
 __device__ void gemm_tile_v(SmemGV &sv, int m, int n, int kb, int ke, float alpha, const float *__restrict__ A,
                             int64_t lda, const float *__restrict__ B, int64_t ldb, bool accumulate, float *C,
                             int64_t ldc, int m0, int n0, int skip = 0) {
+    static_assert((MI == 4 || MI == 8) && (NJ == 4 || NJ == 8), "full or half tile sides");
     const int t = threadIdx.x;
     const int tx = t % 16, ty = t / 16;
     float(*Cs)[GBM + 4] = reinterpret_cast<float(*)[GBM + 4]>(&sv.buf[1]);
@@ -264,11 +269,11 @@ __device__ void gemm_tile_v(SmemGV &sv, int m, int n, int kb, int ke, float alph
     };
     if (c_early) load_c();
 
-    float acc[8][8];
+    float acc[MI][NJ];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < MI; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+        for (int j = 0; j < NJ; ++j) acc[i][j] = 0.0f;
 
     for (int ch = 0; ch < nch; ++ch) {
         const int k0 = kb + ch * kNB;
@@ -286,22 +291,34 @@ __device__ void gemm_tile_v(SmemGV &sv, int m, int n, int kb, int ke, float alph
         const int nk4 = (min(kNB, ke - k0) + 3) / 4;
 #pragma unroll 1
         for (int k4 = 0; k4 < nk4; ++k4) {
-            float4 bq[8];
+            float4 bq[NJ];
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
+            for (int j = 0; j < NJ; ++j)
                 bq[j] = *reinterpret_cast<const float4 *>(&b.Bs[j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4)][4 * k4]);
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
-                const float4 a0 = *reinterpret_cast<const float4 *>(&b.As[4 * k4 + s][tx * 4]);
-                const float4 a1 = *reinterpret_cast<const float4 *>(&b.As[4 * k4 + s][64 + tx * 4]);
-                const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-                float bv[8];
+                float av[MI];
+                {
+                    const float4 a0 = *reinterpret_cast<const float4 *>(&b.As[4 * k4 + s][tx * 4]);
+                    av[0] = a0.x;
+                    av[1] = a0.y;
+                    av[2] = a0.z;
+                    av[3] = a0.w;
+                }
+                if constexpr (MI == 8) {
+                    const float4 a1 = *reinterpret_cast<const float4 *>(&b.As[4 * k4 + s][64 + tx * 4]);
+                    av[MI - 4] = a1.x;
+                    av[MI - 3] = a1.y;
+                    av[MI - 2] = a1.z;
+                    av[MI - 1] = a1.w;
+                }
+                float bv[NJ];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) bv[j] = s == 0 ? bq[j].x : s == 1 ? bq[j].y : s == 2 ? bq[j].z : bq[j].w;
+                for (int j = 0; j < NJ; ++j) bv[j] = s == 0 ? bq[j].x : s == 1 ? bq[j].y : s == 2 ? bq[j].z : bq[j].w;
 #pragma unroll
-                for (int i = 0; i < 8; ++i)
+                for (int i = 0; i < MI; ++i)
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+                    for (int j = 0; j < NJ; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
             }
         }
         __syncthreads();  // buf[ch & 1] is refilled two slices on (or holds C)
@@ -312,12 +329,12 @@ __device__ void gemm_tile_v(SmemGV &sv, int m, int n, int kb, int ke, float alph
         __syncthreads();
     }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < NJ; ++j) {
         const int cl = j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4);
         const int gc = n0 + cl;
         if (gc >= n) continue;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < MI / 4; ++h) {
             const int rl = h * 64 + tx * 4, gr = m0 + rl;
             float v[4];
 #pragma unroll
