@@ -511,6 +511,49 @@ __device__ void otf_residual(int n, uint64_t seed, const double *__restrict__ d,
 // 64-row blocks, the diagonal block solved in FP64 by one warp, the block's
 // column panel applied to the remaining rows by all threads (the block
 // substitution of panel_trsv.hpp:601-747).
+// r[i] -= sum_k LU(i, c0 + k) r[c0 + k] (k = 0..63, in order) for the rows i in
+// [i_begin, i_end): a thread takes four consecutive rows and reads the block
+// column with 16-byte loads (sixteen in flight), instead of one row at a time
+// with 4-byte loads; each row's sum is the same.  Its own register allocation
+// (the persistent kernel around it is at the register limit).
+__device__ __noinline__ void block_column_update(const float *__restrict__ LU, int64_t lda, int c0, double *r,
+                                                 int i_begin, int i_end) {
+    const bool vec = ((reinterpret_cast<uintptr_t>(LU) & 15) == 0) && (lda & 3) == 0 && (i_begin & 3) == 0;
+    if (vec) {
+        for (int i = i_begin + 4 * threadIdx.x; i < i_end; i += 4 * kBatchThreads) {
+            if (i + 4 <= i_end) {
+                double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll 16
+                for (int k = 0; k < kNB; ++k) {
+                    const float4 v = __ldg(reinterpret_cast<const float4 *>(LU + (int64_t)(c0 + k) * lda + i));
+                    const double rk = r[c0 + k];
+                    a0 = __fma_rn((double)v.x, rk, a0);
+                    a1 = __fma_rn((double)v.y, rk, a1);
+                    a2 = __fma_rn((double)v.z, rk, a2);
+                    a3 = __fma_rn((double)v.w, rk, a3);
+                }
+                r[i] -= a0;
+                r[i + 1] -= a1;
+                r[i + 2] -= a2;
+                r[i + 3] -= a3;
+            } else {
+                for (int e = i; e < i_end; ++e) {
+                    double acc = 0.0;
+                    for (int k = 0; k < kNB; ++k) acc = __fma_rn((double)__ldg(LU + (int64_t)(c0 + k) * lda + e), r[c0 + k], acc);
+                    r[e] -= acc;
+                }
+            }
+        }
+    } else {
+        for (int i = i_begin + threadIdx.x; i < i_end; i += kBatchThreads) {
+            double acc = 0.0;
+#pragma unroll 16
+            for (int k = 0; k < kNB; ++k) acc = __fma_rn((double)__ldg(LU + (int64_t)(c0 + k) * lda + i), r[c0 + k], acc);
+            r[i] -= acc;
+        }
+    }
+}
+
 __device__ void lu_solve_shared(int n, const float *__restrict__ LU, double *r, float (*tri)[kNB + 1]) {
     const int64_t lda = n;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -536,12 +579,7 @@ __device__ void lu_solve_shared(int n, const float *__restrict__ LU, double *r, 
             r[c0 + 32 + lane] = z1;
         }
         __syncthreads();
-        for (int i = c0 + kNB + threadIdx.x; i < n; i += kBatchThreads) {
-            double acc = 0.0;
-#pragma unroll 16
-            for (int k = 0; k < kNB; ++k) acc = __fma_rn((double)__ldg(LU + (int64_t)(c0 + k) * lda + i), r[c0 + k], acc);
-            r[i] -= acc;
-        }
+        block_column_update(LU, lda, c0, r, c0 + kNB, n);
         __syncthreads();
     }
     for (int blk = nb - 1; blk >= 0; --blk) {  // backward, upper non-unit
@@ -564,12 +602,7 @@ __device__ void lu_solve_shared(int n, const float *__restrict__ LU, double *r, 
             r[c0 + 32 + lane] = z1;
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < c0; i += kBatchThreads) {
-            double acc = 0.0;
-#pragma unroll 16
-            for (int k = 0; k < kNB; ++k) acc = __fma_rn((double)__ldg(LU + (int64_t)(c0 + k) * lda + i), r[c0 + k], acc);
-            r[i] -= acc;
-        }
+        block_column_update(LU, lda, c0, r, 0, c0);
         __syncthreads();
     }
 }
