@@ -10,7 +10,7 @@ generated matrix on the host cores.  One JSON line per arm.
 Arms are configured as bench.py runs them: fp16_split (plain FP16 Schur,
 split-BF16 TRSM by inverse), fp8_single_fused (FP8 Schur, one BF16 TRSM
 product, E4M3 panels from the TRSM epilogues), bf16x2_split.  Bar: relative
-Frobenius distance <= 1e-3 (the north-star bar for the FP16 forms) overall
+Frobenius distance <= 1e-3 (the factor bar of the FP16 forms) overall
 and on the strict lower and upper parts.  Host memory: about 2.3 x 4 N^2
 bytes (35 GB at N=61440).
 """

@@ -1,6 +1,6 @@
 """Whole blocked LU (mxp_panel_lu) vs the oracle's restatement of
-panel_lu_async_wGPU with the same precision form.  North-star bar for the
-FP16 forms: relative Frobenius distance of the factors <= 1e-3."""
+panel_lu_async_wGPU with the same precision form.  Factor bar for the FP16
+forms: relative Frobenius distance of the factors <= 1e-3."""
 import numpy as np
 import pytest
 

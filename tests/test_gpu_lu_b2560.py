@@ -10,8 +10,8 @@ bench.py runs them:
 - BF16X2 form: split-BF16 TRSM products.
 
 N = 10240 is one full group of four panels; N = 12800 is a group plus a
-one-panel tail.  Bars: relative Frobenius distance <= 1e-3 (the north-star
-bar for the FP16 forms) overall and on the strict lower and upper parts, and
+one-panel tail.  Bars: relative Frobenius distance <= 1e-3 (the factor bar
+the FP16 forms are held to) overall and on the strict lower and upper parts, and
 element-wise: every entry of a strict part within 1e-3 of that part's
 largest entry for the split-BF16 TRSM, within 2 * 2^-8 of it for the single
 BF16 product (the GPU and the oracle reach each operand through different
