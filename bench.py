@@ -477,7 +477,7 @@ def run_gpu(args):
                 "why": ("the headline form's panels are rounded to E4M3 (2^-4) right after the TRSM, so one "
                         "BF16 product (2^-9) does not limit its factors; the reference's own production "
                         "runs use a single low-precision product too (Alt-TRSM, panel_trf_gdirect.hpp:73-107). "
-                        "The plain form keeps FP32-accurate panels as config C3 states")}
+                        "The plain form keeps FP32-accurate panels, as its method (FP32 panels) specifies")}
         if same is not None:
             line["same_trsm"] = {k: same[k] for k in ("form", "value", "ms_per_step", "ir", "phases_ms", "ir_ms")}
             line["same_trsm"]["trsm"] = TRSM_TEXT[args.compare_trsm]

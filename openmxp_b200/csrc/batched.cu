@@ -287,8 +287,8 @@ __device__ void factor_step(Smem &sm, float *stage, float *A, int n, int k0, int
     // the same operations in the same order as with the row blocks outermost;
     // but a column's 64-row slices (256 bytes each) are then read while the
     // group is still in L2, instead of four passes over the whole strip from
-    // DRAM (C5: U strip 163 -> 135 ms per CTA, the diagonal triangle reloaded
-    // per group costs little).
+    // DRAM (2048 systems of orders 256..4096: U strip 163 -> 135 ms per CTA;
+    // the diagonal triangle reloaded per group costs little).
     for (int g0 = 0; g0 < m; g0 += kCT) {
         const int ge = min(m, g0 + kCT);
         for (int c = 0; c < bk; c += kNB) {
