@@ -25,8 +25,13 @@ from oracle.blocked import FORM_BF16
 
 class OracleBackend:
     def __init__(self, b: int, form: int):
-        if form not in (O.FORM_FP16, O.FORM_BF16X2):
-            raise ValueError("CPU backend: FP16 and BF16X2 forms")
+        if form not in (O.FORM_FP16, O.FORM_BF16X2, O.FORM_FP8):
+            raise ValueError("CPU backend: FP16, BF16X2 and FP8 forms")
+        if form == O.FORM_FP8 and b % 128:
+            # the E4M3 scales are per 128 x 128 tile of the operand the
+            # routine is given: with b a multiple of 128 those tiles are whole
+            # blocks, the same on every grid and in the one-process LU
+            raise ValueError("CPU backend: the FP8 form needs b % 128 == 0")
         self.b, self.form = b, form
         self.L = O.lib()
         self._full = {}

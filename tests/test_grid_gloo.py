@@ -13,6 +13,9 @@ Checks, with the depth-1 look-ahead on (the default) and off:
   every grid equal the one-process run's bit for bit, and that run matches
   the numpy restatement of the same algorithm (oracle/blocked.py panel_lu,
   whose FP32 sums run in another order) to 1e-5 relative Frobenius;
+- FP8 Schur updates with b = 128 (each E4M3 scale tile one whole block):
+  factors bit-exact with the oracle's one-process FP8 LU on 2x2, 1x2, 3x1,
+  and with the one-process run when the panels are one-BF16 products;
 - the refinement reaches scaled residual < 16 with the same iteration count
   as on one process, and the solution matches an FP64 solve of the FP64
   system to 1e-10.
@@ -179,6 +182,29 @@ def test_one_process_inverse_panels_match_blocked_oracle(inverse_lu, trsm):
     got = F1.reshape(n, n).T.astype(np.float64)
     want = np.asarray(LU, np.float64)
     assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-5
+
+
+@pytest.mark.parametrize("P,Q,lookahead,trsm", [(2, 2, True, "strsm"), (1, 2, False, "strsm"),
+                                                (3, 1, True, "strsm"), (2, 2, True, "single")])
+def test_grid_fp8_form(reference_lu, inverse_lu, P, Q, lookahead, trsm):
+    """FP8 Schur updates (E4M3 operands, one power-of-two scale per 128 x 128
+    tile): with b = 128 every scale tile is one whole block, so the factors
+    equal the one-process oracle LU's bit for bit on any grid (STRSM panels),
+    or the one-process grid run's (panels by one BF16 product, as the FP8
+    form's TRSM runs)."""
+    from oracle import oracle as O
+    n, b, seed, form = 640, 128, 42, O.FORM_FP8
+    res = _spawn(P, Q, n, b, seed, form, trsm=trsm, lookahead=lookahead)
+    LU, xt = reference_lu(n, b, seed, form)
+    F = res[0][0].reshape(n, n).T
+    if trsm == "strsm":
+        assert np.array_equal(F.view(np.uint32), np.asarray(LU, np.float32).view(np.uint32))
+    else:
+        F1, _, _ = inverse_lu(n, b, seed, form, trsm)
+        assert np.array_equal(res[0][0].view(np.uint32), F1.view(np.uint32))
+    for r, (_, x, its, conv, hpl) in res.items():
+        assert conv and hpl < 16.0, (r, hpl)
+        assert np.max(np.abs(x - xt)) / np.max(np.abs(xt)) < 1e-10
 
 
 def test_single_process_grid_matches_oracle(reference_lu):
