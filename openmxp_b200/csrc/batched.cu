@@ -144,6 +144,34 @@ __device__ __forceinline__ void stage_row_contig(uint8_t *base, int nblk, int ro
     }
 }
 
+// Four consecutive rows r4 .. r4 + 3 of a column-major panel (row i, value k at
+// src[(i - r4) + k * ld], src 16-byte aligned, ld % 4 == 0): each k read as one
+// 16-byte load of the four rows (a warp covers 128 consecutive rows, 512
+// contiguous bytes), instead of a 4-byte load per row.  Not inlined (the
+// persistent kernel around it is at the register limit).
+__device__ __noinline__ void stage_rows4(uint8_t *base, int nblk, int r4, int bk, const float *src, int64_t ld) {
+    const int rt = r4 >> 7, r = r4 & 127;
+    for (int s = 0; s < bk / kSliceK; ++s) {
+        uint8_t *blk = base + ((int64_t)s * nblk + rt) * kBlockBytes;
+#pragma unroll 2
+        for (int c = 0; c < 8; ++c) {
+            const int k = s * kSliceK + c * 8;
+            float4 v[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) v[e] = __ldcg(reinterpret_cast<const float4 *>(src + (int64_t)(k + e) * ld));
+            uint4 q0, q1, q2, q3;
+            q0.x = pack_h2(v[0].x, v[1].x); q0.y = pack_h2(v[2].x, v[3].x); q0.z = pack_h2(v[4].x, v[5].x); q0.w = pack_h2(v[6].x, v[7].x);
+            q1.x = pack_h2(v[0].y, v[1].y); q1.y = pack_h2(v[2].y, v[3].y); q1.z = pack_h2(v[4].y, v[5].y); q1.w = pack_h2(v[6].y, v[7].y);
+            q2.x = pack_h2(v[0].z, v[1].z); q2.y = pack_h2(v[2].z, v[3].z); q2.z = pack_h2(v[4].z, v[5].z); q2.w = pack_h2(v[6].z, v[7].z);
+            q3.x = pack_h2(v[0].w, v[1].w); q3.y = pack_h2(v[2].w, v[3].w); q3.z = pack_h2(v[4].w, v[5].w); q3.w = pack_h2(v[6].w, v[7].w);
+            *reinterpret_cast<uint4 *>(blk + sw128_offset(r + 0, c)) = q0;
+            *reinterpret_cast<uint4 *>(blk + sw128_offset(r + 1, c)) = q1;
+            *reinterpret_cast<uint4 *>(blk + sw128_offset(r + 2, c)) = q2;
+            *reinterpret_cast<uint4 *>(blk + sw128_offset(r + 3, c)) = q3;
+        }
+    }
+}
+
 __device__ __forceinline__ void stage_zero_row(uint8_t *base, int nblk, int row, int bk) {
     const int rt = row >> 7, r = row & 127;
     for (int s = 0; s < bk / kSliceK; ++s) {
@@ -732,11 +760,28 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batched_kernel(BatchKernelAr
             const int np = (m + TN - 1) / TN * TN;
             const float *Ls = A + (k0 + bk) + (int64_t)k0 * lda;
             const float *Us = A + k0 + (int64_t)(k0 + bk) * lda;
-            for (int row = threadIdx.x; row < mp; row += kBatchThreads) {
-                if (row < m)
-                    stage_row(Lst, mp / 128, row, bk, [&](int k) { return __ldcg(Ls + row + (int64_t)k * lda); });
-                else
-                    stage_zero_row(Lst, mp / 128, row, bk);
+            const bool lvec = ((reinterpret_cast<uintptr_t>(Ls) & 15) == 0) && (lda & 3) == 0;
+            if (lvec) {
+                for (int r4 = 4 * threadIdx.x; r4 < mp; r4 += 4 * kBatchThreads) {
+                    if (r4 + 4 <= m) {
+                        stage_rows4(Lst, mp / 128, r4, bk, Ls + r4, lda);
+                    } else {
+                        for (int row = r4; row < r4 + 4 && row < mp; ++row) {
+                            if (row < m)
+                                stage_row(Lst, mp / 128, row, bk,
+                                          [&](int k) { return __ldcg(Ls + row + (int64_t)k * lda); });
+                            else
+                                stage_zero_row(Lst, mp / 128, row, bk);
+                        }
+                    }
+                }
+            } else {
+                for (int row = threadIdx.x; row < mp; row += kBatchThreads) {
+                    if (row < m)
+                        stage_row(Lst, mp / 128, row, bk, [&](int k) { return __ldcg(Ls + row + (int64_t)k * lda); });
+                    else
+                        stage_zero_row(Lst, mp / 128, row, bk);
+                }
             }
             const bool rvec = ((reinterpret_cast<uintptr_t>(Us) & 15) == 0) && (lda & 3) == 0;
             for (int j = threadIdx.x; j < np; j += kBatchThreads) {
